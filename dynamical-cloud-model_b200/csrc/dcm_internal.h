@@ -1,0 +1,127 @@
+// dcm_internal.h -- device work areas and host-side entry points shared by
+// the kernel files and the C-ABI layer.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <utility>
+
+#include "../../include/dcm.h"
+#include "dcm_common.cuh"
+
+namespace dcm {
+
+// scalars of one pressure solve, resident in device memory
+struct SolverScalars {
+    double sc_err, err, rho, alf, omg, bet, nrm, tt, ts;
+    int it, done, status, early;
+};
+
+template <typename T>
+struct SolverWork {
+    T *r, *cr, *p, *v1, *t, *sA, *sB;   // full-size vectors (halo layout)
+    const T *ae, *aw, *an, *as, *au, *ad;  // per-axis stencil coefficients
+    double* partials;
+    unsigned int* ticket;
+    SolverScalars* S;
+};
+
+// per-field scalars of one MPDATA call
+struct MpScalars {
+    double m, lbc, ubc;  // shift and shifted boundary values
+    int early;
+    int pad;
+};
+
+template <typename T>
+struct MpdataWork {
+    T** pa;            // [nq] scratch copies (ping)
+    T** pb;            // [nq] scratch copies (pong)
+    T* va[3];          // antidiffusive velocities
+    T* vl[3];          // limited velocities
+    T* beta[6];        // beta_up / beta_down (6 for the sfvt limiter)
+    double* partials;
+    unsigned int* ticket;
+    MpScalars* M;      // [nq]
+    MpScalars* Mone;   // early = 1 (used when kord < 1)
+    MpScalars* Mzero;  // all zero
+};
+
+template <typename T>
+int solver_run(SolverWork<T>& w, const Dims& d, T* x, const T* b, const T* sw,
+               const T* dzn, double tol, int itmax, int wo, int chunk,
+               cudaStream_t st, SolverScalars* host_S, int* launched_iters);
+
+template <typename T>
+int mpdata_run(MpdataWork<T>& w, const Dims& d, const Metrics<T>& mt, T dt,
+               const T* u, const T* v, const T* wv, T* const* psi_in,
+               T* const* psi_out, int nq, const double* lbc, const double* ubc,
+               int kord, int monotone, int neumann, int variant, bool vec,
+               const T* const* sadd, T dt_add, cudaStream_t st);
+
+template <typename T>
+int upwind_run(MpdataWork<T>& w, const Dims& d, const Metrics<T>& mt, T dt,
+               const T* u, const T* v, const T* wv, const T* psi_in,
+               T* psi_out, int neumann, cudaStream_t st);
+
+// --- k_dynamics.cu ---------------------------------------------------------
+enum HaloMode { HALO_FULL = 0, HALO_DIM = 1, HALO_WO = 2 };
+
+template <typename T>
+void launch_exchange(const Dims& d, T* a, int mode, T lbc, T ubc,
+                     cudaStream_t st);
+
+template <typename T>
+struct Forcing {
+    int damping_layer, forcing, divergence;
+    const T *dampfacn, *dampfac, *u_force, *v_force, *w_subs;
+    T forcing_tau;
+};
+
+// means of u,v,w,th (+ nq q fields) per level k = 0..kp+1 and, when div is
+// non-null, the divergence of rho*u (diagnostics.f90:31-153)
+template <typename T>
+void launch_means_div(const Dims& d, const Metrics<T>& mt, const T* u,
+                      const T* v, const T* w, const T* th, T* const* q, int nq,
+                      T* means /* (4+nq)*(kp+2) */, T* div, double* partials,
+                      unsigned int* ticket, cudaStream_t st);
+
+// sources (dynamics.f90:639-998); sth_reset applies the driver's sth = 0
+// first; rhs_wo applies the driver's exchange_along_dim_wo(psrc)
+template <typename T>
+void launch_sources(const Dims& d, const Metrics<T>& mt, const Forcing<T>& f,
+                    const T* ubar, const T* vbar, const T* wbar, const T* thbar,
+                    const T* zu, const T* zv, const T* zw, const T* u,
+                    const T* v, const T* w, const T* th, T* su, T* sv, T* sw,
+                    T* sth, T* rhs, int sth_reset, int rhs_wo, cudaStream_t st);
+
+template <typename T>
+void launch_advance_momentum(const Dims& d, const Metrics<T>& mt, T dt, T* u,
+                             T* v, T* w, const T* zu, const T* zv, const T* zw,
+                             const T* su, const T* sv, const T* sw, const T* p,
+                             cudaStream_t st);
+
+// resident step: advance_momentum(2dt) into tu, time filter of u in place,
+// then the exchange + boundary rows of the rotated velocities
+// (driver_code.f90:592-674)
+template <typename T>
+void launch_momentum_step(const Dims& d, const Metrics<T>& mt, T dt2, T* u,
+                          T* v, T* w, const T* zu, const T* zv, const T* zw,
+                          T* tu, T* tv, T* tw, const T* su, const T* sv,
+                          const T* sw, const T* p, cudaStream_t st);
+
+// adv_ref_state (+ optional exchange_full(0,0)) from psi into out
+template <typename T>
+void launch_adv_ref_state(const Dims& d, const Metrics<T>& mt, T dt,
+                          const T* w, const T* psi, T* out, const T* psi_ref,
+                          int exch, cudaStream_t st);
+
+template <typename T>
+void launch_advance_scalar(const Dims& d, T dt, T* a, const T* s,
+                           cudaStream_t st);
+
+// psi (+/-) psi_1d(k) over the whole array (mpdata_3d_add :175-188)
+template <typename T>
+void launch_add_profile(const Dims& d, T* a, const T* prof, T sign,
+                        cudaStream_t st);
+
+}  // namespace dcm

@@ -1,0 +1,210 @@
+/*
+ * dcm.h -- C-ABI of the B200 dynamical core (MPDATA advection + BiCGSTAB
+ * pressure solve) of UoM-maul1609/dynamical-cloud-model.
+ *
+ * Plain C types only: pointers, sizes, doubles.  Every 3-D field argument is
+ * a HOST array in the reference's own Fortran layout and kind:
+ *     real(c_double) :: a(0:kp+1, 0:jp+1, 0:ip+1)      (halo 1, k fastest)
+ * passed as its base address, exactly what a Fortran caller passes for a
+ * dimension(*) dummy through ISO_C_BINDING.  1-D profiles are
+ * real(c_double) :: p(0:n+1).  The library copies in and out and never keeps
+ * a host pointer.  Calls on one handle are synchronous and must not overlap.
+ *
+ * The MPI arguments of the reference routines (comm3d, id, rank, dims,
+ * coords) are not part of the ABI: the whole domain lives on one GPU, so the
+ * caller checks dims = [1,1,1] with dcm_check_decomposition() once.
+ *
+ * Every function returns a dcm_status.  Where the reference calls STOP, the
+ * library returns an error code instead; the Fortran shim in
+ * INTEGRATION.md prints the reference's message and stops.
+ */
+#ifndef DCM_H
+#define DCM_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    DCM_OK = 0,
+    DCM_E_NOCONV = 1,      /* bicgstab: no convergence in itmax iterations
+                              (dynamics.f90:431-434)                        */
+    DCM_E_BREAKDOWN = 2,   /* bicgstab: |omega| < tiny (dynamics.f90:414-417) */
+    DCM_E_NONFINITE = 3,   /* a residual norm became NaN / Inf              */
+    DCM_E_CUDA = 4,        /* a CUDA call failed; see dcm_last_error()      */
+    DCM_E_TIMEOUT = 5,     /* a bounded device wait expired                 */
+    DCM_E_DECOMP = 6,      /* process grid is not 1 x 1 x 1                 */
+    DCM_E_ARG = 7,         /* invalid argument                              */
+    DCM_E_UNSUPPORTED = 8  /* configuration outside the implemented path    */
+} dcm_status;
+
+/* Grid description.  All arrays are host pointers, length n+2 (index 0..n+1),
+ * as built by allocate_and_set (initialisation.f90:428-446, :505-578). */
+typedef struct {
+    int ip, jp, kp;
+    const double *dx, *dxn;        /* ip+2 */
+    const double *dy, *dyn;        /* jp+2 */
+    const double *dz, *dzn;        /* kp+2 */
+    const double *rhoa, *rhoan;    /* kp+2 */
+    const double *theta, *thetan;  /* kp+2 */
+    const double *xg, *yg, *zg;    /* ip+2, jp+2, kp+2 (bicgstab test_solver) */
+} dcm_grid;
+
+/* Optional terms of sources (dynamics.f90:800-873); NULL = all off. */
+typedef struct {
+    int damping_layer, forcing, divergence;
+    const double *dampfacn, *dampfac;  /* kp+2 */
+    const double *u_force, *v_force;   /* kp+2 */
+    const double *w_subs;              /* kp+2 */
+    double forcing_tau;
+} dcm_forcing;
+
+typedef struct dcm_handle dcm_handle;
+
+/* ---- lifetime ----------------------------------------------------------- */
+/* Replaces the first-call set-up of bicgstab (allocation of a_e..a_c and
+ * set_mat_a, dynamics.f90:330-352): the stencil coefficients are computed
+ * here once from the 1-D metrics.  device = CUDA ordinal. */
+int dcm_create(const dcm_grid *grid, int device, dcm_handle **out);
+int dcm_destroy(dcm_handle *h);
+const char *dcm_status_string(int status);
+const char *dcm_last_error(const dcm_handle *h);
+/* mpi_cart_initialise (mpi_module.f90:109-297): only dims = [1,1,1] runs
+ * here; anything else returns DCM_E_DECOMP. */
+int dcm_check_decomposition(const int dims[3]);
+
+/* ---- per-call drop-ins (host arrays in, host arrays out) -------------------- */
+
+/* bicgstab, dynamics.f90:293-444.  x: inout (warm start / solution),
+ * b: inout (replaced by the Gaussian test field when test_solver != 0 on the
+ * first call, :354-364), sw: in (bottom fix-up x(0)=x(1)-sw(0)dzn(0),
+ * :437-442).  tol = ptol; itmax = 9999 in the reference.  iters / err may be
+ * NULL.  Interior and the top/bottom rows of x follow the reference; the x/y
+ * halo columns are those of the input (the reference leaves solver residue
+ * there and the driver overwrites them with exchange_along_dim_wo). */
+int dcm_bicgstab(dcm_handle *h, double *x, double *b, const double *sw,
+                 double tol, int test_solver, int itmax, int *iters,
+                 double *err);
+
+/* sources, dynamics.f90:639-1000 with viscous = .false.: su, sv, sw (out,
+ * halos by exchange_full + surface/lid rows), sth (inout: += damping, then
+ * exchange_full), rhs (inout: k = 0..kp+1 over the interior columns).
+ * ubar..thbar are 1-D (kp+2).  zu, zv, zw are read only when damping or
+ * forcing is on. */
+int dcm_sources(dcm_handle *h, const dcm_forcing *forcing,
+                const double *ubar, const double *vbar, const double *wbar,
+                const double *thbar, const double *zu, const double *zv,
+                const double *zw, const double *u, const double *v,
+                const double *w, const double *th, double *su, double *sv,
+                double *sw, double *sth, double *rhs);
+
+/* advance_momentum, dynamics.f90:1019-1099: u,v,w (inout) for k = 0..kp,
+ * interior columns; the driver passes 2*dt (driver_code.f90:592-594). */
+int dcm_advance_momentum(dcm_handle *h, double dt, double *u, double *v,
+                         double *w, const double *zu, const double *zv,
+                         const double *zw, const double *su,
+                         const double *sv, const double *sw,
+                         const double *p);
+
+/* first_order_upstream_3d, pamm/sfvt/advection_3d.F90:39-116 (interior
+ * update only; neumann 0/1/2). */
+int dcm_first_order_upstream_3d(dcm_handle *h, double dt, const double *u,
+                                const double *v, const double *w,
+                                double *psi, int neumann);
+
+/* mpdata_3d, pamm/sfvt/advection_3d.F90:219-714.  lbc / ubc inout (shifted
+ * and unshifted as the reference does).  limiter: 0 = the linked
+ * pamm/sfvt form (:542-675), 1 = the sfvt/advection_3d.F90 form (:544-704). */
+int dcm_mpdata_3d(dcm_handle *h, double dt, const double *u, const double *v,
+                  const double *w, double *psi, double *lbc, double *ubc,
+                  int kord, int monotone, int neumann, int limiter);
+
+/* mpdata_vec_3d, pamm/sfvt/advection_3d.F90:1250-1753: psi holds nq
+ * consecutive fields (Fortran psi(:,:,:,1:nq)); lbc/ubc have length nq. */
+int dcm_mpdata_vec_3d(dcm_handle *h, double dt, const double *u,
+                      const double *v, const double *w, double *psi, int nq,
+                      double *lbc, double *ubc, int kord, int monotone,
+                      int neumann, int limiter);
+
+/* adv_ref_state, pamm/sfvt/advection_3d.F90:1148-1218 (psi_ref = thetan in
+ * the driver, driver_code.f90:518-519). */
+int dcm_adv_ref_state(dcm_handle *h, double dt, const double *w, double *psi,
+                      const double *psi_ref);
+
+/* mpdata_3d_add, pamm/sfvt/advection_3d.F90:139-190. */
+int dcm_mpdata_3d_add(dcm_handle *h, double dt, const double *u,
+                      const double *v, const double *w, double *psi,
+                      const double *psi_1d, double *lbc, double *ubc,
+                      int kord, int monotone, int neumann, int limiter);
+
+/* horizontal_means, diagnostics.f90:31-107: bars are (kp+2) each, qbar is
+ * nq*(kp+2) (Fortran qbar(0:kp+1, nq)); q may be NULL when moisture = 0. */
+int dcm_horizontal_means(dcm_handle *h, int moisture, int nq,
+                         const double *u, const double *v, const double *w,
+                         const double *th, const double *q, double *ubar,
+                         double *vbar, double *wbar, double *thbar,
+                         double *qbar);
+
+/* divergence_calc, diagnostics.f90:120-153 (interior of div written). */
+int dcm_divergence_calc(dcm_handle *h, const double *u, const double *v,
+                        const double *w, double *div);
+
+/* advance_scalar_fields_3d, sgm/subgrid_3d.f90:582-624 (whole arrays). */
+int dcm_advance_scalar_fields_3d(dcm_handle *h, double dt, double *q,
+                                 const double *sq, double *th,
+                                 const double *sth, int nq, int moisture);
+
+/* Halo exchanges of mpi_module.f90 for one rank: exchange_full (:926-1271),
+ * exchange_along_dim (:700-910), exchange_along_dim_wo (:1285-1494). */
+int dcm_exchange_full(dcm_handle *h, double *a, double lbc, double ubc);
+int dcm_exchange_along_dim(dcm_handle *h, double *a, double lbc, double ubc);
+int dcm_exchange_along_dim_wo(dcm_handle *h, double *a);
+
+/* ---- device-resident time loop ------------------------------------------- */
+/* Configuration of model_driver's dry step (driver_code.f90:304-676) with
+ * output, microphysics, radiation, land surface and subgrid off. */
+typedef struct {
+    double dt, ptol;
+    int advection_scheme;   /* 0 upwind, 1 mpdata, 2 mpdata_3d_add        */
+    int kord, monotone, limiter;
+    int itmax;              /* 9999 in the reference                       */
+    int moisture, nq, ncat; /* q categories advected by mpdata_vec_3d      */
+    const int *c_s, *c_e;   /* 1-based category bounds (ncat each)         */
+    double thbase, thtop;   /* lbc / ubc of scheme 2                       */
+    int precision;          /* 0 = FP64 (the reference's VAR_TYPE=1)      */
+    dcm_forcing forcing;
+} dcm_config;
+
+/* Host fields of the driver (all Fortran layout, double).  The three
+ * velocity time levels are passed in their current roles: u,v,w (current),
+ * zu,zv,zw (previous), tu,tv,tw (next / scratch). */
+typedef struct {
+    double *u, *v, *w, *zu, *zv, *zw, *tu, *tv, *tw;
+    double *th, *p, *su, *sv, *sw, *psrc, *div, *sth;
+    double *q, *sq;                            /* nq fields each, or NULL */
+    double *ubar, *vbar, *wbar, *thbar, *qbar; /* kp+2 (qbar nq*(kp+2))   */
+} dcm_fields;
+
+typedef struct {
+    int steps;              /* steps taken in this call                   */
+    int iters_last;         /* BiCGSTAB iterations of the last step       */
+    long long iters_total;  /* summed over the call                       */
+    double err_last;        /* final relative residual of the last solve  */
+    double ms_total;        /* device time of the call (CUDA events)      */
+} dcm_step_stats;
+
+/* Upload the driver state; roles as in dcm_fields. */
+int dcm_state_upload(dcm_handle *h, const dcm_config *cfg,
+                     const dcm_fields *f);
+/* model_driver's pre-loop rows (driver_code.f90:287-295) on the resident
+ * previous-level velocities. */
+int dcm_driver_start(dcm_handle *h);
+/* nsteps passes of the time loop on the device. */
+int dcm_step(dcm_handle *h, int nsteps, dcm_step_stats *stats);
+/* Download the state; velocities come back in their current roles. */
+int dcm_state_download(dcm_handle *h, dcm_fields *f);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DCM_H */
