@@ -1,0 +1,334 @@
+"""Benchmark of the B200 dynamical core (one JSON line on rank 0).
+
+A "step" is one pass of model_driver's time loop (driver_code.f90:304-676):
+means + divergence, sources + Poisson rhs, the BiCGSTAB pressure solve, the
+MPDATA advection of theta and the leap-frog momentum update, on seeded
+synthetic fields of the 256 x 256 x 128 dry warm bubble (dx = dy = dz = 50 m,
+dt = 1 s, kord = 3 monotone, ptol = 1e-10).  The timed steps are steps 1..K
+of the run from the initial state (a warm-up run of W steps precedes them on
+the same handle, then the initial state is uploaded again), so every arm
+times the same time steps with the same solver iteration counts.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+N > 1 (torchrun, one process per GPU): the single domain does not shard
+(whole domain on one GPU), so each rank advances its own replica of the
+workload ("replicas only"); value = all ranks' grid-point steps / max time.
+--impl reference times the CPU restatement of the reference (oracle/, the
+reference Fortran cannot be compiled here) on the host cores, rank 0 only.
+"""
+import argparse
+import importlib.util
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG_DIR = os.path.join(ROOT, "dynamical-cloud-model_b200")
+METRIC = "grid-pt-steps/s at 256x256x128"
+PEAK_FALLBACK_GBS = 6650.0
+
+
+def load_pkg():
+    if "dcm_b200" in sys.modules:
+        return sys.modules["dcm_b200"]
+    spec = importlib.util.spec_from_file_location(
+        "dcm_b200", os.path.join(PKG_DIR, "__init__.py"), submodule_search_locations=[PKG_DIR])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["dcm_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return PEAK_FALLBACK_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            if len(r) < 9:
+                continue
+            for n, v in zip(names, r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# algorithmic field passes per launch of each kernel class (reads + writes of
+# an N-point field; stencil neighbours come from cache).  Jacobi sweeps:
+# B1 3, B2 4, B3 5, C1 3, C2 4, C3 4 -> 23/6; matvecs: B4 3, C4 4 -> 3.5;
+# update 9.  Other classes per launch at this configuration.
+PASSES = {"jacobi": 23.0 / 6.0, "matvec": 3.5, "update": 9.0, "setup": 4.0,
+          "means": 5.0, "sources": 7.0, "rhs": 4.0, "adv_ref": 3.0, "mp_shift": 1.0,
+          "upwind": 5.0, "antidiff": 7.0, "beta": 7.0, "limit": 8.0, "momentum": 16.0}
+
+
+def make_case(pkg, name):
+    from dcm_b200 import cases
+    if name == "warm_bubble":
+        return cases.warm_bubble()
+    if name == "kelvin_helmholtz":
+        return cases.kelvin_helmholtz()
+    if name.startswith("warm_bubble_"):
+        ip, jp, kp = (int(x) for x in name.split("_")[-1].split("x"))
+        return cases.warm_bubble(ip=ip, jp=jp, kp=kp)
+    raise SystemExit("unknown case " + name)
+
+
+def pinned_like(a):
+    """A pinned host copy of a Fortran-ordered field (page-locked through
+    torch's caching host allocator), for the end-to-end copies."""
+    import torch
+    t = torch.empty(a.size, dtype=torch.float64, pin_memory=True)
+    v = t.numpy().reshape(a.shape[::-1]).transpose()
+    v[...] = a
+    return v, t
+
+
+def run_b200(args, rank, world, local_rank, dist):
+    pkg = load_pkg()
+    case = make_case(pkg, args.case)
+    g = case.grid
+    N = g.npoints
+    core = pkg.DynamicalCore(g, device=local_rank)
+    kw = dict(ptol=case.ptol, kord=case.kord, monotone=case.monotone)
+
+    def fresh():
+        core.upload_state(case.state, case.dt, **kw)
+        core.driver_start()
+
+    # warm-up run (allocations, first launches), then restart from step 1
+    fresh()
+    if args.warmup:
+        core.step(args.warmup)
+
+    def barrier():
+        if dist is not None:
+            import torch
+            torch.cuda.synchronize()
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- timed region (device time from CUDA events on the library stream)
+    fresh()
+    core.profile(False)  # reset the launch counters, event timing off
+    clocks = ClockSampler(local_rank)
+    barrier()
+    clocks.start()
+    st = core.step(args.steps)
+    clk = clocks.stop()
+    barrier()
+    ms = max_over_ranks(st.ms_total)
+    launches = sum(c for _, c in core.profile_read().values())
+    iters = st.iters_total
+    value = world * N * args.steps / (ms / 1e3)
+
+    # ---- per-kernel-class timing (same steps again, events around launches)
+    fresh()
+    core.profile(True)
+    st2 = core.step(args.steps)
+    prof = core.profile_read()
+    core.profile(False)
+    peak, peak_kind = peaks()
+    classes = {k: v for k, v in prof.items() if v[1] > 0}
+    dom = max(classes, key=lambda k: classes[k][0])
+    dom_ms, dom_n = classes[dom]
+    dom_bytes = PASSES.get(dom, 0.0) * N * 8.0
+    achieved = dom_bytes / (dom_ms / dom_n / 1e3) / 1e9 if dom_n else None
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "dram_traffic.json")
+    if os.path.exists(tp):
+        with open(tp) as f:
+            tr = json.load(f).get(args.case, {})
+        if dom in tr:
+            traffic = tr[dom]
+    step_bytes = (60.0 + 39.0 * iters / args.steps) * N * 8.0
+    step_gbs = step_bytes / (ms / args.steps / 1e3) / 1e9
+
+    # ---- end to end through the C-ABI with host buffers (pinned)
+    host = {n: pinned_like(getattr(case.state, n)) for n in
+            ("u", "v", "w", "zu", "zv", "zw", "tu", "tv", "tw", "th", "p")}
+    st_host = case.state.copy()
+    for n, (v, _) in host.items():
+        setattr(st_host, n, v)
+    barrier()
+    t0 = time.perf_counter()
+    core.upload_state(st_host, case.dt, **kw)
+    core.driver_start()
+    core.step(args.steps)
+    out = core.download_state()
+    t1 = time.perf_counter()
+    barrier()
+    e2e_s = max_over_ranks(t1 - t0)
+    field_bytes = g.shape[0] * g.shape[1] * g.shape[2] * 8
+    h2d = (11 + 6) * field_bytes  # 9 velocities, th, p + 6 work fields uploaded
+    d2h = sum(a.nbytes for a in out.values() if isinstance(a, np.ndarray))
+    e2e = {"value": world * N * args.steps / e2e_s, "unit": "grid-pt-steps/s",
+           "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
+           "note": "upload of the state, K steps, download of the state per K-step call"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(args, case, min(args.cpu_steps, args.steps))
+    core.close()
+    if rank != 0:
+        return None
+    return {
+        "metric": METRIC, "value": value, "unit": "grid-pt-steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded warm bubble, numpy PCG64 seed %d)" % case.seed,
+        "config": {"workload": case.name, "precision": "fp64", "grid": [g.ip, g.jp, g.kp],
+                   "dt": case.dt, "kord": case.kord, "monotone": bool(case.monotone),
+                   "ptol": case.ptol, "timed_steps": "1..%d from the initial state" % args.steps,
+                   "bicgstab_iters_per_step": iters / args.steps,
+                   "l2": "inputs larger than L2 (20 fields x 69 MB resident)",
+                   "parallelism": "replicas" if world > 1 else "single GPU"},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
+                     "traffic": traffic, "peak_kind": peak_kind,
+                     "bytes_per_launch": dom_bytes, "launches": dom_n,
+                     "avg_launch_us": dom_ms / dom_n * 1e3 if dom_n else None,
+                     "step_model_GBs": step_gbs, "step_model_frac": step_gbs / peak},
+        "kernel_ms": {k: round(v[0], 3) for k, v in classes.items()},
+        "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
+    }
+
+
+def cpu_baseline(args, case, nsteps):
+    """The oracle (CPU restatement of the reference, not the reference
+    binary) on the host cores, steps 1..nsteps of the same case."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    cores = os.cpu_count() or 1
+    oracle.set_threads(cores, True)
+    m = oracle.OracleModel(case.grid, case.state, case.dt, ptol=case.ptol, kord=case.kord,
+                           monotone=case.monotone)
+    m.driver_start()
+    t0 = time.perf_counter()
+    done = 0
+    iters = 0
+    while done < nsteps:
+        it, _ = m.step(1)
+        iters += it
+        done += 1
+        if time.perf_counter() - t0 > args.cpu_budget:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": case.grid.npoints * done / dt, "unit": "grid-pt-steps/s", "cores": cores,
+            "kind": "port",
+            "sample": "%s steps 1..%d (%d BiCGSTAB iterations), %d OpenMP threads, "
+                      "%.1f s" % (case.name, done, iters, cores, dt)}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    pkg = load_pkg()
+    case = make_case(pkg, args.case)
+    cpu = cpu_baseline(args, case, args.steps)
+    return {"impl": "reference", "metric": METRIC, "value": cpu["value"],
+            "unit": "grid-pt-steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": case.name, "precision": "fp64",
+                       "timed_steps": "1..n from the initial state"},
+            "cpu_baseline": cpu,
+            "e2e": {"value": cpu["value"], "unit": "grid-pt-steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--case", default="warm_bubble")
+    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--cpu-budget", type=float, default=60.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if args.impl == "reference":
+        res = run_reference(args, rank, world)
+    else:
+        if world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as tdist
+            torch.cuda.set_device(local_rank)
+            tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+            dist = tdist
+        res = run_b200(args, rank, world, local_rank, dist)
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+    if res is not None:
+        print(json.dumps(res), flush=True)
+
+
+if __name__ == "__main__":
+    main()

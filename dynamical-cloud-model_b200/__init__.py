@@ -106,6 +106,8 @@ def library():
             "dcm_driver_start": [P],
             "dcm_step": [P, C.c_int, C.POINTER(StepStats)],
             "dcm_state_download": [P, C.POINTER(_Fields)],
+            "dcm_profile_enable": [P, C.c_int],
+            "dcm_profile_read": [P, _dp, C.POINTER(C.c_longlong), C.c_int],
         }
         for name, args in sig.items():
             f = getattr(lib, name)
@@ -121,7 +123,12 @@ EXPORTS = ("dcm_create", "dcm_destroy", "dcm_status_string", "dcm_last_error",
            "dcm_adv_ref_state", "dcm_mpdata_3d_add", "dcm_horizontal_means",
            "dcm_divergence_calc", "dcm_advance_scalar_fields_3d", "dcm_exchange_full",
            "dcm_exchange_along_dim", "dcm_exchange_along_dim_wo", "dcm_state_upload",
-           "dcm_driver_start", "dcm_step", "dcm_state_download")
+           "dcm_driver_start", "dcm_step", "dcm_state_download", "dcm_profile_enable",
+           "dcm_profile_read")
+
+PROF_CLASSES = ("setup", "jacobi", "matvec", "update", "post", "means", "sources", "rhs",
+                "adv_ref", "mp_shift", "upwind", "antidiff", "beta", "limit", "restore",
+                "momentum", "other")
 
 
 def _ptr(a):
@@ -359,6 +366,17 @@ class DynamicalCore:
         stats = StepStats()
         self._check(self.lib.dcm_step(self.h, int(nsteps), C.byref(stats)))
         return stats
+
+    def profile(self, on=True):
+        """Enable (and reset) or disable per-kernel-class event timing."""
+        self._check(self.lib.dcm_profile_enable(self.h, int(bool(on))))
+
+    def profile_read(self):
+        n = len(PROF_CLASSES)
+        ms = (C.c_double * n)()
+        cnt = (C.c_longlong * n)()
+        self._check(self.lib.dcm_profile_read(self.h, ms, cnt, n))
+        return {k: (ms[i], cnt[i]) for i, k in enumerate(PROF_CLASSES)}
 
     def download_state(self):
         """Returns a dict of host arrays in the current roles."""

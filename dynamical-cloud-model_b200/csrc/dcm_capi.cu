@@ -8,8 +8,13 @@
 #include <vector>
 
 #include "dcm_internal.h"
+#include "dcm_prof.h"
 
 using namespace dcm;
+
+namespace dcm {
+Profiler* g_prof = nullptr;
+}
 
 namespace {
 
@@ -68,6 +73,7 @@ struct dcm_handle {
     std::vector<double*> owned;
     int last_iters = 0;
     double last_err = 0.0;
+    Profiler prof;
 };
 
 namespace {
@@ -875,6 +881,7 @@ extern "C" int dcm_step(dcm_handle* h, int nsteps, dcm_step_stats* stats) {
     CHECK_H();
     if (!h->resident || nsteps < 0) return fail(h, DCM_E_ARG, "step: no state");
     long long tot = 0;
+    g_prof = &h->prof;
     CK(cudaEventRecord(h->ev0, h->st));
     int done = 0;
     int rc = DCM_OK;
@@ -887,6 +894,8 @@ extern "C" int dcm_step(dcm_handle* h, int nsteps, dcm_step_stats* stats) {
     CK(cudaEventSynchronize(h->ev1));
     float ms = 0.f;
     cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+    if (h->prof.on) h->prof.harvest();
+    g_prof = nullptr;
     if (stats) {
         stats->steps = done;
         stats->iters_last = h->last_iters;
@@ -923,4 +932,24 @@ extern "C" int dcm_state_download(dcm_handle* h, dcm_fields* f) {
         if (f->sq) RC(download(h, f->sq + (size_t)c * h->n, h->sq[c]));
     }
     return sync(h);
+}
+
+// =============================================================================
+// diagnostics
+// =============================================================================
+extern "C" int dcm_profile_enable(dcm_handle* h, int on) {
+    CHECK_H();
+    h->prof.reset();
+    h->prof.on = on != 0;
+    return DCM_OK;
+}
+
+extern "C" int dcm_profile_read(dcm_handle* h, double* ms, long long* launches, int ncat) {
+    CHECK_H();
+    if (!ms || !launches || ncat < P_NCAT) return fail(h, DCM_E_ARG, "profile_read: ncat");
+    for (int c = 0; c < P_NCAT; c++) {
+        ms[c] = h->prof.ms[c];
+        launches[c] = h->prof.count[c];
+    }
+    return DCM_OK;
 }

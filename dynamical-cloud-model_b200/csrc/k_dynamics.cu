@@ -6,6 +6,7 @@
 // (pamm/sfvt/advection_3d.F90:1148-1218), advance_scalar_fields_3d
 // (sgm/subgrid_3d.f90:582-624) and the stand-alone halo exchanges.
 #include "dcm_internal.h"
+#include "dcm_prof.h"
 
 namespace dcm {
 
@@ -28,7 +29,9 @@ __global__ void __launch_bounds__(256) k_exchange(Dims d, T* __restrict__ a, int
 
 template <typename T>
 void launch_exchange(const Dims& d, T* a, int mode, T lbc, T ubc, cudaStream_t st) {
+    { ProfScope ps_(P_OTHER, st);
     k_exchange<T><<<interior_grid(d, d.kp), dim3(BX, BY), 0, st>>>(d, a, mode, lbc, ubc);
+    }
 }
 
 // ---- horizontal means (+ divergence) --------------------------------------
@@ -108,22 +111,32 @@ void launch_means_div(const Dims& d, const Metrics<T>& mt, const T* u, const T* 
                       unsigned int* ticket, cudaStream_t st) {
     const int K2 = d.kp + 2;
     const dim3 g((K2 + BX - 1) / BX, MEAN_GY), b(BX, BY);
+    { ProfScope ps_(P_MEANS, st);
     k_means<T, 4><<<g, b, 0, st>>>(d, mt, u, v, w, th, means, div, partials, ticket);
+    }
     for (int q0 = 0; q0 < nq; q0 += 4) {
         const int n = nq - q0 < 4 ? nq - q0 : 4;
         T* out = means + (size_t)(4 + q0) * K2;
         if (n == 4)
+            { ProfScope ps_(P_MEANS, st);
             k_means<T, 4><<<g, b, 0, st>>>(d, mt, q[q0], q[q0 + 1], q[q0 + 2], q[q0 + 3], out,
                                            nullptr, partials, ticket);
+            }
         else if (n == 3)
+            { ProfScope ps_(P_MEANS, st);
             k_means<T, 3><<<g, b, 0, st>>>(d, mt, q[q0], q[q0 + 1], q[q0 + 2], nullptr, out,
                                            nullptr, partials, ticket);
+            }
         else if (n == 2)
+            { ProfScope ps_(P_MEANS, st);
             k_means<T, 2><<<g, b, 0, st>>>(d, mt, q[q0], q[q0 + 1], nullptr, nullptr, out,
                                            nullptr, partials, ticket);
+            }
         else
+            { ProfScope ps_(P_MEANS, st);
             k_means<T, 1><<<g, b, 0, st>>>(d, mt, q[q0], nullptr, nullptr, nullptr, out,
                                            nullptr, partials, ticket);
+            }
     }
 }
 
@@ -265,10 +278,14 @@ void launch_sources(const Dims& d, const Metrics<T>& mt, const Forcing<T>& f, co
                     const T* zw, const T* u, const T* v, const T* w, const T* th, T* su, T* sv,
                     T* sw, T* sth, T* rhs, int sth_reset, int rhs_wo, cudaStream_t st) {
     const dim3 b(BX, BY);
+    { ProfScope ps_(P_SOURCES, st);
     k_sources<T><<<interior_grid(d, d.kp), b, 0, st>>>(d, mt, f, ubar, vbar, wbar, thbar, zu, zv,
                                                        zw, u, v, w, th, su, sv, sw, sth,
                                                        sth_reset);
+    }
+    { ProfScope ps_(P_RHS, st);
     k_rhs<T><<<interior_grid(d, d.kp + 2), b, 0, st>>>(d, mt, su, sv, sw, rhs, rhs_wo);
+    }
 }
 
 // ---- advance_momentum (drop-in, k = 0..kp, dynamics.f90:1053-1094) --------
@@ -301,8 +318,10 @@ template <typename T>
 void launch_advance_momentum(const Dims& d, const Metrics<T>& mt, T dt, T* u, T* v, T* w,
                              const T* zu, const T* zv, const T* zw, const T* su, const T* sv,
                              const T* sw, const T* p, cudaStream_t st) {
+    { ProfScope ps_(P_MOMENTUM, st);
     k_advance_momentum<T><<<interior_grid(d, d.kp + 1), dim3(BX, BY), 0, st>>>(
         d, mt, dt, u, v, w, zu, zv, zw, su, sv, sw, p);
+    }
 }
 
 // ---- resident momentum step ---------------------------------------------------
@@ -363,8 +382,10 @@ template <typename T>
 void launch_momentum_step(const Dims& d, const Metrics<T>& mt, T dt2, T* u, T* v, T* w,
                           const T* zu, const T* zv, const T* zw, T* tu, T* tv, T* tw,
                           const T* su, const T* sv, const T* sw, const T* p, cudaStream_t st) {
+    { ProfScope ps_(P_MOMENTUM, st);
     k_momentum_step<T><<<full_grid(d), dim3(BX, BY), 0, st>>>(d, mt, dt2, u, v, w, zu, zv, zw,
                                                               tu, tv, tw, su, sv, sw, p);
+    }
 }
 
 // ---- adv_ref_state -----------------------------------------------------------
@@ -399,7 +420,9 @@ void launch_adv_ref_state(const Dims& d, const Metrics<T>& mt, T dt, const T* w,
                           T* out, const T* psi_ref, int exch, cudaStream_t st) {
     const dim3 g = exch ? interior_grid(d, d.kp)
                         : dim3((d.kp + BX - 1) / BX, (d.J + BY - 1) / BY, d.I);
+    { ProfScope ps_(P_ADVREF, st);
     k_adv_ref<T><<<g, dim3(BX, BY), 0, st>>>(d, mt, dt, w, psi, out, psi_ref, exch);
+    }
 }
 
 // ---- whole-array updates -------------------------------------------------------
@@ -412,7 +435,9 @@ __global__ void k_axpy_all(size_t n, T dt, T* __restrict__ a, const T* __restric
 template <typename T>
 void launch_advance_scalar(const Dims& d, T dt, T* a, const T* s, cudaStream_t st) {
     const size_t n = d.n();
+    { ProfScope ps_(P_OTHER, st);
     k_axpy_all<T><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, dt, a, s);
+    }
 }
 
 template <typename T>
@@ -427,7 +452,9 @@ __global__ void k_add_profile(Dims d, T* __restrict__ a, const T* __restrict__ p
 template <typename T>
 void launch_add_profile(const Dims& d, T* a, const T* prof, T sign, cudaStream_t st) {
     const size_t n = d.n();
+    { ProfScope ps_(P_OTHER, st);
     k_add_profile<T><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(d, a, prof, sign);
+    }
 }
 
 #define INST(T)                                                                                 \

@@ -13,6 +13,7 @@
 //   k_beta      beta_up / beta_down (eqs 19/20)
 //   k_limit     limited velocities (eq 18)
 #include "dcm_internal.h"
+#include "dcm_prof.h"
 
 namespace dcm {
 
@@ -415,18 +416,24 @@ int mpdata_run(MpdataWork<T>& w, const Dims& d, const Metrics<T>& mt, T dt,
     const dim3 gf = full_grid(d);
     for (int q = 0; q < nq; q++) {
         if (vec)
+            { ProfScope ps_(P_MPMIN, st);
             k_min<T, true><<<g, b, 0, st>>>(d, psi_in[q], lbc[q], ubc[q], w.partials, w.ticket,
                                             w.M + q);
+            }
         else
+            { ProfScope ps_(P_MPMIN, st);
             k_min<T, false><<<gf, b, 0, st>>>(d, psi_in[q], lbc[q], ubc[q], w.partials, w.ticket,
                                               w.M + q);
+            }
     }
     const MpScalars* gate = w.M;
     if (kord < 1) {
         // empty iteration loop: psi = (psi - m) + m
         for (int q = 0; q < nq; q++)
+            { ProfScope ps_(P_RESTORE, st);
             k_restore<T><<<gf, b, 0, st>>>(d, psi_in[q], psi_out[q], sadd ? sadd[q] : nullptr,
                                            dt_add, w.Mone, w.M + q);
+            }
         return cudaGetLastError() == cudaSuccess ? 0 : DCM_E_CUDA;
     }
     const Vel<T> V0{u, v, wv};
@@ -434,13 +441,17 @@ int mpdata_run(MpdataWork<T>& w, const Dims& d, const Metrics<T>& mt, T dt,
     for (int q = 0; q < nq; q++) {
         const T* sa = sadd ? sadd[q] : nullptr;
         if (kord == 1)
+            { ProfScope ps_(P_UPWIND, st);
             k_upwind<T, true, true><<<g, b, 0, st>>>(d, mt, dt, V0, psi_in[q], psi_out[q], neumann,
                                                      1, sa, dt_add, w.partials, w.ticket, w.M + q,
                                                      nullptr);
+            }
         else
+            { ProfScope ps_(P_UPWIND, st);
             k_upwind<T, true, false><<<g, b, 0, st>>>(d, mt, dt, V0, psi_in[q], w.pa[q], neumann,
                                                       1, nullptr, T(0), w.partials, w.ticket,
                                                       w.M + q, nullptr);
+            }
     }
     // velocity sets: A receives antidiffusive velocities, L limited ones
     VelOut<T> A{w.va[0], w.va[1], w.va[2]}, L{w.vl[0], w.vl[1], w.vl[2]};
@@ -448,20 +459,30 @@ int mpdata_run(MpdataWork<T>& w, const Dims& d, const Metrics<T>& mt, T dt,
     T* const* cur = w.pa;
     T* const* nxt = w.pb;
     for (int it = 2; it <= kord; it++) {
+        { ProfScope ps_(P_ANTIDIFF, st);
         k_antidiff<T><<<g, b, 0, st>>>(d, mt, dt, Vcur, cur[0], A, gate);
+        }
         Vel<T> Vuse{A.u, A.v, A.w};
         if (monotone) {
             if (variant == 1) {
+                { ProfScope ps_(P_BETA, st);
                 k_beta<T, 1><<<g, b, 0, st>>>(d, mt, dt, psi_in[0], cur[0], Vuse, w.beta[0],
                                               w.beta[1], w.beta[2], w.beta[3], w.beta[4],
                                               w.beta[5], gate);
+                }
+                { ProfScope ps_(P_LIMIT, st);
                 k_limit<T, 1><<<g, b, 0, st>>>(d, Vuse, w.beta[0], w.beta[1], w.beta[2],
                                                w.beta[3], w.beta[4], w.beta[5], L, gate);
+                }
             } else {
+                { ProfScope ps_(P_BETA, st);
                 k_beta<T, 0><<<g, b, 0, st>>>(d, mt, dt, psi_in[0], cur[0], Vuse, w.beta[0],
                                               w.beta[1], nullptr, nullptr, nullptr, nullptr, gate);
+                }
+                { ProfScope ps_(P_LIMIT, st);
                 k_limit<T, 0><<<g, b, 0, st>>>(d, Vuse, w.beta[0], w.beta[1], nullptr, nullptr,
                                                nullptr, nullptr, L, gate);
+                }
             }
             // antidiff always writes A from the limited set L (:513-525, :662-667)
             Vuse = Vel<T>{L.u, L.v, L.w};
@@ -474,19 +495,25 @@ int mpdata_run(MpdataWork<T>& w, const Dims& d, const Metrics<T>& mt, T dt,
         for (int q = 0; q < nq; q++) {
             const T* sa = sadd ? sadd[q] : nullptr;
             if (last)
+                { ProfScope ps_(P_UPWIND, st);
                 k_upwind<T, false, true><<<g, b, 0, st>>>(d, mt, dt, Vuse, cur[q], psi_out[q],
                                                           neumann, 1, sa, dt_add, nullptr, nullptr,
                                                           w.M + q, gate);
+                }
             else
+                { ProfScope ps_(P_UPWIND, st);
                 k_upwind<T, false, false><<<g, b, 0, st>>>(d, mt, dt, Vuse, cur[q], nxt[q],
                                                            neumann, 1, nullptr, T(0), nullptr,
                                                            nullptr, w.M + q, gate);
+                }
         }
         std::swap(cur, nxt);
     }
     for (int q = 0; q < nq; q++)
+        { ProfScope ps_(P_RESTORE, st);
         k_restore<T><<<gf, b, 0, st>>>(d, psi_in[q], psi_out[q], sadd ? sadd[q] : nullptr, dt_add,
                                        gate, w.M + q);
+        }
     return cudaGetLastError() == cudaSuccess ? 0 : DCM_E_CUDA;
 }
 
@@ -497,8 +524,10 @@ int upwind_run(MpdataWork<T>& w, const Dims& d, const Metrics<T>& mt, T dt, cons
                cudaStream_t st) {
     const dim3 g = interior_grid(d, d.kp), b(BX, BY);
     Vel<T> V0{u, v, wv};
+    { ProfScope ps_(P_UPWIND, st);
     k_upwind<T, false, false><<<g, b, 0, st>>>(d, mt, dt, V0, psi_in, psi_out, neumann, 0, nullptr,
                                                T(0), nullptr, nullptr, w.Mzero, nullptr);
+    }
     return cudaGetLastError() == cudaSuccess ? 0 : DCM_E_CUDA;
 }
 

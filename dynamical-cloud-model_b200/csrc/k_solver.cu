@@ -22,6 +22,7 @@
 // host never waits inside an iteration.  Every kernel first checks the
 // device-side `done` flag, which lets the host launch iterations in chunks.
 #include "dcm_internal.h"
+#include "dcm_prof.h"
 
 namespace dcm {
 
@@ -365,18 +366,28 @@ static void launch_iteration(const SolverArgs& a, const Coef<T>& c,
                              SolverWork<T>& w, T* x, cudaStream_t st) {
     const dim3 g = interior_grid(a.d, a.d.kp), b(BX, BY);
     // phase B
-    k_jacobi<T, 0, 1, false><<<g, b, 0, st>>>(a, c, w.r, w.v1, nullptr, w.sA, w.S);
-    k_jacobi<T, 0, 2, false><<<g, b, 0, st>>>(a, c, w.r, w.v1, w.sA, w.sB, w.S);
-    k_jacobi<T, 0, 3, true><<<g, b, 0, st>>>(a, c, w.r, w.v1, w.sB, w.p, w.S);
-    k_bicg_matvec_p<T><<<g, b, 0, st>>>(a, c, w.p, w.cr, w.v1, w.partials, w.ticket, w.S);
+    { ProfScope ps(P_JACOBI, st);
+      k_jacobi<T, 0, 1, false><<<g, b, 0, st>>>(a, c, w.r, w.v1, nullptr, w.sA, w.S); }
+    { ProfScope ps(P_JACOBI, st);
+      k_jacobi<T, 0, 2, false><<<g, b, 0, st>>>(a, c, w.r, w.v1, w.sA, w.sB, w.S); }
+    { ProfScope ps(P_JACOBI, st);
+      k_jacobi<T, 0, 3, true><<<g, b, 0, st>>>(a, c, w.r, w.v1, w.sB, w.p, w.S); }
+    { ProfScope ps(P_MATVEC, st);
+      k_bicg_matvec_p<T><<<g, b, 0, st>>>(a, c, w.p, w.cr, w.v1, w.partials, w.ticket, w.S); }
     // phase C
-    k_jacobi<T, 1, 1, false><<<g, b, 0, st>>>(a, c, w.r, w.v1, nullptr, w.sA, w.S);
-    k_jacobi<T, 1, 2, false><<<g, b, 0, st>>>(a, c, w.r, w.v1, w.sA, w.sB, w.S);
-    k_jacobi<T, 1, 3, false><<<g, b, 0, st>>>(a, c, w.r, w.v1, w.sB, w.sA, w.S);
-    k_bicg_matvec_cs<T><<<g, b, 0, st>>>(a, c, w.sA, w.r, w.v1, w.t, w.partials, w.ticket, w.S);
+    { ProfScope ps(P_JACOBI, st);
+      k_jacobi<T, 1, 1, false><<<g, b, 0, st>>>(a, c, w.r, w.v1, nullptr, w.sA, w.S); }
+    { ProfScope ps(P_JACOBI, st);
+      k_jacobi<T, 1, 2, false><<<g, b, 0, st>>>(a, c, w.r, w.v1, w.sA, w.sB, w.S); }
+    { ProfScope ps(P_JACOBI, st);
+      k_jacobi<T, 1, 3, false><<<g, b, 0, st>>>(a, c, w.r, w.v1, w.sB, w.sA, w.S); }
+    { ProfScope ps(P_MATVEC, st);
+      k_bicg_matvec_cs<T><<<g, b, 0, st>>>(a, c, w.sA, w.r, w.v1, w.t, w.partials, w.ticket,
+                                           w.S); }
     // phase D
-    k_bicg_update<T><<<g, b, 0, st>>>(a, x, w.p, w.sA, w.r, w.v1, w.t, w.cr, w.partials,
-                                      w.ticket, w.S);
+    { ProfScope ps(P_UPDATE, st);
+      k_bicg_update<T><<<g, b, 0, st>>>(a, x, w.p, w.sA, w.r, w.v1, w.t, w.cr, w.partials,
+                                        w.ticket, w.S); }
 }
 
 template <typename T>
@@ -389,7 +400,8 @@ int solver_run(SolverWork<T>& w, const Dims& d, T* x, const T* b, const T* sw,
     a.tol = tol;
     const Coef<T> c = coef_of(w);
     const dim3 g = interior_grid(d, d.kp), bl(BX, BY);
-    k_bicg_setup<T><<<g, bl, 0, st>>>(a, c, x, b, w.r, w.cr, w.partials, w.ticket, w.S);
+    { ProfScope ps(P_SETUP, st);
+      k_bicg_setup<T><<<g, bl, 0, st>>>(a, c, x, b, w.r, w.cr, w.partials, w.ticket, w.S); }
     if (cudaGetLastError() != cudaSuccess) return DCM_E_CUDA;
     int launched = 0;
     for (;;) {
@@ -401,7 +413,8 @@ int solver_run(SolverWork<T>& w, const Dims& d, T* x, const T* b, const T* sw,
             launch_iteration<T>(a, c, w, x, st);
         if (cudaGetLastError() != cudaSuccess) return DCM_E_CUDA;
     }
-    k_bicg_post<T><<<g, bl, 0, st>>>(d, x, sw, dzn, w.S, wo);
+    { ProfScope ps(P_POST, st);
+      k_bicg_post<T><<<g, bl, 0, st>>>(d, x, sw, dzn, w.S, wo); }
     cudaMemcpyAsync(host_S, w.S, sizeof(SolverScalars), cudaMemcpyDeviceToHost, st);
     if (cudaStreamSynchronize(st) != cudaSuccess) return DCM_E_CUDA;
     if (launched_iters) *launched_iters = launched;

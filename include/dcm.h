@@ -204,6 +204,19 @@ int dcm_step(dcm_handle *h, int nsteps, dcm_step_stats *stats);
 /* Download the state; velocities come back in their current roles. */
 int dcm_state_download(dcm_handle *h, dcm_fields *f);
 
+/* ---- diagnostics (no counterpart in the reference) ----------------------- */
+/* Per-kernel-class launch counts (always kept during dcm_step) and device
+ * time (CUDA events recorded on the launching stream around every launch of
+ * dcm_step while timing is enabled).  dcm_profile_enable resets both.
+ * Classes:
+ * 0 solver setup, 1 Jacobi sweeps, 2 matvecs, 3 x/r update, 4 solver post,
+ * 5 means+divergence, 6 sources, 7 Poisson rhs, 8 adv_ref_state,
+ * 9 MPDATA shift, 10 donor cell, 11 antidiffusive velocities, 12 beta,
+ * 13 limiter, 14 MPDATA restore, 15 momentum, 16 other. */
+#define DCM_PROF_NCAT 17
+int dcm_profile_enable(dcm_handle *h, int on);
+int dcm_profile_read(dcm_handle *h, double *ms, long long *launches, int ncat);
+
 #ifdef __cplusplus
 }
 #endif

@@ -193,7 +193,8 @@ void orc_mat_ax(const orc_grid *g, double *x, double *ax) {
             A3(x, 0, j, i) = A3(x, 1, j, i);
             A3(x, kp + 1, j, i) = A3(x, kp, j, i);
         }
-    memset(ax, 0, NTOT * sizeof(double));
+#pragma omp parallel for schedule(static)
+    for (size_t q = 0; q < NTOT; q++) ax[q] = 0.0;
 #pragma omp parallel for schedule(static)
     for (int i = 1; i <= ip; i++)
         for (int j = 1; j <= jp; j++)
@@ -214,6 +215,7 @@ void orc_precondition(const orc_grid *g, const double *r, double *s,
                       int prit) {
     const int ip = g->ip, jp = g->jp, kp = g->kp;
     double *t = falloc(g);
+#pragma omp parallel for schedule(static)
     for (int i = 0; i <= ip + 1; i++)
         for (int j = 0; j <= jp + 1; j++)
             for (int k = 0; k <= kp + 1; k++)
@@ -261,6 +263,7 @@ int orc_bicgstab(const orc_grid *g, double *x, double *b, const double *sw,
     sc_err = dmax(sc_err, 0.01);
 
     orc_mat_ax(g, x, ax);
+#pragma omp parallel for schedule(static)
     for (size_t q = 0; q < n; q++) {
         r[q] = b[q] - ax[q];
         cr[q] = r[q];
@@ -281,12 +284,15 @@ int orc_bicgstab(const orc_grid *g, double *x, double *b, const double *sw,
         for (it = 1; it <= itmax; it++) {
             rho = orc_inn_prod(g, r, cr);
             bet = (rho / nrm) * (alf / omg);
+#pragma omp parallel for schedule(static)
             for (size_t q = 0; q < n; q++) t[q] = r[q] - bet * (omg * v1[q]);
             orc_precondition(g, t, s, prit);
+#pragma omp parallel for schedule(static)
             for (size_t q = 0; q < n; q++) p[q] = s[q] + bet * p[q];
             orc_mat_ax(g, p, v1);
             nrm = orc_inn_prod(g, cr, v1);
             alf = rho / nrm;
+#pragma omp parallel for schedule(static)
             for (size_t q = 0; q < n; q++) s[q] = r[q] - alf * v1[q];
             orc_precondition(g, s, cs, prit);
             orc_mat_ax(g, cs, t);
@@ -299,6 +305,7 @@ int orc_bicgstab(const orc_grid *g, double *x, double *b, const double *sw,
                 *err_out = err;
                 goto done;
             }
+#pragma omp parallel for schedule(static)
             for (size_t q = 0; q < n; q++) {
                 x[q] = x[q] + alf * p[q] + omg * cs[q];
                 r[q] = s[q] - omg * t[q];
@@ -937,6 +944,7 @@ void orc_mpdata_3d(const orc_grid *g, double dt, const double *u,
     double mn = psi[0];
     for (size_t q = 1; q < n; q++) mn = dmin(mn, psi[q]);
     mn = dmin(dmin(mn, *lbc), *ubc);
+#pragma omp parallel for schedule(static)
     for (size_t q = 0; q < n; q++) psi[q] = psi[q] - mn;
     *lbc = *lbc - mn;
     *ubc = *ubc - mn;
@@ -952,6 +960,7 @@ void orc_mpdata_3d(const orc_grid *g, double dt, const double *u,
     }
     mpdata_core(g, dt, u, v, w, psi, 1, lbc, ubc, kord, monotone, neumann,
                 limiter_variant);
+#pragma omp parallel for schedule(static)
     for (size_t q = 0; q < n; q++) psi[q] = psi[q] + mn;
     *lbc = *lbc + mn;
     *ubc = *ubc + mn;
@@ -1008,6 +1017,7 @@ void orc_adv_ref_state(const orc_grid *g, double dt, const double *w,
                        double *psi, const double *psi_ref) {
     const int ip = g->ip, jp = g->jp, kp = g->kp;
     const double *dz = g->dz, *rhoa = g->rhoa, *rhoan = g->rhoan;
+#pragma omp parallel for schedule(static)
     for (int i = 0; i <= ip + 1; i++)
         for (int j = 0; j <= jp + 1; j++)
             for (int k = 1; k <= kp; k++)
@@ -1085,6 +1095,7 @@ void orc_horizontal_means(const orc_grid *g, int moisture, int nq,
 void orc_divergence_calc(const orc_grid *g, const double *u, const double *v,
                          const double *w, double *div) {
     const int ip = g->ip, jp = g->jp, kp = g->kp;
+#pragma omp parallel for schedule(static)
     for (int i = 1; i <= ip; i++)
         for (int j = 1; j <= jp; j++)
             for (int k = 1; k <= kp; k++)
@@ -1100,6 +1111,7 @@ void orc_advance_scalar_fields_3d(const orc_grid *g, double dt, double *q,
                                   const double *sq, double *th,
                                   const double *sth, int nq, int moisture) {
     const size_t n = NTOT;
+#pragma omp parallel for schedule(static)
     for (size_t e = 0; e < n; e++) th[e] = th[e] + sth[e] * dt;
     if (moisture)
         for (size_t e = 0; e < (size_t)nq * n; e++) q[e] = q[e] + sq[e] * dt;
@@ -1212,6 +1224,7 @@ int orc_model_step(const orc_grid *g, const orc_config *c, orc_state *s) {
                          s->sw, s->p); /* :592-594 */
     orc_advance_scalar_fields_3d(g, dt, s->q, s->sq, s->th, s->sth, c->nq,
                                  c->moisture); /* :601 */
+#pragma omp parallel for schedule(static)
     for (size_t e = 0; e < n; e++) { /* time filter :618-626 */
         const double ut_ = 0.99 * u[e] + 0.01 * zu[e];
         const double vt_ = 0.99 * v[e] + 0.01 * zv[e];

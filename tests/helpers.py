@@ -1,0 +1,65 @@
+"""Seeded inputs and comparison helpers shared by the tests."""
+import numpy as np
+
+from conftest import load_dcm
+
+dcm = load_dcm()
+cases = __import__("dcm_b200.cases", fromlist=["cases"])
+
+
+def fz(g):
+    return np.zeros((g.kp + 2, g.jp + 2, g.ip + 2), order="F")
+
+
+def rand_field(g, rng, lo=-1.0, hi=1.0):
+    """Random values in every cell, halos included (the routines must read
+    the halos they are given)."""
+    a = fz(g)
+    a[...] = rng.uniform(lo, hi, size=a.shape)
+    return a
+
+
+def velocities(g, rng, dt, courant=0.35):
+    """Random velocities with |u| dt/dx <= courant, halos exchanged."""
+    u, v, w = fz(g), fz(g), fz(g)
+    for a, d in ((u, g.dx[1]), (v, g.dy[1]), (w, g.dz[1])):
+        a[...] = rng.uniform(-1.0, 1.0, size=a.shape) * courant * d / dt
+        cases.exchange_full(a, 0.0, 0.0)
+    w[0] = 0.0
+    w[g.kp + 1] = 0.0
+    return u, v, w
+
+
+def relerr(a, b, mask=None):
+    a = np.asarray(a)
+    b = np.asarray(b)
+    if mask is not None:
+        a = a[mask]
+        b = b[mask]
+    den = np.max(np.abs(b))
+    num = np.max(np.abs(a - b))
+    if den == 0.0:
+        return num
+    return num / den
+
+
+def live_mask_p(g):
+    """Cells of p that the reference computes and later reads: everything
+    except the halo rings of the top/bottom rows and the vertical halo edges,
+    which hold solver residue in the reference and are never read."""
+    m = np.ones((g.kp + 2, g.jp + 2, g.ip + 2), dtype=bool, order="F")
+    jh = np.zeros(g.jp + 2, dtype=bool)
+    jh[[0, g.jp + 1]] = True
+    ih = np.zeros(g.ip + 2, dtype=bool)
+    ih[[0, g.ip + 1]] = True
+    ring = jh[:, None] | ih[None, :]
+    m[0][ring] = False
+    m[g.kp + 1][ring] = False
+    edge = jh[:, None] & ih[None, :]
+    m[1:g.kp + 1][:, edge] = False
+    return m
+
+
+def small_bubble(ip=24, jp=20, kp=16, seed=7, dxyz=100.0):
+    return cases.warm_bubble(ip=ip, jp=jp, kp=kp, dxyz=dxyz, radius=500.0, zc=800.0,
+                             seed=seed)

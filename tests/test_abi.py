@@ -1,0 +1,57 @@
+"""CPU checks of the C-ABI boundary: the library loads without a GPU and
+exports every function include/dcm.h declares (no compute calls here)."""
+import ctypes
+import os
+import re
+
+from conftest import ROOT, load_dcm
+
+HEADER = os.path.join(ROOT, "include", "dcm.h")
+
+
+def declared():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(dcm_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_header_declares_the_boundary():
+    names = declared()
+    for n in ("dcm_create", "dcm_bicgstab", "dcm_mpdata_3d", "dcm_sources",
+              "dcm_advance_momentum", "dcm_step"):
+        assert n in names
+
+
+def test_library_exports_every_declared_symbol():
+    dcm = load_dcm()
+    lib = ctypes.CDLL(dcm.LIBPATH)
+    missing = [n for n in declared() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_binding_covers_the_exports():
+    dcm = load_dcm()
+    assert set(declared()) == set(dcm.EXPORTS)
+
+
+def test_status_strings_and_decomposition_without_gpu():
+    dcm = load_dcm()
+    lib = dcm.library()
+    assert lib.dcm_status_string(0) == b"ok"
+    assert lib.dcm_status_string(1) == b"convergence failure"
+    dcm.check_decomposition((1, 1, 1))
+    try:
+        dcm.check_decomposition((2, 1, 1))
+    except dcm.DCMError as e:
+        assert e.status == dcm.DCM_E_DECOMP
+    else:
+        raise AssertionError("a 2x1x1 process grid must be rejected")
+
+
+def test_create_rejects_bad_grid_before_touching_the_device():
+    dcm = load_dcm()
+    lib = dcm.library()
+    g = dcm._Grid()
+    g.ip, g.jp, g.kp = 8, 8, 1  # kp < 3
+    h = ctypes.c_void_p()
+    assert lib.dcm_create(ctypes.byref(g), 0, ctypes.byref(h)) == dcm.DCM_E_ARG

@@ -1,0 +1,102 @@
+"""GPU parity of the device-resident time loop (model_driver's dry step)
+against the oracle's restatement of the same loop.
+
+Bar: 1e-10 relative max-norm per field after one step (the FP64 parity bar).
+After several steps the two runs drift apart only through round-off of the
+iterative solve (tolerance 1e-10 on the residual); the multi-step tolerance
+is 1e-8 per field.
+"""
+import numpy as np
+import pytest
+
+from helpers import cases, live_mask_p, relerr, small_bubble
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ("u", "v", "w", "zu", "zv", "zw", "th", "su", "sv", "sw", "psrc", "div", "sth")
+
+
+def _run(dcm, orc, c, nsteps, **kw):
+    core = dcm.DynamicalCore(c.grid)
+    core.upload_state(c.state, c.dt, ptol=c.ptol, kord=c.kord, monotone=c.monotone,
+                      nq=c.nq, c_s=c.c_s, c_e=c.c_e, **kw)
+    core.driver_start()
+    its = [core.step(1).iters_last for _ in range(nsteps)]
+    got = core.download_state()
+    core.close()
+    m = orc.OracleModel(c.grid, c.state, c.dt, ptol=c.ptol, kord=c.kord, monotone=c.monotone,
+                        nq=c.nq, c_s=c.c_s, c_e=c.c_e, **kw)
+    m.driver_start()
+    oits = [m.step(1)[0] for _ in range(nsteps)]
+    return got, m.fields(), its, oits
+
+
+def _scaled(a, b, scale):
+    """max|a - b| relative to max(max|b|, scale): quantities that are zero up
+    to round-off (the projected divergence, the level means of v and w) are
+    measured against the size of the terms they are made of."""
+    num = np.max(np.abs(np.asarray(a) - np.asarray(b)))
+    den = max(np.max(np.abs(b)), scale)
+    return num / den if den > 0 else num
+
+
+def _compare(c, got, ref, tol):
+    g = c.grid
+    errs = {}
+    for n in FIELDS:
+        errs[n] = relerr(got[n], ref[n])
+    # div = sum of three rho*du/dx terms that cancel to round-off
+    vmax = max(np.max(np.abs(ref[n])) for n in ("u", "v", "w"))
+    errs["div"] = _scaled(got["div"], ref["div"], np.max(g.rhoa) * vmax / g.dz[1])
+    errs["p"] = relerr(got["p"], ref["p"], live_mask_p(g))
+    for n, fld in (("ubar", "u"), ("vbar", "v"), ("wbar", "w"), ("thbar", "th")):
+        errs[n] = _scaled(got[n], ref[n], np.max(np.abs(ref[fld])))
+    bad = {k: v for k, v in errs.items() if not v <= tol}
+    assert not bad, bad
+    return errs
+
+
+@pytest.mark.parametrize("case", ["bubble", "kh"])
+def test_one_step(dcm, orc, case):
+    c = small_bubble() if case == "bubble" else cases.kelvin_helmholtz(ip=40, jp=1, kp=12)
+    got, ref, its, oits = _run(dcm, orc, c, 1)
+    assert its == oits
+    _compare(c, got, ref, 1e-10)
+
+
+def test_ten_steps_bubble(dcm, orc):
+    c = small_bubble()
+    got, ref, its, oits = _run(dcm, orc, c, 10)
+    assert max(abs(a - b) for a, b in zip(its, oits)) <= 1
+    _compare(c, got, ref, 1e-8)
+
+
+@pytest.mark.parametrize("scheme,limiter", [(0, 0), (2, 0), (1, 1)])
+def test_scheme_variants(dcm, orc, scheme, limiter):
+    c = small_bubble(ip=16, jp=12, kp=12)
+    kw = dict(advection_scheme=scheme, limiter=limiter)
+    if scheme == 2:
+        kw.update(thbase=float(c.grid.thetan[0]), thtop=float(c.grid.thetan[-1]))
+    got, ref, its, oits = _run(dcm, orc, c, 2, **kw)
+    _compare(c, got, ref, 1e-10)
+
+
+def test_tracers(dcm, orc):
+    c = cases.sheared_convection(ip=16, jp=12, kp=12, ntracers=3)
+    got, ref, its, oits = _run(dcm, orc, c, 2)
+    _compare(c, got, ref, 1e-10)
+    for q in range(3):
+        assert relerr(got["q"][q], ref["q"][q]) <= 1e-10
+
+
+def test_damping_forcing(dcm, orc):
+    c = small_bubble(ip=16, jp=12, kp=12)
+    K2 = c.grid.kp + 2
+    z = c.grid.z
+    forcing = dict(damping_layer=1, forcing=1, divergence=1,
+                   dampfacn=np.where(c.grid.zn > 800.0, -1.0 / 300.0, 0.0),
+                   dampfac=np.where(z > 800.0, -1.0 / 300.0, 0.0),
+                   u_force=np.full(K2, 0.5), v_force=np.full(K2, -0.25),
+                   w_subs=-1e-5 * z, forcing_tau=900.0)
+    got, ref, its, oits = _run(dcm, orc, c, 2, forcing=forcing)
+    _compare(c, got, ref, 1e-10)

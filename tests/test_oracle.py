@@ -1,0 +1,152 @@
+"""CPU tests of the oracle (the CPU restatement used as the checker).
+
+Parity with the Fortran reference is unpinned (no compiler for it here and no
+golden vectors in it); these tests pin the restatement to independent
+restatements and to analytic invariants instead.
+"""
+import numpy as np
+import pytest
+
+from helpers import cases, fz, rand_field, relerr, small_bubble, velocities
+
+
+@pytest.fixture(scope="module")
+def g():
+    return small_bubble().grid
+
+
+def test_exchange_full_matches_independent_restatement(orc, g):
+    rng = np.random.default_rng(0)
+    a = rand_field(g, rng)
+    b = a.copy(order="F")
+    orc.OracleCore(g).exchange_full(a, 0.25, -0.5)
+    cases.exchange_full(b, 0.25, -0.5)
+    assert np.array_equal(a, b)
+
+
+def test_exchange_along_dim_rows_and_faces(orc, g):
+    rng = np.random.default_rng(1)
+    a = rand_field(g, rng)
+    ref = a.copy(order="F")
+    orc.OracleCore(g).exchange_along_dim(a, 3.0, 4.0)
+    kp, jp, ip = g.kp, g.jp, g.ip
+    assert np.all(a[0] == 3.0) and np.all(a[kp + 1] == 4.0)
+    assert np.array_equal(a[1:kp + 1, 1:jp + 1, 0], ref[1:kp + 1, 1:jp + 1, ip])
+    assert np.array_equal(a[1:kp + 1, 0, 1:ip + 1], ref[1:kp + 1, jp, 1:ip + 1])
+    # vertical edges untouched
+    assert np.array_equal(a[1:kp + 1, 0, 0], ref[1:kp + 1, 0, 0])
+
+
+def test_mpdata_keeps_constant_in_nondivergent_flow(orc, g):
+    """u(z), v(z), w = 0 is non-divergent: a constant tracer must stay
+    constant through kord = 3 monotone MPDATA."""
+    rng = np.random.default_rng(2)
+    o = orc.OracleCore(g)
+    u, v, w = fz(g), fz(g), fz(g)
+    prof = rng.uniform(-3, 3, size=g.kp + 2)
+    u[...] = prof[:, None, None]
+    v[...] = -prof[:, None, None]
+    psi = fz(g) + 1.7
+    lb, ub = o.mpdata_3d(1.0, u, v, w, psi, 1.7, 1.7, 3, True)
+    assert np.max(np.abs(psi - 1.7)) < 1e-13
+    assert lb == 1.7 and ub == 1.7
+
+
+def test_mpdata_conserves_mass(orc, g):
+    """Periodic x, y and w = 0 at the bottom and top faces: sum rhoan*psi is
+    conserved to round-off by the donor cell and the antidiffusive passes."""
+    rng = np.random.default_rng(3)
+    o = orc.OracleCore(g)
+    u, v, w = velocities(g, rng, 1.0)
+    w[g.kp] = 0.0
+    psi = rand_field(g, rng, 0.0, 1.0)
+    cases.exchange_full(psi, 0.0, 0.0)
+    m0 = np.sum(g.rhoan[1:-1, None, None] * psi[1:-1, 1:-1, 1:-1])
+    o.mpdata_3d(1.0, u, v, w, psi, 0.0, 0.0, 3, True)
+    m1 = np.sum(g.rhoan[1:-1, None, None] * psi[1:-1, 1:-1, 1:-1])
+    assert abs(m1 - m0) / abs(m0) < 1e-12
+
+
+def test_mpdata_monotone_bounds(orc, g):
+    """The FCT limiter keeps the result inside the range spanned by the input
+    and its donor-cell update (the flow is divergent, so the donor cell may
+    itself exceed the input range); without the limiter it overshoots."""
+    rng = np.random.default_rng(4)
+    o = orc.OracleCore(g)
+    u, v, w = velocities(g, rng, 1.0, courant=0.2)
+    psi = fz(g)
+    psi[1:-1, 1:-1, 1:-1] = (rng.uniform(size=(g.kp, g.jp, g.ip)) > 0.7).astype(float)
+    cases.exchange_full(psi, 0.0, 0.0)
+    up = psi.copy(order="F")
+    o.first_order_upstream_3d(1.0, u, v, w, up)
+    lo = min(psi.min(), up[1:-1, 1:-1, 1:-1].min())
+    hi = max(psi.max(), up[1:-1, 1:-1, 1:-1].max())
+    free = psi.copy(order="F")
+    o.mpdata_3d(1.0, u, v, w, psi, 0.0, 0.0, 3, True)
+    assert psi.min() >= lo - 1e-12 and psi.max() <= hi + 1e-12
+    o.mpdata_3d(1.0, u, v, w, free, 0.0, 0.0, 3, False)
+    assert free.max() > hi or free.min() < lo
+
+
+def test_bicgstab_manufactured_solution(orc, g):
+    """b = A p* for a smooth p* obeying the Neumann rows; the solve from zero
+    must reproduce p* up to the null space (a constant) within tolerance."""
+    o = orc.OracleCore(g)
+    kp, jp, ip = g.kp, g.jp, g.ip
+    X = 2 * np.pi * np.arange(ip + 2) / ip
+    Y = 2 * np.pi * np.arange(jp + 2) / jp
+    Z = np.pi * (np.arange(kp + 2) - 0.5) / kp
+    ps = np.asfortranarray(np.cos(Z)[:, None, None] * np.cos(X)[None, None, :] *
+                           (1 + 0.5 * np.sin(Y))[None, :, None])
+    b = fz(g)
+    o.mat_ax(ps.copy(order="F"), b)
+    x = fz(g)
+    sw = fz(g)
+    st, it, err = o.bicgstab(x, b, sw, 1e-10)
+    assert st == 0 and err < 1e-10 and it > 0
+    d = x[1:-1, 1:-1, 1:-1] - ps[1:-1, 1:-1, 1:-1]
+    d -= d.mean()
+    assert np.max(np.abs(d)) < 1e-6 * np.max(np.abs(ps))
+
+
+def test_bicgstab_itmax_reports_noconv(orc, g):
+    rng = np.random.default_rng(5)
+    o = orc.OracleCore(g)
+    b = fz(g)
+    b[1:-1, 1:-1, 1:-1] = rng.normal(size=(g.kp, g.jp, g.ip))
+    b[1:-1, 1:-1, 1:-1] -= b[1:-1, 1:-1, 1:-1].mean()
+    st, it, err = o.bicgstab(fz(g), b, fz(g), 1e-10, itmax=1)
+    assert st == 1 and it == 1 and err > 1e-10
+
+
+def test_horizontal_means_match_numpy(orc, g):
+    rng = np.random.default_rng(6)
+    f = [rand_field(g, rng) for _ in range(4)]
+    bars = orc.OracleCore(g).horizontal_means(*f)
+    for a, bar in zip(f, bars[:4]):
+        ref = a[:, 1:-1, 1:-1].mean(axis=(1, 2))
+        assert relerr(bar, ref) < 1e-14
+
+
+def test_step_projection_is_divergence_free(orc):
+    """After a step the rho-weighted divergence of the new velocity is at the
+    level of the solver tolerance (the pressure projection works)."""
+    c = small_bubble()
+    m = orc.OracleModel(c.grid, c.state, c.dt, ptol=c.ptol, kord=c.kord)
+    m.driver_start()
+    m.step(2)
+    f = m.fields()
+    div = fz(c.grid)
+    m.core.divergence_calc(f["u"], f["v"], f["w"], div)
+    rho_u = np.max(np.abs(f["w"])) * np.max(c.grid.rhoa) / c.grid.dz[1]
+    assert np.max(np.abs(div[1:-1, 1:-1, 1:-1])) < 1e-6 * rho_u
+
+
+def test_step_kh_2d_runs(orc):
+    c = cases.kelvin_helmholtz(ip=32, jp=1, kp=16)
+    m = orc.OracleModel(c.grid, c.state, c.dt, ptol=c.ptol, kord=c.kord)
+    m.driver_start()
+    it, err = m.step(3)
+    assert it > 0 and err < 1e-10
+    f = m.fields()
+    assert np.all(np.isfinite(f["u"])) and np.all(np.isfinite(f["th"]))
