@@ -47,6 +47,9 @@ struct dcm_handle {
     double* partials = nullptr;
     size_t npartials = 0;
     unsigned int* ticket = nullptr;
+    double* gpartials = nullptr;  // two-level reductions
+    unsigned int* gtick = nullptr;
+    unsigned int* ticket2 = nullptr;
     SolverScalars* S = nullptr;
     SolverScalars* hS = nullptr;  // pinned
     MpScalars* M = nullptr;       // NQMAX + 2 (Mone, Mzero)
@@ -111,7 +114,7 @@ double* slot(dcm_handle* h, int idx) {
 enum {
     S_U = 0, S_V, S_W, S_ZU, S_ZV, S_ZW, S_SU, S_SV, S_SW, S_P, S_TH, S_STH, S_RHS, S_X, S_B,
     // solver work
-    S_R, S_CR, S_PP, S_V1, S_T, S_SA, S_SB,
+    S_R, S_CR, S_PP, S_V1, S_T, S_SA, S_SB, S_RH, S_VH,
     // mpdata work
     S_VA0, S_VA1, S_VA2, S_VL0, S_VL1, S_VL2, S_B0, S_B1, S_B2, S_B3, S_B4, S_B5,
     S_PSI_OUT,
@@ -140,8 +143,11 @@ SolverWork<double> solver_work(dcm_handle* h) {
     SolverWork<double> w;
     w.r = slot(h, S_R); w.cr = slot(h, S_CR); w.p = slot(h, S_PP); w.v1 = slot(h, S_V1);
     w.t = slot(h, S_T); w.sA = slot(h, S_SA); w.sB = slot(h, S_SB);
+    w.rh = slot(h, S_RH); w.vh = slot(h, S_VH);
     w.ae = h->ae; w.aw = h->aw; w.an = h->an; w.as = h->as; w.au = h->au; w.ad = h->ad;
     w.partials = h->partials; w.ticket = h->ticket; w.S = h->S;
+    w.red.partials = h->partials; w.red.gpartials = h->gpartials; w.red.gtick = h->gtick;
+    w.red.ticket = h->ticket2;
     return w;
 }
 
@@ -303,6 +309,14 @@ extern "C" int dcm_create(const dcm_grid* g, int device, dcm_handle** out) {
     CK(cudaMalloc(&h->partials, h->npartials * sizeof(double)));
     CK(cudaMalloc(&h->ticket, sizeof(unsigned int)));
     CK(cudaMemset(h->ticket, 0, sizeof(unsigned int)));
+    {
+        const size_t ng = np / RGROUP + 2;
+        CK(cudaMalloc(&h->gpartials, 2 * ng * sizeof(double)));
+        CK(cudaMalloc(&h->gtick, ng * sizeof(unsigned int)));
+        CK(cudaMemset(h->gtick, 0, ng * sizeof(unsigned int)));
+        CK(cudaMalloc(&h->ticket2, sizeof(unsigned int)));
+        CK(cudaMemset(h->ticket2, 0, sizeof(unsigned int)));
+    }
     CK(cudaMalloc(&h->S, sizeof(SolverScalars)));
     CK(cudaMemset(h->S, 0, sizeof(SolverScalars)));
     CK(cudaMallocHost(&h->hS, sizeof(SolverScalars)));
@@ -334,6 +348,9 @@ extern "C" int dcm_destroy(dcm_handle* h) {
     cudaFree(h->metric_block);
     cudaFree(h->partials);
     cudaFree(h->ticket);
+    cudaFree(h->gpartials);
+    cudaFree(h->gtick);
+    cudaFree(h->ticket2);
     cudaFree(h->S);
     cudaFreeHost(h->hS);
     cudaFree(h->M);
@@ -386,7 +403,7 @@ extern "C" int dcm_bicgstab(dcm_handle* h, double* x, double* b, const double* s
     double *X = slot(h, S_X), *B = slot(h, S_B), *SW = slot(h, S_SW);
     NEED(X); NEED(B); NEED(SW);
     SolverWork<double> w = solver_work(h);
-    NEED(w.r); NEED(w.sB);
+    NEED(w.r); NEED(w.sB); NEED(w.rh); NEED(w.vh);
     RC(upload(h, X, x));
     RC(upload(h, B, b));
     RC(upload(h, SW, sw));
@@ -719,7 +736,7 @@ int one_step(dcm_handle* h) {
     CK(cudaGetLastError());
     // bicgstab + exchange_along_dim_wo(p), :496-507
     SolverWork<double> sw = solver_work(h);
-    NEED(sw.r); NEED(sw.sB);
+    NEED(sw.r); NEED(sw.sB); NEED(sw.rh); NEED(sw.vh);
     h->first_call = 0;
     const int st = solver_run<double>(sw, d, h->p, h->psrc, h->sw, h->mt.dzn, c.ptol, c.itmax, 1,
                                       4, h->st, h->hS, nullptr);

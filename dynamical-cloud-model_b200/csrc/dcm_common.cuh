@@ -233,4 +233,67 @@ __device__ __forceinline__ void final_reduce(double (&out)[NV],
 
 inline unsigned int nblocks_of(dim3 g) { return g.x * g.y * g.z; }
 
+// Two-level deterministic reduction for grids of many blocks: blocks are
+// grouped by consecutive index (RGROUP per group); the last block of a group
+// (group ticket) sums the group's partials in a fixed order, and the last
+// group (global ticket) sums the group partials in a fixed order.  The
+// atomics spread over many addresses instead of one.  Call with the block
+// result valid in thread 0 of v; returns true in the single block that holds
+// the final result (valid in thread 0 of out).  Tickets are reset for reuse.
+constexpr int RGROUP = 64;
+
+struct Red2 {
+    double* partials;     // NV * nblocks
+    double* gpartials;    // NV * ngroups
+    unsigned int* gtick;  // ngroups
+    unsigned int* ticket; // 1
+};
+
+template <int NV>
+__device__ __forceinline__ bool reduce2(const double (&v)[NV], const Red2& R, double* smem,
+                                        double (&out)[NV]) {
+    __shared__ int s_flag;
+    const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+    const int nthreads = blockDim.x * blockDim.y * blockDim.z;
+    const unsigned int nb = gridDim.x * gridDim.y * gridDim.z;
+    const unsigned int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+    const unsigned int ng = (nb + RGROUP - 1) / RGROUP;
+    const unsigned int g = bid / RGROUP;
+    const unsigned int gsize = min((unsigned int)RGROUP, nb - g * RGROUP);
+    if (tid == 0) {
+#pragma unroll
+        for (int q = 0; q < NV; q++) R.partials[(size_t)q * nb + bid] = v[q];
+        __threadfence();
+        s_flag = (atomicAdd(R.gtick + g, 1u) == gsize - 1);
+    }
+    __syncthreads();
+    if (!s_flag) return false;
+    __threadfence();
+    double x[NV];
+#pragma unroll
+    for (int q = 0; q < NV; q++)
+        x[q] = tid < (int)gsize ? __ldcg(R.partials + (size_t)q * nb + g * RGROUP + tid) : 0.0;
+    block_reduce<R_SUM, NV>(x, smem);
+    if (tid == 0) {
+#pragma unroll
+        for (int q = 0; q < NV; q++) R.gpartials[(size_t)q * ng + g] = x[q];
+        R.gtick[g] = 0u;
+        __threadfence();
+        s_flag = (atomicAdd(R.ticket, 1u) == ng - 1);
+    }
+    __syncthreads();
+    if (!s_flag) return false;
+    __threadfence();
+#pragma unroll
+    for (int q = 0; q < NV; q++) {
+        double acc = 0.0;
+        for (unsigned int b = tid; b < ng; b += nthreads) acc += __ldcg(R.gpartials + (size_t)q * ng + b);
+        out[q] = acc;
+    }
+    block_reduce<R_SUM, NV>(out, smem);
+    if (tid == 0) *R.ticket = 0u;
+    return true;
+}
+
+
 }  // namespace dcm

@@ -19,9 +19,11 @@ struct SolverScalars {
 template <typename T>
 struct SolverWork {
     T *r, *cr, *p, *v1, *t, *sA, *sB;   // full-size vectors (halo layout)
+    T *rh, *vh;                          // r / a_p and v1 / a_p
     const T *ae, *aw, *an, *as, *au, *ad;  // per-axis stencil coefficients
     double* partials;
     unsigned int* ticket;
+    Red2 red;
     SolverScalars* S;
 };
 

@@ -207,9 +207,17 @@ def test_bicgstab(setup, orc, dcm):
     assert st == 0
     assert it1 == it2
     assert err1 < 1e-10 and err2 < 1e-10
+    # Both solves stop at ||r|| < tol * max(||b||, 0.01) (dynamics.f90:370-428),
+    # so ||A (x1 - x2)|| <= 2 tol sc_err is what the algorithm guarantees;
+    # the two runs differ only in dot-product summation order.
+    d = x - x2
+    ad = fz(g)
+    ocore.mat_ax(np.asfortranarray(d), ad)
+    sc = max(np.sqrt(np.sum(b[1:-1, 1:-1, 1:-1] ** 2)), 0.01)
+    assert np.sqrt(np.sum(ad[1:-1, 1:-1, 1:-1] ** 2)) <= 2e-10 * sc
     ocore.exchange_along_dim_wo(x2)  # the driver's exchange after the solve
     m = live_mask_p(g)
-    assert relerr(x, x2, m) <= 1e-10
+    assert relerr(x, x2, m) <= 1e-9
 
 
 def test_bicgstab_noconv_status(setup, dcm):
