@@ -106,6 +106,7 @@ def library():
             "dcm_driver_start": [P],
             "dcm_step": [P, C.c_int, C.POINTER(StepStats)],
             "dcm_state_download": [P, C.POINTER(_Fields)],
+            "dcm_horizontal_means_noalloc": [C.c_int, C.c_int, C.c_int, P, P, P, P, P, P],
             "dcm_profile_enable": [P, C.c_int],
             "dcm_profile_read": [P, _dp, C.POINTER(C.c_longlong), C.c_int],
         }
@@ -124,7 +125,7 @@ EXPORTS = ("dcm_create", "dcm_destroy", "dcm_status_string", "dcm_last_error",
            "dcm_divergence_calc", "dcm_advance_scalar_fields_3d", "dcm_exchange_full",
            "dcm_exchange_along_dim", "dcm_exchange_along_dim_wo", "dcm_state_upload",
            "dcm_driver_start", "dcm_step", "dcm_state_download", "dcm_profile_enable",
-           "dcm_profile_read")
+           "dcm_profile_read", "dcm_horizontal_means_noalloc")
 
 PROF_CLASSES = ("setup", "jacobi", "matvec", "update", "post", "means", "sources", "rhs",
                 "adv_ref", "mp_shift", "upwind", "antidiff", "beta", "limit", "restore",

@@ -79,6 +79,9 @@ struct Forcing {
     T forcing_tau;
 };
 
+// blocks per level of the means reduction (its partials are 4 x (kp+2) x MEAN_GY)
+constexpr int MEAN_GY = 128;
+
 // means of u,v,w,th (+ nq q fields) per level k = 0..kp+1 and, when div is
 // non-null, the divergence of rho*u (diagnostics.f90:31-153)
 template <typename T>

@@ -38,7 +38,6 @@ void launch_exchange(const Dims& d, T* a, int mode, T lbc, T ubc, cudaStream_t s
 // threadIdx.x -> k (0..kp+1), threadIdx.y + blockIdx.y -> a fixed strided
 // set of (j,i) columns; per-(field, k) partials reduced in a fixed order by
 // the last block.  means layout: [field][k], k = 0..kp+1.
-constexpr int MEAN_GY = 128;
 
 template <typename T, int NF>
 __global__ void __launch_bounds__(256) k_means(Dims d, Metrics<T> mt, const T* f0, const T* f1,

@@ -204,6 +204,26 @@ int dcm_step(dcm_handle *h, int nsteps, dcm_step_stats *stats);
 /* Download the state; velocities come back in their current roles. */
 int dcm_state_download(dcm_handle *h, dcm_fields *f);
 
+/* ---- horizontal means without device allocation ------------------------- */
+/* No counterpart in the reference.  Same per-level means as
+ * dcm_horizontal_means (u, v, w, th over the interior columns for
+ * k = 0..kp+1, written to means[0:4*(kp+2)] as ubar, vbar, wbar, thbar), for
+ * hosts that keep the fields on the device and do not allow library code to
+ * allocate or free device memory (their memory belongs to their own pool or
+ * budget, and cudaFree would synchronise the whole device).  All pointers
+ * are device pointers; stream is a cudaStream_t (NULL = default stream) and
+ * the work is queued on it without waiting.  The reduction's scratch is a
+ * fixed 4 MiB device array inside the library, shared by every call on a
+ * device: calls whose work overlaps on the GPU race and must be serialised
+ * by the caller.  The first call on each device resolves that array's
+ * device address (with the device current); make that first call before any
+ * stream capture.  kp > DCM_NOALLOC_MAX_KP returns DCM_E_ARG. */
+#define DCM_NOALLOC_MAX_KP 1024
+int dcm_horizontal_means_noalloc(int ip, int jp, int kp, const double *u,
+                                 const double *v, const double *w,
+                                 const double *th, double *means,
+                                 void *stream);
+
 /* ---- diagnostics (no counterpart in the reference) ----------------------- */
 /* Per-kernel-class launch counts (always kept during dcm_step) and device
  * time (CUDA events recorded on the launching stream around every launch of
