@@ -52,7 +52,7 @@ class _Config(C.Structure):
                 ("itmax", C.c_int), ("moisture", C.c_int), ("nq", C.c_int), ("ncat", C.c_int),
                 ("c_s", C.POINTER(C.c_int)), ("c_e", C.POINTER(C.c_int)),
                 ("thbase", C.c_double), ("thtop", C.c_double), ("precision", C.c_int),
-                ("forcing", _Forcing)]
+                ("inner_tol", C.c_double), ("forcing", _Forcing)]
 
 
 class _Fields(C.Structure):
@@ -326,7 +326,7 @@ class DynamicalCore:
     # ---- the device-resident time loop (model_driver) ---------------------------
     def upload_state(self, state, dt, ptol=1e-10, kord=3, monotone=True, advection_scheme=1,
                      limiter=0, itmax=9999, nq=0, c_s=(), c_e=(), thbase=0.0, thtop=0.0,
-                     forcing=None, precision=0):
+                     forcing=None, precision=0, inner_tol=0.1):
         K2 = self.grid.kp + 2
         cfg = _Config()
         cfg.dt, cfg.ptol = float(dt), float(ptol)
@@ -338,6 +338,7 @@ class DynamicalCore:
         self._ce = (C.c_int * max(1, len(c_e)))(*c_e)
         cfg.c_s, cfg.c_e = self._cs, self._ce
         cfg.thbase, cfg.thtop, cfg.precision = float(thbase), float(thtop), int(precision)
+        cfg.inner_tol = float(inner_tol)
         fs, fkeep = self._forcing(forcing)
         if fs is not None:
             cfg.forcing = fs

@@ -4,6 +4,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <type_traits>
 #include <string>
 #include <vector>
 
@@ -26,14 +27,25 @@ struct DevBuf {
     size_t n = 0;
 };
 
+// resident fields of one precision (velocity time levels in buffers 0..2)
+template <typename T>
+struct State {
+    T *U[3]{}, *V[3]{}, *W[3]{};
+    T *th = nullptr, *th2 = nullptr, *su = nullptr, *sv = nullptr, *sw = nullptr,
+      *sth = nullptr, *means = nullptr;
+    std::vector<T*> q, sq, qtmp;
+};
+
 }  // namespace
 
 struct dcm_handle {
     int device = 0;
     cudaStream_t st = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    Dims d{};
-    size_t n = 0;
+    Dims d{};      // pitched device layout of the fields
+    Dims hd{};     // dense layout of the caller's host arrays
+    size_t n = 0;  // elements of a device field (pitched, without FIELD_PAD)
+    size_t nh = 0; // elements of a host field
     std::string err;
 
     // 1-D metrics (device) and the per-axis stencil coefficients
@@ -59,23 +71,33 @@ struct dcm_handle {
     std::vector<double*> slots;
     int first_call = 1;  // bicgstab_first, dynamics.f90:17
 
+    // FP32 copies for the mixed-precision form
+    float* metric_block_f = nullptr;
+    Metrics<float> mtf{};
+    float *aef = nullptr, *awf = nullptr, *anf = nullptr, *asf = nullptr, *auf = nullptr,
+          *adf = nullptr;
+    std::vector<float*> fslots;
+    SolverScalars* S2 = nullptr;   // scalars of the inner (FP32) solve
+    SolverScalars* hS2 = nullptr;  // pinned
+
     // ---- resident state -------------------------------------------------------
     bool resident = false;
     dcm_config cfg{};
     std::vector<int> cs, ce;
-    std::vector<double> forcing_host;  // 5*(kp+2)
     double* forcing_dev = nullptr;
-    double *U[3]{}, *V[3]{}, *W[3]{};
+    float* forcing_f = nullptr;
     int nstep = 0;
-    double *th = nullptr, *th2 = nullptr, *p = nullptr, *su = nullptr, *sv = nullptr,
-           *sw = nullptr, *psrc = nullptr, *div = nullptr, *sth = nullptr;
-    std::vector<double*> q, sq, qtmp;
-    double* means = nullptr;
+    int prec = 0;  // 0 FP64, 1 FP32 fields + FP64 refinement
+    State<double> s64;
+    State<float> s32;
+    double *p = nullptr, *div = nullptr, *psrc = nullptr;  // FP64 in both forms
     double t1 = 0.0, t2 = 0.0;
     std::vector<double> q1, q2;
-    std::vector<double*> owned;
+    std::vector<void*> owned;
     int last_iters = 0;
     double last_err = 0.0;
+    RefineStats last_refine{};
+    long long refine_outer_total = 0;
     Profiler prof;
 };
 
@@ -99,15 +121,32 @@ int cuda_fail(dcm_handle* h, cudaError_t e, const char* where) {
         if (e_ != cudaSuccess) return cuda_fail(h, e_, #call);    \
     } while (0)
 
+// A device field in the pitched layout: the returned pointer is FIELD_SHIFT
+// elements into a zeroed allocation of n + FIELD_PAD elements (free with
+// free_field).
+template <typename T>
+T* alloc_field(dcm_handle* h) {
+    T* raw = nullptr;
+    const size_t cnt = h->n + FIELD_PAD;
+    if (cudaMalloc(&raw, cnt * sizeof(T)) != cudaSuccess) return nullptr;
+    cudaMemsetAsync(raw, 0, cnt * sizeof(T), h->st);
+    return raw + FIELD_SHIFT;
+}
+template <typename T>
+void free_field(T* p) {
+    if (p) cudaFree(p - FIELD_SHIFT);
+}
+
 double* slot(dcm_handle* h, int idx) {
     if ((int)h->slots.size() <= idx) h->slots.resize(idx + 1, nullptr);
-    if (!h->slots[idx]) {
-        double* p = nullptr;
-        if (cudaMalloc(&p, h->n * sizeof(double)) != cudaSuccess) return nullptr;
-        cudaMemsetAsync(p, 0, h->n * sizeof(double), h->st);
-        h->slots[idx] = p;
-    }
+    if (!h->slots[idx]) h->slots[idx] = alloc_field<double>(h);
     return h->slots[idx];
+}
+
+float* fslot(dcm_handle* h, int idx) {
+    if ((int)h->fslots.size() <= idx) h->fslots.resize(idx + 1, nullptr);
+    if (!h->fslots[idx]) h->fslots[idx] = alloc_field<float>(h);
+    return h->fslots[idx];
 }
 
 // slot numbering of the per-call drop-ins
@@ -117,20 +156,32 @@ enum {
     S_R, S_CR, S_PP, S_V1, S_T, S_SA, S_SB, S_RH, S_VH,
     // mpdata work
     S_VA0, S_VA1, S_VA2, S_VL0, S_VL1, S_VL2, S_B0, S_B1, S_B2, S_B3, S_B4, S_B5,
-    S_PSI_OUT,
+    S_PSI_OUT, S_STAGE,
     S_DYN = 64  // psi fields / scratch for vec: S_DYN + 4*q + {in, out, pa, pb}
 };
 
+// n = 0: a whole field, dense host columns of kp+2 into pitched device
+// columns of K (one 2-D copy); n > 0: n contiguous elements (1-D profiles).
 int upload(dcm_handle* h, double* dst, const double* src, size_t n = 0) {
     if (!src) return DCM_OK;
-    const size_t cnt = n ? n : h->n;
-    CK(cudaMemcpyAsync(dst, src, cnt * sizeof(double), cudaMemcpyHostToDevice, h->st));
+    if (n) {
+        CK(cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyHostToDevice, h->st));
+        return DCM_OK;
+    }
+    const size_t w = (size_t)h->hd.K * sizeof(double);
+    CK(cudaMemcpy2DAsync(dst, (size_t)h->d.K * sizeof(double), src, w, w,
+                         (size_t)h->d.J * h->d.I, cudaMemcpyHostToDevice, h->st));
     return DCM_OK;
 }
 int download(dcm_handle* h, double* dst, const double* src, size_t n = 0) {
     if (!dst) return DCM_OK;
-    const size_t cnt = n ? n : h->n;
-    CK(cudaMemcpyAsync(dst, src, cnt * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    if (n) {
+        CK(cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+        return DCM_OK;
+    }
+    const size_t w = (size_t)h->hd.K * sizeof(double);
+    CK(cudaMemcpy2DAsync(dst, w, src, (size_t)h->d.K * sizeof(double), w,
+                         (size_t)h->d.J * h->d.I, cudaMemcpyDeviceToHost, h->st));
     return DCM_OK;
 }
 int sync(dcm_handle* h) {
@@ -248,12 +299,14 @@ extern "C" int dcm_create(const dcm_grid* g, int device, dcm_handle** out) {
                              g->dzn, g->rhoa, g->rhoan, g->theta, g->thetan};
     for (auto p : req)
         if (!p) return DCM_E_ARG;
-    const Dims d = make_dims(g->ip, g->jp, g->kp);
-    if (d.n() >= (size_t)1 << 31) return DCM_E_UNSUPPORTED;  // int32 indexing
+    const Dims d = make_dims_pitched(g->ip, g->jp, g->kp);
+    if (d.n() + FIELD_PAD >= (size_t)1 << 31) return DCM_E_UNSUPPORTED;  // int32 indexing
     dcm_handle* h = new dcm_handle();
     h->device = device;
     h->d = d;
+    h->hd = make_dims(g->ip, g->jp, g->kp);
     h->n = d.n();
+    h->nh = h->hd.n();
     CK(cudaSetDevice(device));
     CK(cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking));
     CK(cudaEventCreate(&h->ev0));
@@ -261,13 +314,19 @@ extern "C" int dcm_create(const dcm_grid* g, int device, dcm_handle** out) {
     const size_t I2 = g->ip + 2, J2 = g->jp + 2, K2 = g->kp + 2;
     // metrics block: dx dxn (I2) dy dyn (J2) dz dzn rhoa rhoan theta thetan (K2)
     //                ae aw (I2) an as (J2) au ad (K2)
-    const size_t nm = 2 * I2 + 2 * J2 + 6 * K2 + 2 * I2 + 2 * J2 + 2 * K2;
+    // Each table starts FIELD_SHIFT elements past a multiple of FIELD_ALIGN,
+    // so its element 1 is aligned like the fields' k = 1 (16-byte vector
+    // loads of per-level coefficients); FIELD_PAD spare elements follow each.
+    auto slot_len = [](size_t len) {
+        return (len + FIELD_PAD + FIELD_ALIGN - 1) / FIELD_ALIGN * FIELD_ALIGN;
+    };
+    const size_t nm = 4 * slot_len(I2) + 4 * slot_len(J2) + 8 * slot_len(K2) + FIELD_ALIGN;
     std::vector<double> hm(nm, 0.0);
-    size_t o = 0;
+    size_t o = FIELD_SHIFT;
     auto put = [&](const double* src, size_t len) {
         const size_t at = o;
         std::memcpy(hm.data() + o, src, len * sizeof(double));
-        o += len;
+        o += slot_len(len);
         return at;
     };
     const size_t o_dx = put(g->dx, I2), o_dxn = put(g->dxn, I2), o_dy = put(g->dy, J2),
@@ -327,14 +386,31 @@ extern "C" int dcm_create(const dcm_grid* g, int device, dcm_handle** out) {
     CK(cudaMemcpy(h->M, h->hM, (NQMAX + 2) * sizeof(MpScalars), cudaMemcpyHostToDevice));
     CK(cudaMalloc(&h->forcing_dev, 5 * K2 * sizeof(double)));
     CK(cudaMemset(h->forcing_dev, 0, 5 * K2 * sizeof(double)));
+    CK(cudaMalloc(&h->forcing_f, 5 * K2 * sizeof(float)));
+    CK(cudaMemset(h->forcing_f, 0, 5 * K2 * sizeof(float)));
+    // FP32 copies of the metric block for the mixed-precision form
+    CK(cudaMalloc(&h->metric_block_f, nm * sizeof(float)));
+    launch_convert<float, double>(nm, h->metric_block_f, h->metric_block, h->st);
+    float* mf = h->metric_block_f;
+    h->mtf.dx = mf + o_dx; h->mtf.dxn = mf + o_dxn; h->mtf.dy = mf + o_dy; h->mtf.dyn = mf + o_dyn;
+    h->mtf.dz = mf + o_dz; h->mtf.dzn = mf + o_dzn; h->mtf.rhoa = mf + o_ra;
+    h->mtf.rhoan = mf + o_rn; h->mtf.theta = mf + o_th; h->mtf.thetan = mf + o_thn;
+    h->aef = mf + o_ae; h->awf = mf + o_aw; h->anf = mf + o_an; h->asf = mf + o_as;
+    h->auf = mf + o_au; h->adf = mf + o_ad;
+    CK(cudaMalloc(&h->S2, sizeof(SolverScalars)));
+    CK(cudaMemset(h->S2, 0, sizeof(SolverScalars)));
+    CK(cudaMallocHost(&h->hS2, sizeof(SolverScalars)));
+    CK(cudaStreamSynchronize(h->st));
     *out = h;
     return DCM_OK;
 }
 
 static void free_state(dcm_handle* h) {
-    for (double* p : h->owned) cudaFree(p);
+    for (void* p : h->owned) cudaFree(p);
     h->owned.clear();
-    h->q.clear(); h->sq.clear(); h->qtmp.clear();
+    h->s64 = State<double>();
+    h->s32 = State<float>();
+    h->p = h->div = h->psrc = nullptr;
     h->resident = false;
 }
 
@@ -343,8 +419,12 @@ extern "C" int dcm_destroy(dcm_handle* h) {
     cudaSetDevice(h->device);
     if (h->st) cudaStreamSynchronize(h->st);
     free_state(h);
-    for (double* p : h->slots)
-        if (p) cudaFree(p);
+    for (double* p : h->slots) free_field(p);
+    for (float* p : h->fslots) free_field(p);
+    cudaFree(h->metric_block_f);
+    cudaFree(h->S2);
+    cudaFreeHost(h->hS2);
+    cudaFree(h->forcing_f);
     cudaFree(h->metric_block);
     cudaFree(h->partials);
     cudaFree(h->ticket);
@@ -393,7 +473,7 @@ extern "C" int dcm_bicgstab(dcm_handle* h, double* x, double* b, const double* s
             for (int i = 1; i <= d.ip; i++)
                 for (int j = 1; j <= d.jp; j++)
                     for (int k = 1; k <= d.kp; k++)
-                        b[d.at(k, j, i)] =
+                        b[h->hd.at(k, j, i)] =
                             std::exp(-1.0 / 5.e6 *
                                      (h->h_xg[i] * h->h_xg[i] + h->h_yg[j] * h->h_yg[j] +
                                       std::pow(h->h_zg[k] - 4000.0, 2.0)));
@@ -448,8 +528,9 @@ extern "C" int dcm_sources(dcm_handle* h, const dcm_forcing* forcing, const doub
     RC(upload(h, STH, sth)); RC(upload(h, RHS, rhs));
     RC(upload(h, BARS, ubar, K2)); RC(upload(h, BARS + K2, vbar, K2));
     RC(upload(h, BARS + 2 * K2, wbar, K2)); RC(upload(h, BARS + 3 * K2, thbar, K2));
-    launch_sources<double>(d, h->mt, F, BARS, BARS + K2, BARS + 2 * K2, BARS + 3 * K2, ZU, ZV, ZW,
-                           U, V, W, TH, SU, SV, SWd, STH, RHS, 0, 0, h->st);
+    launch_sources<double, double>(d, h->mt, h->mt, F, BARS, BARS + K2, BARS + 2 * K2,
+                                   BARS + 3 * K2, ZU, ZV, ZW, U, V, W, TH, SU, SV, SWd, STH, RHS,
+                                   0, 0, h->st);
     CK(cudaGetLastError());
     RC(download(h, su, SU)); RC(download(h, sv, SV)); RC(download(h, sw, SWd));
     RC(download(h, sth, STH)); RC(download(h, rhs, RHS));
@@ -512,10 +593,10 @@ static int mpdata_dropin(dcm_handle* h, double dt, const double* u, const double
     MpBufs mb;
     if (!mpdata_work(h, nq, mb)) return fail(h, DCM_E_CUDA, "device allocation failed");
     RC(upload(h, U, u)); RC(upload(h, V, v)); RC(upload(h, W, w));
-    for (int q = 0; q < nq; q++) RC(upload(h, pin[q], psi + (size_t)q * h->n));
+    for (int q = 0; q < nq; q++) RC(upload(h, pin[q], psi + (size_t)q * h->nh));
     RC(mpdata_run<double>(mb.w, h->d, h->mt, dt, U, V, W, pin.data(), pout.data(), nq, lbc, ubc,
                           kord, monotone, neumann, limiter, vec, nullptr, 0.0, h->st));
-    for (int q = 0; q < nq; q++) RC(download(h, psi + (size_t)q * h->n, pout[q]));
+    for (int q = 0; q < nq; q++) RC(download(h, psi + (size_t)q * h->nh, pout[q]));
     CK(cudaMemcpyAsync(h->hM, h->M, nq * sizeof(MpScalars), cudaMemcpyDeviceToHost, h->st));
     RC(sync(h));
     for (int q = 0; q < nq; q++) {  // :711-713 / :1748-1752
@@ -603,8 +684,8 @@ extern "C" int dcm_horizontal_means(dcm_handle* h, int moisture, int nq, const d
     NEED(OUT);
     if ((4 + (size_t)nqq) * K2 > h->n) return fail(h, DCM_E_ARG, "horizontal_means: too many q");
     RC(upload(h, U, u)); RC(upload(h, V, v)); RC(upload(h, W, w)); RC(upload(h, TH, th));
-    for (int c = 0; c < nqq; c++) RC(upload(h, Q[c], q + (size_t)c * h->n));
-    launch_means_div<double>(h->d, h->mt, U, V, W, TH, Q.data(), nqq, OUT, nullptr, h->partials,
+    for (int c = 0; c < nqq; c++) RC(upload(h, Q[c], q + (size_t)c * h->nh));
+    launch_means_div<double, double>(h->d, h->mt, U, V, W, TH, Q.data(), nqq, OUT, nullptr, h->partials,
                              h->ticket, h->st);
     CK(cudaGetLastError());
     RC(download(h, ubar, OUT, K2)); RC(download(h, vbar, OUT + K2, K2));
@@ -621,7 +702,7 @@ extern "C" int dcm_divergence_calc(dcm_handle* h, const double* u, const double*
            *OUT = slot(h, S_PSI_OUT);
     NEED(U); NEED(V); NEED(W); NEED(DV); NEED(OUT);
     RC(upload(h, U, u)); RC(upload(h, V, v)); RC(upload(h, W, w)); RC(upload(h, DV, div));
-    launch_means_div<double>(h->d, h->mt, U, V, W, W, nullptr, 0, OUT, DV, h->partials,
+    launch_means_div<double, double>(h->d, h->mt, U, V, W, W, nullptr, 0, OUT, DV, h->partials,
                              h->ticket, h->st);
     CK(cudaGetLastError());
     RC(download(h, div, DV));
@@ -641,9 +722,9 @@ extern "C" int dcm_advance_scalar_fields_3d(dcm_handle* h, double dt, double* q,
     RC(download(h, th, A));
     if (moisture) {
         for (int c = 0; c < nq; c++) {
-            RC(upload(h, A, q + (size_t)c * h->n)); RC(upload(h, S, sq + (size_t)c * h->n));
+            RC(upload(h, A, q + (size_t)c * h->nh)); RC(upload(h, S, sq + (size_t)c * h->nh));
             launch_advance_scalar<double>(h->d, dt, A, S, h->st);
-            RC(download(h, q + (size_t)c * h->n, A));
+            RC(download(h, q + (size_t)c * h->nh, A));
         }
     }
     CK(cudaGetLastError());
@@ -676,12 +757,15 @@ extern "C" int dcm_exchange_along_dim_wo(dcm_handle* h, double* a) {
 // =============================================================================
 namespace {
 
-double* alloc_owned(dcm_handle* h) {
-    double* p = nullptr;
-    if (cudaMalloc(&p, h->n * sizeof(double)) != cudaSuccess) return nullptr;
-    cudaMemsetAsync(p, 0, h->n * sizeof(double), h->st);
-    h->owned.push_back(p);
-    return p;
+// n = 0: a pitched field; n > 0: n contiguous elements
+template <typename T>
+T* alloc_owned(dcm_handle* h, size_t n = 0) {
+    T* raw = nullptr;
+    const size_t cnt = n ? n : h->n + FIELD_PAD;
+    if (cudaMalloc(&raw, cnt * sizeof(T)) != cudaSuccess) return nullptr;
+    cudaMemsetAsync(raw, 0, cnt * sizeof(T), h->st);
+    h->owned.push_back(raw);
+    return n ? raw : raw + FIELD_SHIFT;
 }
 
 // velocity roles after n steps: (u, zu, tu) -> buffers (0,1,2), (2,0,1),
@@ -694,73 +778,187 @@ void roles(const dcm_handle* h, int& cu, int& cz, int& ct) {
     ct = RT[m];
 }
 
-__global__ void k_driver_start(Dims d, double* zu, double* zv, double* zw) {
+template <typename T>
+__global__ void k_driver_start(Dims d, T* zu, T* zv, T* zw) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = blockIdx.y;
     if (j > d.jp + 1) return;
     zw[d.at(0, j, i)] = -zw[d.at(1, j, i)];  // driver_code.f90:288
-    zu[d.at(1, j, i)] = 0.0;
-    zv[d.at(1, j, i)] = 0.0;
+    zu[d.at(1, j, i)] = T(0);
+    zv[d.at(1, j, i)] = T(0);
     zw[d.at(d.kp, j, i)] = -zw[d.at(d.kp - 1, j, i)];  // :292-294
-    zw[d.at(d.kp + 1, j, i)] = 0.0;
-    zu[d.at(d.kp, j, i)] = 0.0;
-    zv[d.at(d.kp, j, i)] = 0.0;
+    zw[d.at(d.kp + 1, j, i)] = T(0);
+    zu[d.at(d.kp, j, i)] = T(0);
+    zv[d.at(d.kp, j, i)] = T(0);
 }
 
-int one_step(dcm_handle* h) {
-    const Dims& d = h->d;
+template <typename T>
+State<T>& state_of(dcm_handle* h);
+template <>
+State<double>& state_of<double>(dcm_handle* h) { return h->s64; }
+template <>
+State<float>& state_of<float>(dcm_handle* h) { return h->s32; }
+
+template <typename T>
+const Metrics<T>& metrics_of(dcm_handle* h);
+template <>
+const Metrics<double>& metrics_of<double>(dcm_handle* h) { return h->mt; }
+template <>
+const Metrics<float>& metrics_of<float>(dcm_handle* h) { return h->mtf; }
+
+// MPDATA scratch in the field precision (slots for FP64, fslots for FP32)
+template <typename T>
+struct MpBufsT {
+    MpdataWork<T> w;
+    std::vector<T*> pa, pb;
+};
+
+template <typename T>
+T* tslot(dcm_handle* h, int idx);
+template <>
+double* tslot<double>(dcm_handle* h, int idx) { return slot(h, idx); }
+template <>
+float* tslot<float>(dcm_handle* h, int idx) { return fslot(h, idx); }
+
+template <typename T>
+bool mpdata_work_t(dcm_handle* h, int nq, MpBufsT<T>& b) {
+    b.pa.resize(nq);
+    b.pb.resize(nq);
+    for (int q = 0; q < nq; q++) {
+        b.pa[q] = tslot<T>(h, S_DYN + 4 * q + 2);
+        b.pb[q] = tslot<T>(h, S_DYN + 4 * q + 3);
+        if (!b.pa[q] || !b.pb[q]) return false;
+    }
+    b.w.pa = b.pa.data();
+    b.w.pb = b.pb.data();
+    const int va[3] = {S_VA0, S_VA1, S_VA2}, vl[3] = {S_VL0, S_VL1, S_VL2};
+    for (int c = 0; c < 3; c++) {
+        b.w.va[c] = tslot<T>(h, va[c]);
+        b.w.vl[c] = tslot<T>(h, vl[c]);
+        if (!b.w.va[c] || !b.w.vl[c]) return false;
+    }
+    const int bt[6] = {S_B0, S_B1, S_B2, S_B3, S_B4, S_B5};
+    for (int c = 0; c < 6; c++) {
+        b.w.beta[c] = tslot<T>(h, bt[c]);
+        if (!b.w.beta[c]) return false;
+    }
+    b.w.partials = h->partials;
+    b.w.ticket = h->ticket;
+    b.w.M = h->M;
+    b.w.Mone = h->M + NQMAX;
+    b.w.Mzero = h->M + NQMAX + 1;
+    return true;
+}
+
+SolverWork<float> solver_work_f(dcm_handle* h) {
+    SolverWork<float> w;
+    w.r = fslot(h, S_R); w.cr = fslot(h, S_CR); w.p = fslot(h, S_PP); w.v1 = fslot(h, S_V1);
+    w.t = fslot(h, S_T); w.sA = fslot(h, S_SA); w.sB = fslot(h, S_SB);
+    w.rh = fslot(h, S_RH); w.vh = fslot(h, S_VH);
+    w.ae = h->aef; w.aw = h->awf; w.an = h->anf; w.as = h->asf; w.au = h->auf; w.ad = h->adf;
+    w.partials = h->partials; w.ticket = h->ticket; w.S = h->S2;
+    w.red.partials = h->partials; w.red.gpartials = h->gpartials; w.red.gtick = h->gtick;
+    w.red.ticket = h->ticket2;
+    return w;
+}
+
+template <typename T>
+Forcing<T> forcing_t(dcm_handle* h);
+template <>
+Forcing<double> forcing_t<double>(dcm_handle* h) {
+    const size_t K2 = h->d.kp + 2;
+    Forcing<double> F{};
     const dcm_config& c = h->cfg;
-    const size_t K2 = d.kp + 2;
-    int cu, cz, ct;
-    roles(h, cu, cz, ct);
-    double *u = h->U[cu], *v = h->V[cu], *w = h->W[cu];
-    double *zu = h->U[cz], *zv = h->V[cz], *zw = h->W[cz];
-    double *tu = h->U[ct], *tv = h->V[ct], *tw = h->W[ct];
-    const int nqq = c.moisture ? c.nq : 0;
-    // horizontal_means + divergence_calc, driver_code.f90:433-444
-    launch_means_div<double>(d, h->mt, u, v, w, h->th, h->q.data(), nqq, h->means, h->div,
-                             h->partials, h->ticket, h->st);
-    // sources (sth = 0 first, :340) + exchange_along_dim_wo(psrc), :455-487
-    int rc = DCM_OK;
-    Forcing<double> F = forcing_of(h, nullptr, h->forcing_dev, &rc);
     F.damping_layer = c.forcing.damping_layer;
     F.forcing = c.forcing.forcing;
     F.divergence = c.forcing.divergence;
     F.forcing_tau = c.forcing.forcing_tau;
-    F.dampfacn = h->forcing_dev; F.dampfac = h->forcing_dev + K2;
-    F.u_force = h->forcing_dev + 2 * K2; F.v_force = h->forcing_dev + 3 * K2;
-    F.w_subs = h->forcing_dev + 4 * K2;
-    const double* ubar = h->means;
-    launch_sources<double>(d, h->mt, F, ubar, ubar + K2, ubar + 2 * K2, ubar + 3 * K2, zu, zv, zw,
-                           u, v, w, h->th, h->su, h->sv, h->sw, h->sth, h->psrc, 1, 1, h->st);
+    double* f = h->forcing_dev;
+    F.dampfacn = f; F.dampfac = f + K2; F.u_force = f + 2 * K2; F.v_force = f + 3 * K2;
+    F.w_subs = f + 4 * K2;
+    return F;
+}
+template <>
+Forcing<float> forcing_t<float>(dcm_handle* h) {
+    const size_t K2 = h->d.kp + 2;
+    Forcing<float> F{};
+    const dcm_config& c = h->cfg;
+    F.damping_layer = c.forcing.damping_layer;
+    F.forcing = c.forcing.forcing;
+    F.divergence = c.forcing.divergence;
+    F.forcing_tau = (float)c.forcing.forcing_tau;
+    float* f = h->forcing_f;
+    F.dampfacn = f; F.dampfac = f + K2; F.u_force = f + 2 * K2; F.v_force = f + 3 * K2;
+    F.w_subs = f + 4 * K2;
+    return F;
+}
+
+// one pass of the time loop (driver_code.f90:304-676) with fields in T and
+// the pressure in FP64
+template <typename T>
+int one_step(dcm_handle* h) {
+    const Dims& d = h->d;
+    const dcm_config& c = h->cfg;
+    State<T>& S = state_of<T>(h);
+    const Metrics<T>& mt = metrics_of<T>(h);
+    const size_t K2 = d.kp + 2;
+    int cu, cz, ct;
+    roles(h, cu, cz, ct);
+    T *u = S.U[cu], *v = S.V[cu], *w = S.W[cu];
+    T *zu = S.U[cz], *zv = S.V[cz], *zw = S.W[cz];
+    T *tu = S.U[ct], *tv = S.V[ct], *tw = S.W[ct];
+    const int nqq = c.moisture ? c.nq : 0;
+    const T dt = (T)c.dt;
+    // horizontal_means + divergence_calc (FP64 divergence), driver_code.f90:433-444
+    launch_means_div<T, double>(d, h->mt, u, v, w, S.th, S.q.data(), nqq, S.means, h->div,
+                                h->partials, h->ticket, h->st);
+    // sources (sth = 0 first, :340) + exchange_along_dim_wo(psrc), :455-487
+    const Forcing<T> F = forcing_t<T>(h);
+    const T* ubar = S.means;
+    launch_sources<T, double>(d, mt, h->mt, F, ubar, ubar + K2, ubar + 2 * K2, ubar + 3 * K2, zu,
+                              zv, zw, u, v, w, S.th, S.su, S.sv, S.sw, S.sth, h->psrc, 1, 1,
+                              h->st);
     CK(cudaGetLastError());
-    // bicgstab + exchange_along_dim_wo(p), :496-507
-    SolverWork<double> sw = solver_work(h);
-    NEED(sw.r); NEED(sw.sB); NEED(sw.rh); NEED(sw.vh);
+    // pressure: bicgstab + exchange_along_dim_wo(p), :496-507
+    SolverWork<double> swd = solver_work(h);
+    NEED(swd.r); NEED(swd.sB); NEED(swd.rh); NEED(swd.vh);
     h->first_call = 0;
-    const int st = solver_run<double>(sw, d, h->p, h->psrc, h->sw, h->mt.dzn, c.ptol, c.itmax, 1,
-                                      4, h->st, h->hS, nullptr);
-    h->last_iters = h->hS->it;
-    h->last_err = h->hS->err;
+    int st;
+    if constexpr (std::is_same<T, double>::value) {
+        st = solver_run<double>(swd, d, h->p, h->psrc, S.sw, h->mt.dzn, c.ptol, c.itmax, 1, 4,
+                                h->st, h->hS, nullptr);
+        h->last_iters = h->hS->it;
+        h->last_err = h->hS->err;
+    } else {
+        SolverWork<float> swf = solver_work_f(h);
+        NEED(swf.r); NEED(swf.sB); NEED(swf.rh); NEED(swf.vh);
+        float* dx = fslot(h, S_B);
+        NEED(dx);
+        st = refine_run(swf, swd, d, h->p, h->psrc, S.sw, h->mt.dzn, dx, c.ptol,
+                        c.inner_tol > 0 ? c.inner_tol : 0.1, c.itmax, 1000, h->st, h->hS,
+                        h->hS2, &h->last_refine);
+        h->last_iters = h->last_refine.inner;
+        h->last_err = h->last_refine.err;
+        h->refine_outer_total += h->last_refine.outer;
+    }
     if (st != DCM_OK) {
         h->err = dcm_status_string(st);
         return st;
     }
     // scalar advection, :514-560, with advance_scalar_fields_3d (:601) fused
-    MpBufs mb;
-    if (!mpdata_work(h, std::max(1, nqq), mb)) return fail(h, DCM_E_CUDA, "device allocation");
-    if (c.advection_scheme == 0 || c.advection_scheme == 1) {
-        launch_adv_ref_state<double>(d, h->mt, c.dt, w, h->th, h->th2, h->mt.thetan, 1, h->st);
-    }
+    MpBufsT<T> mb;
+    if (!mpdata_work_t<T>(h, std::max(1, nqq), mb))
+        return fail(h, DCM_E_CUDA, "device allocation");
+    if (c.advection_scheme == 0 || c.advection_scheme == 1)
+        launch_adv_ref_state<T>(d, mt, dt, w, S.th, S.th2, mt.thetan, 1, h->st);
     if (c.advection_scheme == 1) {
         double lb = h->t1, ub = h->t2;
-        double* pin = h->th2;
-        double* pout = h->th;
-        const double* sadd = h->sth;
-        RC(mpdata_run<double>(mb.w, d, h->mt, c.dt, u, v, w, &pin, &pout, 1, &lb, &ub, c.kord,
-                              c.monotone, 0, c.limiter, false, &sadd, c.dt, h->st));
-        // t1, t2 return unshifted: (t - m) + m; kept on the host.  (0 - m) + m == 0
-        // exactly, so the values only change when they start non-zero.
+        T* pin = S.th2;
+        T* pout = S.th;
+        const T* sadd = S.sth;
+        RC(mpdata_run<T>(mb.w, d, mt, dt, u, v, w, &pin, &pout, 1, &lb, &ub, c.kord, c.monotone,
+                         0, c.limiter, false, &sadd, dt, h->st));
+        // t1, t2 return as (t - m) + m, which is exactly t when t = 0
         if (h->t1 != 0.0 || h->t2 != 0.0) {
             CK(cudaMemcpyAsync(h->hM, h->M, sizeof(MpScalars), cudaMemcpyDeviceToHost, h->st));
             RC(sync(h));
@@ -769,22 +967,21 @@ int one_step(dcm_handle* h) {
         }
     } else if (c.advection_scheme == 0) {
         // donor cell + exchange_full(th, t1, t2), :539-545, then th += sth*dt
-        CK(cudaMemcpyAsync(h->th, h->th2, h->n * sizeof(double), cudaMemcpyDeviceToDevice,
-                           h->st));
-        RC(upwind_run<double>(mb.w, d, h->mt, c.dt, u, v, w, h->th2, h->th, 0, h->st));
-        launch_exchange<double>(d, h->th, HALO_FULL, h->t1, h->t2, h->st);
-        launch_advance_scalar<double>(d, c.dt, h->th, h->sth, h->st);
+        CK(cudaMemcpyAsync(S.th, S.th2, h->n * sizeof(T), cudaMemcpyDeviceToDevice, h->st));
+        RC(upwind_run<T>(mb.w, d, mt, dt, u, v, w, S.th2, S.th, 0, h->st));
+        launch_exchange<T>(d, S.th, HALO_FULL, (T)h->t1, (T)h->t2, h->st);
+        launch_advance_scalar<T>(d, dt, S.th, S.sth, h->st);
     } else if (c.advection_scheme == 2) {
         // mpdata_3d_add with thetan, thbase, thtop, :552-556
         double lb = c.thbase, ub = c.thtop;
-        launch_add_profile<double>(d, h->th, h->mt.thetan, 1.0, h->st);
-        double* pin = h->th;
-        double* pout = h->th2;
-        RC(mpdata_run<double>(mb.w, d, h->mt, c.dt, u, v, w, &pin, &pout, 1, &lb, &ub, c.kord,
-                              c.monotone, 0, c.limiter, false, nullptr, 0.0, h->st));
-        launch_add_profile<double>(d, h->th2, h->mt.thetan, -1.0, h->st);
-        launch_advance_scalar<double>(d, c.dt, h->th2, h->sth, h->st);
-        std::swap(h->th, h->th2);
+        launch_add_profile<T>(d, S.th, mt.thetan, T(1), h->st);
+        T* pin = S.th;
+        T* pout = S.th2;
+        RC(mpdata_run<T>(mb.w, d, mt, dt, u, v, w, &pin, &pout, 1, &lb, &ub, c.kord, c.monotone,
+                         0, c.limiter, false, nullptr, T(0), h->st));
+        launch_add_profile<T>(d, S.th2, mt.thetan, T(-1), h->st);
+        launch_advance_scalar<T>(d, dt, S.th2, S.sth, h->st);
+        std::swap(S.th, S.th2);
     } else {
         return fail(h, DCM_E_UNSUPPORTED, "advection_scheme");
     }
@@ -793,26 +990,137 @@ int one_step(dcm_handle* h) {
         for (int cat = 0; cat < c.ncat; cat++) {
             const int a = h->cs[cat] - 1, b = h->ce[cat] - 1;
             const int nc = b - a + 1;
-            std::vector<double*> qin(nc), qout(nc);
-            std::vector<const double*> sadd(nc);
+            std::vector<T*> qin(nc), qout(nc);
+            std::vector<const T*> sadd(nc);
             for (int e = 0; e < nc; e++) {
-                CK(cudaMemcpyAsync(h->qtmp[a + e], h->q[a + e], h->n * sizeof(double),
-                                   cudaMemcpyDeviceToDevice, h->st));
-                qin[e] = h->qtmp[a + e];
-                qout[e] = h->q[a + e];
-                sadd[e] = h->sq[a + e];
+                // the current q becomes the read-only input; the result goes
+                // to the other buffer of the pair (no copy)
+                std::swap(S.q[a + e], S.qtmp[a + e]);
+                qin[e] = S.qtmp[a + e];
+                qout[e] = S.q[a + e];
+                sadd[e] = S.sq[a + e];
             }
-            RC(mpdata_run<double>(mb.w, d, h->mt, c.dt, u, v, w, qin.data(), qout.data(), nc,
-                                  h->q1.data() + a, h->q2.data() + a, c.kord, c.monotone, 0,
-                                  c.limiter, true, sadd.data(), c.dt, h->st));
+            RC(mpdata_run<T>(mb.w, d, mt, dt, u, v, w, qin.data(), qout.data(), nc,
+                             h->q1.data() + a, h->q2.data() + a, c.kord, c.monotone, 0, c.limiter,
+                             true, sadd.data(), dt, h->st));
         }
     }
     // advance_momentum(2dt) + time filter + rotation + exchange + rows, :592-674
-    launch_momentum_step<double>(d, h->mt, 2.0 * c.dt, u, v, w, zu, zv, zw, tu, tv, tw, h->su,
-                                 h->sv, h->sw, h->p, h->st);
+    launch_momentum_step<T, double>(d, mt, h->mt, (T)(2.0 * c.dt), u, v, w, zu, zv, zw, tu, tv,
+                                    tw, S.su, S.sv, S.sw, h->p, h->st);
     CK(cudaGetLastError());
     h->nstep += 1;
     return DCM_OK;
+}
+
+// host double field -> device field of precision T (via an FP64 staging slot)
+template <typename T>
+int put_field(dcm_handle* h, T* dst, const double* src) {
+    if (!src) return DCM_OK;
+    if constexpr (std::is_same<T, double>::value) return upload(h, dst, src);
+    double* stage = slot(h, S_STAGE);
+    NEED(stage);
+    RC(upload(h, stage, src));
+    launch_convert<T, double>(h->n, dst, stage, h->st);
+    return DCM_OK;
+}
+template <typename T>
+int get_field(dcm_handle* h, double* dst, const T* src, size_t n = 0) {
+    if (!dst) return DCM_OK;
+    if constexpr (std::is_same<T, double>::value) return download(h, dst, src, n);
+    double* stage = slot(h, S_STAGE);
+    NEED(stage);
+    launch_convert<double, T>(n ? n : h->n, stage, src, h->st);
+    RC(download(h, dst, stage, n));
+    RC(sync(h));  // the staging slot is reused by the next field
+    return DCM_OK;
+}
+
+template <typename T>
+int upload_state_t(dcm_handle* h, const dcm_fields* f) {
+    State<T>& S = state_of<T>(h);
+    const dcm_config& cfg = h->cfg;
+    const int nqq = cfg.moisture ? cfg.nq : 0;
+    const double* in3[9] = {f->u, f->zu, f->tu, f->v, f->zv, f->tv, f->w, f->zw, f->tw};
+    T** dst3[9] = {&S.U[0], &S.U[1], &S.U[2], &S.V[0], &S.V[1],
+                   &S.V[2], &S.W[0], &S.W[1], &S.W[2]};
+    for (int c = 0; c < 9; c++) {
+        if (!in3[c]) return fail(h, DCM_E_ARG, "state_upload: missing velocity");
+        *dst3[c] = alloc_owned<T>(h);
+        NEED(*dst3[c]);
+        RC(put_field<T>(h, *dst3[c], in3[c]));
+        RC(sync(h));
+    }
+    T** fl[6] = {&S.th, &S.th2, &S.su, &S.sv, &S.sw, &S.sth};
+    for (auto pp : fl) {
+        *pp = alloc_owned<T>(h);
+        NEED(*pp);
+    }
+    if (!f->th || !f->p) return fail(h, DCM_E_ARG, "state_upload: missing th or p");
+    const double* src[5] = {f->th, f->su, f->sv, f->sw, f->sth};
+    T* dst[5] = {S.th, S.su, S.sv, S.sw, S.sth};
+    for (int c = 0; c < 5; c++) {
+        RC(put_field<T>(h, dst[c], src[c]));
+        RC(sync(h));
+    }
+    const size_t K2 = h->d.kp + 2;
+    S.means = alloc_owned<T>(h, (4 + nqq) * K2);
+    NEED(S.means);
+    for (int c = 0; c < nqq; c++) {
+        T* a = alloc_owned<T>(h);
+        T* sq = alloc_owned<T>(h);
+        T* t = alloc_owned<T>(h);
+        NEED(a); NEED(sq); NEED(t);
+        RC(put_field<T>(h, a, f->q + (size_t)c * h->nh));
+        RC(sync(h));
+        // sq is zeroed by the driver each step (:342) and nothing in the dry
+        // step writes it, so it stays zero
+        S.q.push_back(a);
+        S.sq.push_back(sq);
+        S.qtmp.push_back(t);
+    }
+    if constexpr (std::is_same<T, float>::value) {
+        launch_convert<float, double>(5 * K2, h->forcing_f, h->forcing_dev, h->st);
+    }
+    return DCM_OK;
+}
+
+template <typename T>
+int download_state_t(dcm_handle* h, dcm_fields* f) {
+    State<T>& S = state_of<T>(h);
+    int cu, cz, ct;
+    roles(h, cu, cz, ct);
+    RC(get_field<T>(h, f->u, S.U[cu])); RC(get_field<T>(h, f->v, S.V[cu]));
+    RC(get_field<T>(h, f->w, S.W[cu]));
+    RC(get_field<T>(h, f->zu, S.U[cz])); RC(get_field<T>(h, f->zv, S.V[cz]));
+    RC(get_field<T>(h, f->zw, S.W[cz]));
+    RC(get_field<T>(h, f->tu, S.U[ct])); RC(get_field<T>(h, f->tv, S.V[ct]));
+    RC(get_field<T>(h, f->tw, S.W[ct]));
+    RC(get_field<T>(h, f->th, S.th));
+    RC(download(h, f->p, h->p));
+    RC(get_field<T>(h, f->su, S.su)); RC(get_field<T>(h, f->sv, S.sv));
+    RC(get_field<T>(h, f->sw, S.sw));
+    RC(download(h, f->psrc, h->psrc));
+    RC(download(h, f->div, h->div));
+    RC(get_field<T>(h, f->sth, S.sth));
+    const size_t K2 = h->d.kp + 2;
+    RC(get_field<T>(h, f->ubar, S.means, K2));
+    RC(get_field<T>(h, f->vbar, S.means + K2, K2));
+    RC(get_field<T>(h, f->wbar, S.means + 2 * K2, K2));
+    RC(get_field<T>(h, f->thbar, S.means + 3 * K2, K2));
+    const int nqq = h->cfg.moisture ? h->cfg.nq : 0;
+    if (nqq && f->qbar) {
+        if constexpr (std::is_same<T, double>::value) {
+            RC(download(h, f->qbar, S.means + 4 * K2, nqq * K2));
+        } else {
+            RC(get_field<T>(h, f->qbar, S.means + 4 * K2, nqq * K2));
+        }
+    }
+    for (int c = 0; c < nqq; c++) {
+        if (f->q) RC(get_field<T>(h, f->q + (size_t)c * h->nh, S.q[c]));
+        if (f->sq) RC(get_field<T>(h, f->sq + (size_t)c * h->nh, S.sq[c]));
+    }
+    return sync(h);
 }
 
 }  // namespace
@@ -820,14 +1128,16 @@ int one_step(dcm_handle* h) {
 extern "C" int dcm_state_upload(dcm_handle* h, const dcm_config* cfg, const dcm_fields* f) {
     CHECK_H();
     if (!cfg || !f) return fail(h, DCM_E_ARG, "state_upload: bad argument");
-    if (cfg->precision != 0) return fail(h, DCM_E_UNSUPPORTED, "precision");
+    if (cfg->precision != 0 && cfg->precision != 1)
+        return fail(h, DCM_E_UNSUPPORTED, "precision must be 0 (FP64) or 1 (mixed)");
     if (cfg->advection_scheme < 0 || cfg->advection_scheme > 2 || cfg->itmax < 1 || cfg->dt <= 0)
         return fail(h, DCM_E_ARG, "state_upload: bad config");
     if (cfg->moisture && (cfg->nq < 1 || cfg->nq > NQMAX || cfg->ncat < 1 || !cfg->c_s ||
-                          !cfg->c_e || !f->q || !f->sq))
+                          !cfg->c_e || !f->q))
         return fail(h, DCM_E_ARG, "state_upload: bad moisture config");
     free_state(h);
     h->cfg = *cfg;
+    h->prec = cfg->precision;
     const int nqq = cfg->moisture ? cfg->nq : 0;
     if (nqq) {
         h->cs.assign(cfg->c_s, cfg->c_s + cfg->ncat);
@@ -838,47 +1148,22 @@ extern "C" int dcm_state_upload(dcm_handle* h, const dcm_config* cfg, const dcm_
         h->cfg.c_s = h->cs.data();
         h->cfg.c_e = h->ce.data();
     }
-    double* in3[9] = {f->u, f->zu, f->tu, f->v, f->zv, f->tv, f->w, f->zw, f->tw};
-    double** dst3[9] = {&h->U[0], &h->U[1], &h->U[2], &h->V[0], &h->V[1],
-                        &h->V[2], &h->W[0], &h->W[1], &h->W[2]};
-    for (int c = 0; c < 9; c++) {
-        *dst3[c] = alloc_owned(h);
-        NEED(*dst3[c]);
-        if (!in3[c]) return fail(h, DCM_E_ARG, "state_upload: missing velocity");
-        RC(upload(h, *dst3[c], in3[c]));
-    }
-    h->nstep = 0;
-    double** fl[9] = {&h->th, &h->th2, &h->p, &h->su, &h->sv, &h->sw, &h->psrc, &h->div, &h->sth};
-    for (auto pp : fl) {
-        *pp = alloc_owned(h);
-        NEED(*pp);
-    }
-    if (!f->th || !f->p) return fail(h, DCM_E_ARG, "state_upload: missing th or p");
-    RC(upload(h, h->th, f->th)); RC(upload(h, h->p, f->p));
-    RC(upload(h, h->su, f->su)); RC(upload(h, h->sv, f->sv)); RC(upload(h, h->sw, f->sw));
-    RC(upload(h, h->psrc, f->psrc)); RC(upload(h, h->div, f->div)); RC(upload(h, h->sth, f->sth));
-    const size_t K2 = h->d.kp + 2;
-    CK(cudaMalloc(&h->means, (4 + nqq) * K2 * sizeof(double)));
-    h->owned.push_back(h->means);
-    CK(cudaMemsetAsync(h->means, 0, (4 + nqq) * K2 * sizeof(double), h->st));
-    for (int c = 0; c < nqq; c++) {
-        double* a = alloc_owned(h);
-        double* s = alloc_owned(h);
-        double* t = alloc_owned(h);
-        NEED(a); NEED(s); NEED(t);
-        RC(upload(h, a, f->q + (size_t)c * h->n));
-        RC(upload(h, s, f->sq + (size_t)c * h->n));
-        h->q.push_back(a);
-        h->sq.push_back(s);
-        h->qtmp.push_back(t);
-    }
-    h->q1.assign(nqq, 0.0);  // driver_code.f90:275-276
-    h->q2.assign(nqq, 0.0);
-    h->t1 = h->t2 = 0.0;  // saved locals, :260
-    // forcing profiles
     int rc = DCM_OK;
     forcing_of(h, &cfg->forcing, h->forcing_dev, &rc);
     if (rc != DCM_OK) return fail(h, rc, "state_upload: forcing arrays");
+    h->nstep = 0;
+    h->p = alloc_owned<double>(h);
+    h->div = alloc_owned<double>(h);
+    h->psrc = alloc_owned<double>(h);
+    NEED(h->p); NEED(h->div); NEED(h->psrc);
+    RC(upload(h, h->p, f->p));
+    RC(upload(h, h->div, f->div));
+    RC(upload(h, h->psrc, f->psrc));
+    RC(h->prec == 0 ? upload_state_t<double>(h, f) : upload_state_t<float>(h, f));
+    h->q1.assign(nqq, 0.0);  // driver_code.f90:275-276
+    h->q2.assign(nqq, 0.0);
+    h->t1 = h->t2 = 0.0;  // saved locals, :260
+    h->refine_outer_total = 0;
     h->resident = true;
     return sync(h);
 }
@@ -889,7 +1174,12 @@ extern "C" int dcm_driver_start(dcm_handle* h) {
     int cu, cz, ct;
     roles(h, cu, cz, ct);
     const dim3 g((h->d.J + 127) / 128, h->d.I);
-    k_driver_start<<<g, 128, 0, h->st>>>(h->d, h->U[cz], h->V[cz], h->W[cz]);
+    if (h->prec == 0)
+        k_driver_start<double><<<g, 128, 0, h->st>>>(h->d, h->s64.U[cz], h->s64.V[cz],
+                                                     h->s64.W[cz]);
+    else
+        k_driver_start<float><<<g, 128, 0, h->st>>>(h->d, h->s32.U[cz], h->s32.V[cz],
+                                                    h->s32.W[cz]);
     CK(cudaGetLastError());
     return sync(h);
 }
@@ -903,7 +1193,7 @@ extern "C" int dcm_step(dcm_handle* h, int nsteps, dcm_step_stats* stats) {
     int done = 0;
     int rc = DCM_OK;
     for (; done < nsteps; done++) {
-        rc = one_step(h);
+        rc = h->prec == 0 ? one_step<double>(h) : one_step<float>(h);
         tot += h->last_iters;
         if (rc != DCM_OK) break;
     }
@@ -926,29 +1216,7 @@ extern "C" int dcm_step(dcm_handle* h, int nsteps, dcm_step_stats* stats) {
 extern "C" int dcm_state_download(dcm_handle* h, dcm_fields* f) {
     CHECK_H();
     if (!h->resident || !f) return fail(h, DCM_E_ARG, "state_download: no state");
-    int cu, cz, ct;
-    roles(h, cu, cz, ct);
-    RC(download(h, f->u, h->U[cu])); RC(download(h, f->v, h->V[cu]));
-    RC(download(h, f->w, h->W[cu]));
-    RC(download(h, f->zu, h->U[cz])); RC(download(h, f->zv, h->V[cz]));
-    RC(download(h, f->zw, h->W[cz]));
-    RC(download(h, f->tu, h->U[ct])); RC(download(h, f->tv, h->V[ct]));
-    RC(download(h, f->tw, h->W[ct]));
-    RC(download(h, f->th, h->th)); RC(download(h, f->p, h->p));
-    RC(download(h, f->su, h->su)); RC(download(h, f->sv, h->sv)); RC(download(h, f->sw, h->sw));
-    RC(download(h, f->psrc, h->psrc)); RC(download(h, f->div, h->div));
-    RC(download(h, f->sth, h->sth));
-    const size_t K2 = h->d.kp + 2;
-    RC(download(h, f->ubar, h->means, K2)); RC(download(h, f->vbar, h->means + K2, K2));
-    RC(download(h, f->wbar, h->means + 2 * K2, K2));
-    RC(download(h, f->thbar, h->means + 3 * K2, K2));
-    const int nqq = h->cfg.moisture ? h->cfg.nq : 0;
-    if (nqq && f->qbar) RC(download(h, f->qbar, h->means + 4 * K2, nqq * K2));
-    for (int c = 0; c < nqq; c++) {
-        if (f->q) RC(download(h, f->q + (size_t)c * h->n, h->q[c]));
-        if (f->sq) RC(download(h, f->sq + (size_t)c * h->n, h->sq[c]));
-    }
-    return sync(h);
+    return h->prec == 0 ? download_state_t<double>(h, f) : download_state_t<float>(h, f);
 }
 
 // =============================================================================

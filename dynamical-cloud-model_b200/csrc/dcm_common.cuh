@@ -36,10 +36,28 @@ struct Dims {
     }
 };
 
+// Dense Fortran layout a(0:kp+1, 0:jp+1, 0:ip+1): the layout of host arrays
+// and of device arrays a caller owns.
 inline Dims make_dims(int ip, int jp, int kp) {
     Dims d;
     d.ip = ip; d.jp = jp; d.kp = kp;
     d.K = kp + 2; d.J = jp + 2; d.I = ip + 2;
+    return d;
+}
+
+// Pitched device layout of the fields a handle owns.  The leading (k)
+// dimension is padded to K = round_up(kp + 4, 8) and every field pointer
+// sits FIELD_SHIFT elements past a 256-byte aligned allocation, so element
+// (1, j, i) of every column starts on a 32-byte boundary (64 bytes for
+// double).  Stencil kernels then move 16-byte vectors of consecutive
+// k-levels; a vector that starts at k <= kp ends at k <= kp + 3 < K, inside
+// its own column.  A field takes n() + FIELD_PAD elements.
+constexpr int FIELD_ALIGN = 8;
+constexpr int FIELD_SHIFT = FIELD_ALIGN - 1;
+constexpr int FIELD_PAD = FIELD_ALIGN;
+inline Dims make_dims_pitched(int ip, int jp, int kp) {
+    Dims d = make_dims(ip, jp, kp);
+    d.K = (kp + 4 + FIELD_ALIGN - 1) / FIELD_ALIGN * FIELD_ALIGN;
     return d;
 }
 
@@ -132,7 +150,7 @@ inline dim3 interior_grid(const Dims& d, int k_extent) {
     return dim3((k_extent + BX - 1) / BX, (d.jp + BY - 1) / BY, d.ip);
 }
 inline dim3 full_grid(const Dims& d) {
-    return dim3((d.K + BX - 1) / BX, (d.J + BY - 1) / BY, d.I);
+    return dim3((d.kp + 2 + BX - 1) / BX, (d.J + BY - 1) / BY, d.I);
 }
 
 // ---- deterministic reductions -------------------------------------------

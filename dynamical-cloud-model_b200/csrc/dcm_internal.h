@@ -14,6 +14,11 @@ namespace dcm {
 struct SolverScalars {
     double sc_err, err, rho, alf, omg, bet, nrm, tt, ts;
     int it, done, status, early;
+    // reliable updates of the mixed-precision solve: pause the FP32
+    // iteration when its residual has fallen by `delta` since the last FP64
+    // residual (ru_norm) or below the tolerance
+    double ru_norm, delta;
+    int ru, pause, updates, pad;
 };
 
 template <typename T>
@@ -51,7 +56,21 @@ struct MpdataWork {
 template <typename T>
 int solver_run(SolverWork<T>& w, const Dims& d, T* x, const T* b, const T* sw,
                const T* dzn, double tol, int itmax, int wo, int chunk,
-               cudaStream_t st, SolverScalars* host_S, int* launched_iters);
+               cudaStream_t st, SolverScalars* host_S, int* launched_iters,
+               double sc_floor = 0.01, bool post = true);
+
+struct RefineStats {
+    int outer, inner;
+    double err;
+};
+
+// mixed-precision pressure solve: FP32 BiCGSTAB with FP64 reliable updates
+// of the residual; x is the FP64 pressure, dx FP32 scratch
+int refine_run(SolverWork<float>& wf, SolverWork<double>& wd, const Dims& d,
+               double* x, const double* b, const float* sw, const double* dzn,
+               float* dx, double tol, double delta, int itmax, int max_updates,
+               cudaStream_t st, SolverScalars* hS_out, SolverScalars* hS_in,
+               RefineStats* rs);
 
 template <typename T>
 int mpdata_run(MpdataWork<T>& w, const Dims& d, const Metrics<T>& mt, T dt,
@@ -84,20 +103,21 @@ constexpr int MEAN_GY = 128;
 
 // means of u,v,w,th (+ nq q fields) per level k = 0..kp+1 and, when div is
 // non-null, the divergence of rho*u (diagnostics.f90:31-153)
-template <typename T>
-void launch_means_div(const Dims& d, const Metrics<T>& mt, const T* u,
+template <typename T, typename D>
+void launch_means_div(const Dims& d, const Metrics<D>& mt, const T* u,
                       const T* v, const T* w, const T* th, T* const* q, int nq,
-                      T* means /* (4+nq)*(kp+2) */, T* div, double* partials,
+                      T* means /* (4+nq)*(kp+2) */, D* div, double* partials,
                       unsigned int* ticket, cudaStream_t st);
 
 // sources (dynamics.f90:639-998); sth_reset applies the driver's sth = 0
 // first; rhs_wo applies the driver's exchange_along_dim_wo(psrc)
-template <typename T>
-void launch_sources(const Dims& d, const Metrics<T>& mt, const Forcing<T>& f,
-                    const T* ubar, const T* vbar, const T* wbar, const T* thbar,
-                    const T* zu, const T* zv, const T* zw, const T* u,
-                    const T* v, const T* w, const T* th, T* su, T* sv, T* sw,
-                    T* sth, T* rhs, int sth_reset, int rhs_wo, cudaStream_t st);
+template <typename T, typename R>
+void launch_sources(const Dims& d, const Metrics<T>& mt, const Metrics<R>& mtr,
+                    const Forcing<T>& f, const T* ubar, const T* vbar,
+                    const T* wbar, const T* thbar, const T* zu, const T* zv,
+                    const T* zw, const T* u, const T* v, const T* w,
+                    const T* th, T* su, T* sv, T* sw, T* sth, R* rhs,
+                    int sth_reset, int rhs_wo, cudaStream_t st);
 
 template <typename T>
 void launch_advance_momentum(const Dims& d, const Metrics<T>& mt, T dt, T* u,
@@ -108,11 +128,12 @@ void launch_advance_momentum(const Dims& d, const Metrics<T>& mt, T dt, T* u,
 // resident step: advance_momentum(2dt) into tu, time filter of u in place,
 // then the exchange + boundary rows of the rotated velocities
 // (driver_code.f90:592-674)
-template <typename T>
-void launch_momentum_step(const Dims& d, const Metrics<T>& mt, T dt2, T* u,
-                          T* v, T* w, const T* zu, const T* zv, const T* zw,
-                          T* tu, T* tv, T* tw, const T* su, const T* sv,
-                          const T* sw, const T* p, cudaStream_t st);
+template <typename T, typename P>
+void launch_momentum_step(const Dims& d, const Metrics<T>& mt,
+                          const Metrics<P>& mtp, T dt2, T* u, T* v, T* w,
+                          const T* zu, const T* zv, const T* zw, T* tu, T* tv,
+                          T* tw, const T* su, const T* sv, const T* sw,
+                          const P* p, cudaStream_t st);
 
 // adv_ref_state (+ optional exchange_full(0,0)) from psi into out
 template <typename T>
@@ -123,6 +144,10 @@ void launch_adv_ref_state(const Dims& d, const Metrics<T>& mt, T dt,
 template <typename T>
 void launch_advance_scalar(const Dims& d, T dt, T* a, const T* s,
                            cudaStream_t st);
+
+// element-wise precision conversion of n values
+template <typename TO, typename FROM>
+void launch_convert(size_t n, TO* to, const FROM* from, cudaStream_t st);
 
 // psi (+/-) psi_1d(k) over the whole array (mpdata_3d_add :175-188)
 template <typename T>

@@ -64,7 +64,7 @@ extern "C" int dcm_horizontal_means_noalloc(int ip, int jp, int kp, const double
     // it set, so clear it on the caller's stream before the kernel
     if (cudaMemsetAsync(ticket, 0, sizeof(unsigned int), st) != cudaSuccess) return DCM_E_CUDA;
     dcm::Metrics<double> none{};  // the divergence is not formed here
-    dcm::launch_means_div<double>(d, none, u, v, w, th, nullptr, 0, means, nullptr, partials,
+    dcm::launch_means_div<double, double>(d, none, u, v, w, th, nullptr, 0, means, nullptr, partials,
                                   ticket, st);
     return cudaGetLastError() == cudaSuccess ? DCM_OK : DCM_E_CUDA;
 }

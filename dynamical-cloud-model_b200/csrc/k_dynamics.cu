@@ -39,10 +39,10 @@ void launch_exchange(const Dims& d, T* a, int mode, T lbc, T ubc, cudaStream_t s
 // set of (j,i) columns; per-(field, k) partials reduced in a fixed order by
 // the last block.  means layout: [field][k], k = 0..kp+1.
 
-template <typename T, int NF>
-__global__ void __launch_bounds__(256) k_means(Dims d, Metrics<T> mt, const T* f0, const T* f1,
+template <typename T, int NF, typename D>
+__global__ void __launch_bounds__(256) k_means(Dims d, Metrics<D> mt, const T* f0, const T* f1,
                                                const T* f2, const T* f3, T* __restrict__ means,
-                                               T* __restrict__ div, double* partials,
+                                               D* __restrict__ div, double* partials,
                                                unsigned int* ticket) {
     __shared__ double red[NF][BY][BX];
     const int k = blockIdx.x * BX + threadIdx.x;
@@ -59,13 +59,14 @@ __global__ void __launch_bounds__(256) k_means(Dims d, Metrics<T> mt, const T* f
             for (int q = 0; q < NF; q++) acc[q] += (double)f[q][o];
             if (div && k >= 1 && k <= d.kp) {
                 // divergence_calc, diagnostics.f90:144-146
+                // in D (FP64 for the mixed-precision form: the divergence check)
                 const T* u = f0;
                 const T* v = f1;
                 const T* w = f2;
-                const T rn = ld(mt.rhoan + k);
-                div[o] = rn * (u[o] - u[d.at(k, j, i - 1)]) / ld(mt.dx + i - 1) +
-                         rn * (v[o] - v[d.at(k, j - 1, i)]) / ld(mt.dy + j - 1) +
-                         (ld(mt.rhoa + k) * w[o] - ld(mt.rhoa + k - 1) * w[d.at(k - 1, j, i)]) /
+                const D rn = ld(mt.rhoan + k);
+                div[o] = rn * ((D)u[o] - (D)u[d.at(k, j, i - 1)]) / ld(mt.dx + i - 1) +
+                         rn * ((D)v[o] - (D)v[d.at(k, j - 1, i)]) / ld(mt.dy + j - 1) +
+                         (ld(mt.rhoa + k) * (D)w[o] - ld(mt.rhoa + k - 1) * (D)w[d.at(k - 1, j, i)]) /
                              ld(mt.dz + k - 1);
             }
         }
@@ -104,36 +105,36 @@ __global__ void __launch_bounds__(256) k_means(Dims d, Metrics<T> mt, const T* f
     if (tid == 0) *ticket = 0u;
 }
 
-template <typename T>
-void launch_means_div(const Dims& d, const Metrics<T>& mt, const T* u, const T* v, const T* w,
-                      const T* th, T* const* q, int nq, T* means, T* div, double* partials,
+template <typename T, typename D>
+void launch_means_div(const Dims& d, const Metrics<D>& mt, const T* u, const T* v, const T* w,
+                      const T* th, T* const* q, int nq, T* means, D* div, double* partials,
                       unsigned int* ticket, cudaStream_t st) {
     const int K2 = d.kp + 2;
     const dim3 g((K2 + BX - 1) / BX, MEAN_GY), b(BX, BY);
     { ProfScope ps_(P_MEANS, st);
-    k_means<T, 4><<<g, b, 0, st>>>(d, mt, u, v, w, th, means, div, partials, ticket);
+    k_means<T, 4, D><<<g, b, 0, st>>>(d, mt, u, v, w, th, means, div, partials, ticket);
     }
     for (int q0 = 0; q0 < nq; q0 += 4) {
         const int n = nq - q0 < 4 ? nq - q0 : 4;
         T* out = means + (size_t)(4 + q0) * K2;
         if (n == 4)
             { ProfScope ps_(P_MEANS, st);
-            k_means<T, 4><<<g, b, 0, st>>>(d, mt, q[q0], q[q0 + 1], q[q0 + 2], q[q0 + 3], out,
+            k_means<T, 4, D><<<g, b, 0, st>>>(d, mt, q[q0], q[q0 + 1], q[q0 + 2], q[q0 + 3], out,
                                            nullptr, partials, ticket);
             }
         else if (n == 3)
             { ProfScope ps_(P_MEANS, st);
-            k_means<T, 3><<<g, b, 0, st>>>(d, mt, q[q0], q[q0 + 1], q[q0 + 2], nullptr, out,
+            k_means<T, 3, D><<<g, b, 0, st>>>(d, mt, q[q0], q[q0 + 1], q[q0 + 2], nullptr, out,
                                            nullptr, partials, ticket);
             }
         else if (n == 2)
             { ProfScope ps_(P_MEANS, st);
-            k_means<T, 2><<<g, b, 0, st>>>(d, mt, q[q0], q[q0 + 1], nullptr, nullptr, out,
+            k_means<T, 2, D><<<g, b, 0, st>>>(d, mt, q[q0], q[q0 + 1], nullptr, nullptr, out,
                                            nullptr, partials, ticket);
             }
         else
             { ProfScope ps_(P_MEANS, st);
-            k_means<T, 1><<<g, b, 0, st>>>(d, mt, q[q0], nullptr, nullptr, nullptr, out,
+            k_means<T, 1, D><<<g, b, 0, st>>>(d, mt, q[q0], nullptr, nullptr, nullptr, out,
                                            nullptr, partials, ticket);
             }
     }
@@ -245,25 +246,28 @@ __global__ void __launch_bounds__(256) k_sources(Dims d, Metrics<T> mt, Forcing<
 
 // rhs of the Poisson equation, dynamics.f90:977-998 (k = 0..kp+1); with wo
 // also the driver's exchange_along_dim_wo(psrc), driver_code.f90:485-487
-template <typename T>
-__global__ void __launch_bounds__(256) k_rhs(Dims d, Metrics<T> mt, const T* __restrict__ su,
+template <typename T, typename R>
+__global__ void __launch_bounds__(256) k_rhs(Dims d, Metrics<R> mt, const T* __restrict__ su,
                                              const T* __restrict__ sv,
-                                             const T* __restrict__ sw, T* __restrict__ rhs,
+                                             const T* __restrict__ sw, R* __restrict__ rhs,
                                              int wo) {
     const int k = blockIdx.x * BX + threadIdx.x;  // 0..kp+1
     const int j = 1 + blockIdx.y * BY + threadIdx.y;
     const int i = 1 + blockIdx.z;
     if (k > d.kp + 1 || j > d.jp) return;
     const int o = d.at(k, j, i);
-    T r;
+    // in R: FP64 in the mixed-precision form, so that the right-hand side of
+    // the singular (periodic / Neumann) Poisson problem sums to zero to FP64
+    // round-off and the FP64-refined solve stays consistent
+    R r;
     if (k >= 1) {
-        r = ((su[o] - su[d.at(k, j, i - 1)]) / ld(mt.dx + i - 1) +
-             (sv[o] - sv[d.at(k, j - 1, i)]) / ld(mt.dy + j - 1) +
-             (sw[o] - sw[d.at(k - 1, j, i)]) / ld(mt.dz + k - 1));
+        r = (((R)su[o] - (R)su[d.at(k, j, i - 1)]) / ld(mt.dx + i - 1) +
+             ((R)sv[o] - (R)sv[d.at(k, j - 1, i)]) / ld(mt.dy + j - 1) +
+             ((R)sw[o] - (R)sw[d.at(k - 1, j, i)]) / ld(mt.dz + k - 1));
     } else {
-        r = ((su[o] - su[d.at(0, j, i - 1)]) / ld(mt.dx + i - 1) +
-             (sv[o] - sv[d.at(0, j - 1, i)]) / ld(mt.dy + j - 1) +
-             (sw[o] + sw[d.at(1, j, i)]) / ld(mt.dz + 1));
+        r = (((R)su[o] - (R)su[d.at(0, j, i - 1)]) / ld(mt.dx + i - 1) +
+             ((R)sv[o] - (R)sv[d.at(0, j - 1, i)]) / ld(mt.dy + j - 1) +
+             ((R)sw[o] + (R)sw[d.at(1, j, i)]) / ld(mt.dz + 1));
     }
     if (wo && k >= 1 && k <= d.kp)
         put_wo(rhs, d, k, j, i, r);
@@ -271,11 +275,12 @@ __global__ void __launch_bounds__(256) k_rhs(Dims d, Metrics<T> mt, const T* __r
         rhs[o] = r;
 }
 
-template <typename T>
-void launch_sources(const Dims& d, const Metrics<T>& mt, const Forcing<T>& f, const T* ubar,
-                    const T* vbar, const T* wbar, const T* thbar, const T* zu, const T* zv,
-                    const T* zw, const T* u, const T* v, const T* w, const T* th, T* su, T* sv,
-                    T* sw, T* sth, T* rhs, int sth_reset, int rhs_wo, cudaStream_t st) {
+template <typename T, typename R>
+void launch_sources(const Dims& d, const Metrics<T>& mt, const Metrics<R>& mtr,
+                    const Forcing<T>& f, const T* ubar, const T* vbar, const T* wbar,
+                    const T* thbar, const T* zu, const T* zv, const T* zw, const T* u, const T* v,
+                    const T* w, const T* th, T* su, T* sv, T* sw, T* sth, R* rhs, int sth_reset,
+                    int rhs_wo, cudaStream_t st) {
     const dim3 b(BX, BY);
     { ProfScope ps_(P_SOURCES, st);
     k_sources<T><<<interior_grid(d, d.kp), b, 0, st>>>(d, mt, f, ubar, vbar, wbar, thbar, zu, zv,
@@ -283,7 +288,7 @@ void launch_sources(const Dims& d, const Metrics<T>& mt, const Forcing<T>& f, co
                                                        sth_reset);
     }
     { ProfScope ps_(P_RHS, st);
-    k_rhs<T><<<interior_grid(d, d.kp + 2), b, 0, st>>>(d, mt, su, sv, sw, rhs, rhs_wo);
+    k_rhs<T, R><<<interior_grid(d, d.kp + 2), b, 0, st>>>(d, mtr, su, sv, sw, rhs, rhs_wo);
     }
 }
 
@@ -331,8 +336,8 @@ void launch_advance_momentum(const Dims& d, const Metrics<T>& mt, T dt, T* u, T*
 // the exchange_full(0,0) images of the rotated u (:656-661) and the rows of
 // :663-674: u(0) = -u(1), v(0) = -v(1), w(0) = 0, u(kp+1) = u(kp),
 // v(kp+1) = v(kp), w(kp+1) = 0.
-template <typename T>
-__global__ void __launch_bounds__(256) k_momentum_step(Dims d, Metrics<T> mt, T dt2,
+template <typename T, typename P>
+__global__ void __launch_bounds__(256) k_momentum_step(Dims d, Metrics<T> mt, Metrics<P> mtp, T dt2,
                                                        T* __restrict__ u, T* __restrict__ v,
                                                        T* __restrict__ w,
                                                        const T* __restrict__ zu,
@@ -343,7 +348,7 @@ __global__ void __launch_bounds__(256) k_momentum_step(Dims d, Metrics<T> mt, T 
                                                        const T* __restrict__ su,
                                                        const T* __restrict__ sv,
                                                        const T* __restrict__ sw,
-                                                       const T* __restrict__ p) {
+                                                       const P* __restrict__ p) {
     const int k = blockIdx.x * BX + threadIdx.x;  // 0..kp+1
     const int j = blockIdx.y * BY + threadIdx.y;  // 0..jp+1
     const int i = blockIdx.z;                     // 0..ip+1
@@ -355,13 +360,15 @@ __global__ void __launch_bounds__(256) k_momentum_step(Dims d, Metrics<T> mt, T 
     v[o] = c99 * v[o] + c01 * zvo;
     w[o] = c99 * w[o] + c01 * zwo;
     if (k < 1 || k > d.kp || j < 1 || j > d.jp || i < 1 || i > d.ip) return;
-    const T pc = p[o];
-    const T nu = zuo + ((su[o] - (p[d.at(k, j, i + 1)] - pc) / (ld(mt.dxn + i))) * dt2) /
-                           ld(mt.rhoan + k);
-    const T nv = zvo + ((sv[o] - (p[d.at(k, j + 1, i)] - pc) / (ld(mt.dyn + j))) * dt2) /
-                           ld(mt.rhoan + k);
-    const T nw = zwo + ((sw[o] - (p[d.at(k + 1, j, i)] - pc) / (ld(mt.dzn + k))) * dt2) /
-                           ld(mt.rhoa + k);
+    // pressure gradient in P (FP64 in the mixed-precision form, where p is
+    // the refined FP64 solution), the rest in T
+    const P pc = p[o];
+    const T gx = (T)((p[d.at(k, j, i + 1)] - pc) / (ld(mtp.dxn + i)));
+    const T gy = (T)((p[d.at(k, j + 1, i)] - pc) / (ld(mtp.dyn + j)));
+    const T gz = (T)((p[d.at(k + 1, j, i)] - pc) / (ld(mtp.dzn + k)));
+    const T nu = zuo + ((su[o] - gx) * dt2) / ld(mt.rhoan + k);
+    const T nv = zvo + ((sv[o] - gy) * dt2) / ld(mt.rhoan + k);
+    const T nw = zwo + ((sw[o] - gz) * dt2) / ld(mt.rhoa + k);
     put_plane_images(tu, d, k, j, i, nu);
     put_plane_images(tv, d, k, j, i, nv);
     put_plane_images(tw, d, k, j, i, nw);
@@ -377,13 +384,15 @@ __global__ void __launch_bounds__(256) k_momentum_step(Dims d, Metrics<T> mt, T 
     }
 }
 
-template <typename T>
-void launch_momentum_step(const Dims& d, const Metrics<T>& mt, T dt2, T* u, T* v, T* w,
-                          const T* zu, const T* zv, const T* zw, T* tu, T* tv, T* tw,
-                          const T* su, const T* sv, const T* sw, const T* p, cudaStream_t st) {
+template <typename T, typename P>
+void launch_momentum_step(const Dims& d, const Metrics<T>& mt, const Metrics<P>& mtp, T dt2,
+                          T* u, T* v, T* w, const T* zu, const T* zv, const T* zw, T* tu, T* tv,
+                          T* tw, const T* su, const T* sv, const T* sw, const P* p,
+                          cudaStream_t st) {
     { ProfScope ps_(P_MOMENTUM, st);
-    k_momentum_step<T><<<full_grid(d), dim3(BX, BY), 0, st>>>(d, mt, dt2, u, v, w, zu, zv, zw,
-                                                              tu, tv, tw, su, sv, sw, p);
+    k_momentum_step<T, P><<<full_grid(d), dim3(BX, BY), 0, st>>>(d, mt, mtp, dt2, u, v, w, zu,
+                                                                 zv, zw, tu, tv, tw, su, sv, sw,
+                                                                 p);
     }
 }
 
@@ -445,6 +454,7 @@ __global__ void k_add_profile(Dims d, T* __restrict__ a, const T* __restrict__ p
     const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= n) return;
     const int k = (int)(e % d.K);
+    if (k > d.kp + 1) return;  // column padding of the pitched layout
     a[e] = sign > T(0) ? a[e] + prof[k] : a[e] - prof[k];
 }
 
@@ -456,26 +466,44 @@ void launch_add_profile(const Dims& d, T* a, const T* prof, T sign, cudaStream_t
     }
 }
 
-#define INST(T)                                                                                 \
+#define INST(T, D)                                                                              \
     template void launch_exchange<T>(const Dims&, T*, int, T, T, cudaStream_t);                 \
-    template void launch_means_div<T>(const Dims&, const Metrics<T>&, const T*, const T*,       \
-                                      const T*, const T*, T* const*, int, T*, T*, double*,      \
-                                      unsigned int*, cudaStream_t);                             \
-    template void launch_sources<T>(const Dims&, const Metrics<T>&, const Forcing<T>&,          \
-                                    const T*, const T*, const T*, const T*, const T*,           \
-                                    const T*, const T*, const T*, const T*, const T*,           \
-                                    const T*, T*, T*, T*, T*, T*, int, int, cudaStream_t);      \
+    template void launch_means_div<T, D>(const Dims&, const Metrics<D>&, const T*, const T*,    \
+                                         const T*, const T*, T* const*, int, T*, D*, double*,   \
+                                         unsigned int*, cudaStream_t);                          \
+    template void launch_sources<T, D>(const Dims&, const Metrics<T>&, const Metrics<D>&,       \
+                                       const Forcing<T>&, const T*, const T*, const T*,         \
+                                       const T*, const T*, const T*, const T*, const T*,        \
+                                       const T*, const T*, const T*, T*, T*, T*, T*, D*, int,   \
+                                       int, cudaStream_t);                                      \
     template void launch_advance_momentum<T>(const Dims&, const Metrics<T>&, T, T*, T*, T*,     \
                                              const T*, const T*, const T*, const T*,            \
                                              const T*, const T*, const T*, cudaStream_t);       \
-    template void launch_momentum_step<T>(const Dims&, const Metrics<T>&, T, T*, T*, T*,        \
-                                          const T*, const T*, const T*, T*, T*, T*, const T*,   \
-                                          const T*, const T*, const T*, cudaStream_t);          \
+    template void launch_momentum_step<T, D>(const Dims&, const Metrics<T>&, const Metrics<D>&, \
+                                             T, T*, T*, T*, const T*, const T*, const T*, T*,   \
+                                             T*, T*, const T*, const T*, const T*, const D*,    \
+                                             cudaStream_t);                                     \
     template void launch_adv_ref_state<T>(const Dims&, const Metrics<T>&, T, const T*,          \
                                           const T*, T*, const T*, int, cudaStream_t);           \
     template void launch_advance_scalar<T>(const Dims&, T, T*, const T*, cudaStream_t);         \
     template void launch_add_profile<T>(const Dims&, T*, const T*, T, cudaStream_t);
 
-INST(double)
+INST(double, double)
+INST(float, double)
+
+// ---- precision conversion of whole arrays ------------------------------------
+template <typename TO, typename FROM>
+__global__ void k_convert(size_t n, TO* __restrict__ to, const FROM* __restrict__ from) {
+    const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < n) to[e] = (TO)from[e];
+}
+
+template <typename TO, typename FROM>
+void launch_convert(size_t n, TO* to, const FROM* from, cudaStream_t st) {
+    if (!n) return;
+    k_convert<TO, FROM><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, to, from);
+}
+template void launch_convert<float, double>(size_t, float*, const double*, cudaStream_t);
+template void launch_convert<double, float>(size_t, double*, const float*, cudaStream_t);
 
 }  // namespace dcm

@@ -535,6 +535,13 @@ template int mpdata_run<double>(MpdataWork<double>&, const Dims&, const Metrics<
                                 const double*, const double*, const double*, double* const*,
                                 double* const*, int, const double*, const double*, int, int, int,
                                 int, bool, const double* const*, double, cudaStream_t);
+template int mpdata_run<float>(MpdataWork<float>&, const Dims&, const Metrics<float>&, float,
+                               const float*, const float*, const float*, float* const*,
+                               float* const*, int, const double*, const double*, int, int, int,
+                               int, bool, const float* const*, float, cudaStream_t);
+template int upwind_run<float>(MpdataWork<float>&, const Dims&, const Metrics<float>&, float,
+                               const float*, const float*, const float*, const float*, float*,
+                               int, cudaStream_t);
 template int upwind_run<double>(MpdataWork<double>&, const Dims&, const Metrics<double>&, double,
                                 const double*, const double*, const double*, const double*,
                                 double*, int, cudaStream_t);

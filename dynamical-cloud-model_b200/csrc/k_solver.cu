@@ -35,6 +35,9 @@
 // a_p once.  The result agrees with the reference's order of operations to a
 // few ulp per sweep, far below the 1e-10 parity bar.  The iteration then
 // moves 41 field passes instead of 39.
+#include <cstdio>
+#include <cstdlib>
+
 #include "dcm_internal.h"
 #include "dcm_prof.h"
 
@@ -51,9 +54,8 @@ struct SolverArgs {
     Dims d;
     int itmax;
     double tol;
-    int ich;       // i-planes per tile
-    int nkt, njt;  // tiles in k, j
-    int ntiles;
+    double sc_floor;  // max(||b||, sc_floor) scales the residual (0.01, :371)
+    int nkt;          // k-chunks of a warp task
 };
 
 // a_p exactly as set_mat_a forms it (dynamics.f90:93-95)
@@ -104,116 +106,251 @@ struct StenCtx {
     bool first;
 };
 
-// one warp task: 32 consecutive k-levels (k0 = 1 + 32 kt) of column (j, i)
-template <typename T, int OP, int MODE, int NV>
-__device__ __forceinline__ void sten_task(const StenCtx<T, OP, MODE>& C, int kt, int j, int i,
-                                          double (&acc)[NV]) {
-    const Dims& d = C.d;
-    const int lane = threadIdx.x & 31;
-    const int ip = d.ip, jp = d.jp, kp = d.kp;
-    const int k = 1 + kt * BX + lane;
-    const bool valid = k <= kp;
-    auto X = [&](int kk, int jj, int ii) -> T {
-        const int o = d.at(kk, jj, ii);
-        if (OP == OP_SW1) return s0val<T, MODE>(C.rh, C.vh, o, C.bet, C.omg, C.alf, C.first);
-        return C.gx[o];
-    };
-    const int km = min(k, kp);
-    const T xc = X(km, j, i);
-    T xd = __shfl_up_sync(0xffffffffu, xc, 1);
-    T xu = __shfl_down_sync(0xffffffffu, xc, 1);
-    if (lane == 0) xd = X(max(km - 1, 1), j, i);
-    if (lane == BX - 1) xu = X(min(km + 1, kp), j, i);
-    if (!valid) return;
-    const Coef<T>& c = C.c;
-    const T xm = X(k, j, i == 1 ? ip : i - 1), xp = X(k, j, i == ip ? 1 : i + 1);
-    const T xs = X(k, j == 1 ? jp : j - 1, i), xn = X(k, j == jp ? 1 : j + 1, i);
-    const T ae = ld(c.ae + i), aw = ld(c.aw + i), an = ld(c.an + j), as = ld(c.as + j),
-            au = ld(c.au + k), ad = ld(c.ad + k);
-    const T ap = -ae - aw - an - as - au - ad;
-    // mat_ax, dynamics.f90:219-222 (a_c = 0)
-    const T Ax = aw * xm + ae * xp + as * xs + an * xn + ad * xd + au * xu + ap * xc + T(0);
-    const int o = d.at(k, j, i);
-    const SolverBufs& B = C.B;
-    T* __restrict__ out = (T*)B.out;
-    if (OP == OP_SETUP) {
-        const T bv = ((const T*)B.b)[o];
-        const T rv = bv - Ax;  // :377
-        out[o] = rv;
-        ((T*)B.out2)[o] = rv;
-        ((T*)B.out3)[o] = rv / ap;
-        acc[0] += (double)bv * (double)bv;
-        acc[NV - 1] += (double)rv * (double)rv;
-    } else if (OP == OP_MATP) {
-        out[o] = Ax;
-        ((T*)B.out3)[o] = Ax / ap;
-        acc[0] += (double)((const T*)B.cr)[o] * (double)Ax;
-    } else if (OP == OP_MATC) {
-        out[o] = Ax;
-        const T sv = ((const T*)B.r)[o] - C.alf * ((const T*)B.v1)[o];  // s of :404
-        acc[0] += (double)Ax * (double)Ax;
-        acc[NV - 1] += (double)Ax * (double)sv;
+// Warp-task iterator of the persistent kernels: task t = kt + nkt*(jr +
+// njr*(i-1)), visited at start, start+stride, ...; the stride is split into
+// its (kt, jr, i) parts once so that each step is a carry chain, not a divide.
+struct TaskIter {
+    int kt, jr, i;
+    int dkt, djr, di, nkt, njr;
+    __device__ __forceinline__ TaskIter(unsigned start, unsigned stride, int nkt_, int njr_)
+        : nkt(nkt_), njr(njr_) {
+        kt = (int)(start % (unsigned)nkt);
+        const unsigned q = start / (unsigned)nkt;
+        jr = (int)(q % (unsigned)njr);
+        i = 1 + (int)(q / (unsigned)njr);
+        dkt = (int)(stride % (unsigned)nkt);
+        const unsigned sq = stride / (unsigned)nkt;
+        djr = (int)(sq % (unsigned)njr);
+        di = (int)(sq / (unsigned)njr);
+    }
+    __device__ __forceinline__ void next() {
+        kt += dkt;
+        const int c1 = kt >= nkt;
+        kt -= c1 ? nkt : 0;
+        jr += djr + c1;
+        const int c2 = jr >= njr;
+        jr -= c2 ? njr : 0;
+        i += di + c2;
+    }
+};
+
+// 16-byte vectors of consecutive k-levels: the pitched layout puts k = 1 of
+// every column on a 32-byte boundary, so the vector starting at
+// k0 = 1 + V m is aligned.
+template <typename T>
+struct KVec;
+template <>
+struct KVec<float> {
+    static constexpr int V = 4;
+    using type = float4;
+};
+template <>
+struct KVec<double> {
+    static constexpr int V = 2;
+    using type = double2;
+};
+
+template <typename T>
+__device__ __forceinline__ void vld(const T* p, T (&v)[KVec<T>::V]) {
+    using VT = typename KVec<T>::type;
+    const VT a = __ldg(reinterpret_cast<const VT*>(p));
+    if constexpr (KVec<T>::V == 4) {
+        v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
     } else {
-        // precondition, dynamics.f90:260-264:
-        //   s_new = s + (q - A s)/a_p = s + q/a_p - (A s)/a_p
-        const T s0c =
-            OP == OP_SW1 ? xc : s0val<T, MODE>(C.rh, C.vh, o, C.bet, C.omg, C.alf, C.first);
-        const T sn = xc + s0c - Ax / ap;
-        if (OP == OP_SW3P)
-            out[o] = C.first ? sn + C.bet * T(0) : sn + C.bet * out[o];  // :397
-        else
-            out[o] = sn;
+        v[0] = a.x; v[1] = a.y;
+    }
+}
+// coherent load, for an array the kernel also writes
+template <typename T>
+__device__ __forceinline__ void vld_rw(const T* p, T (&v)[KVec<T>::V]) {
+    using VT = typename KVec<T>::type;
+    const VT a = *reinterpret_cast<const VT*>(p);
+    if constexpr (KVec<T>::V == 4) {
+        v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+    } else {
+        v[0] = a.x; v[1] = a.y;
+    }
+}
+// store the levels k0 + c <= kp (a whole vector when all are)
+template <typename T>
+__device__ __forceinline__ void vst(T* p, const T (&v)[KVec<T>::V], int nvalid) {
+    using VT = typename KVec<T>::type;
+    constexpr int V = KVec<T>::V;
+    if (nvalid >= V) {
+        VT a;
+        if constexpr (V == 4) {
+            a.x = v[0]; a.y = v[1]; a.z = v[2]; a.w = v[3];
+        } else {
+            a.x = v[0]; a.y = v[1];
+        }
+        *reinterpret_cast<VT*>(p) = a;
+    } else {
+#pragma unroll
+        for (int c = 0; c < V; c++)
+            if (c < nvalid) p[c] = v[c];
     }
 }
 
-// Sweeps (no reduction): one warp task per warp, grid (k-chunks, j/8, i).
-// Reducing kernels: persistent blocks, each warp strides over the warp tasks
-// and the block publishes one partial.
+// X values of a vector: the operand field, or for the first sweep s0 = q/a_p
+// formed from rh and vh
 template <typename T, int OP, int MODE>
-__global__ void __launch_bounds__(256) k_sten(SolverArgs a, Coef<T> c, SolverBufs B, Red2 R,
-                                              SolverScalars* S) {
-    constexpr int NV = (OP == OP_SETUP || OP == OP_MATC) ? 2 : 1;
-    constexpr bool RED = OP == OP_SETUP || OP == OP_MATC || OP == OP_MATP;
-    __shared__ double smem[64];
-    if (OP != OP_SETUP && S->done) return;
-    StenCtx<T, OP, MODE> C;
-    C.d = a.d;
-    C.c = c;
-    C.gx = (const T*)(OP == OP_SETUP ? B.x : B.sin);
-    C.rh = (const T*)B.rh;
-    C.vh = (const T*)B.vh;
-    C.B = B;
-    C.bet = (T)S->bet;
-    C.omg = (T)S->omg;
-    C.alf = (T)S->alf;
-    C.first = S->it == 0;
-    const Dims& d = a.d;
-    double acc[NV];
+__device__ __forceinline__ void xload(const StenCtx<T, OP, MODE>& C, int o,
+                                      T (&x)[KVec<T>::V]) {
+    constexpr int V = KVec<T>::V;
+    if (OP == OP_SW1) {
+        T a[V], b[V];
+        vld(C.rh + o, a);
+        if (MODE == 0 && C.first) {
 #pragma unroll
-    for (int q = 0; q < NV; q++) acc[q] = 0.0;
-    if (!RED) {
-        const int j = 1 + blockIdx.y * BY + threadIdx.y;
-        if (j <= d.jp) sten_task<T, OP, MODE, NV>(C, blockIdx.x, j, 1 + blockIdx.z, acc);
-        return;
+            for (int c = 0; c < V; c++) x[c] = a[c] - C.bet * (C.omg * T(0));
+            return;
+        }
+        vld(C.vh + o, b);
+#pragma unroll
+        for (int c = 0; c < V; c++)
+            x[c] = MODE == 0 ? a[c] - C.bet * (C.omg * b[c]) : a[c] - C.alf * b[c];
+    } else {
+        vld(C.gx + o, x);
     }
-    const int nkt = a.nkt;
-    const long long ntask = (long long)nkt * d.jp * d.ip;
-    const int warps = blockDim.y;
-    for (long long t = (long long)blockIdx.x * warps + threadIdx.y; t < ntask;
-         t += (long long)gridDim.x * warps) {
-        const int kt = (int)(t % nkt);
-        const long long r2 = t / nkt;
-        const int j = 1 + (int)(r2 % d.jp);
-        const int i = 1 + (int)(r2 / d.jp);
-        sten_task<T, OP, MODE, NV>(C, kt, j, i, acc);
+}
+template <typename T, int OP, int MODE>
+__device__ __forceinline__ T xload1(const StenCtx<T, OP, MODE>& C, int o) {
+    if (OP == OP_SW1) return s0val<T, MODE>(C.rh, C.vh, o, C.bet, C.omg, C.alf, C.first);
+    return C.gx[o];
+}
+
+// One warp task: V x 32 consecutive k-levels (lane l holds k0 = 1 +
+// V (32 kc + l) .. k0 + V - 1) of row j, plane i.  k neighbours are the
+// adjacent vector elements, the neighbour lanes' end elements by shuffle, and
+// at the warp's two ends one scalar load each; Neumann mirror at k = 1, kp
+// (dynamics.f90:206-211).  j and i neighbours (periodic) are vector loads of
+// the adjacent columns.
+template <typename T, int OP, int MODE, int NV>
+__device__ __forceinline__ void sten_task(const StenCtx<T, OP, MODE>& C, int kc, int j, int i,
+                                          double (&acc)[NV]) {
+    constexpr int V = KVec<T>::V;
+    const Dims& d = C.d;
+    const int lane = threadIdx.x & 31;
+    const int ip = d.ip, jp = d.jp, kp = d.kp;
+    const int k0 = 1 + V * (kc * BX + lane);
+    const bool live = k0 <= kp;
+    const int nvalid = live ? min(V, kp - k0 + 1) : 0;
+    const int K = d.K, KJ = d.K * d.J;
+    const int o = (live ? k0 : 1) + K * j + KJ * i;  // idle lanes read column start
+    const int os = o + (j == 1 ? jp - 1 : -1) * K, on = o + (j == jp ? 1 - jp : 1) * K;
+    const int ow = o + (i == 1 ? ip - 1 : -1) * KJ, oe = o + (i == ip ? 1 - ip : 1) * KJ;
+    T xc[V], xs[V], xn[V], xw[V], xe[V];
+    xload(C, o, xc);
+    xload(C, os, xs);
+    xload(C, on, xn);
+    xload(C, ow, xw);
+    xload(C, oe, xe);
+    T prev = __shfl_up_sync(0xffffffffu, xc[V - 1], 1);
+    T next = __shfl_down_sync(0xffffffffu, xc[0], 1);
+    if (lane == 0 && live && k0 > 1) prev = xload1(C, o - 1);
+    if (lane == BX - 1 && live && k0 + V <= kp) next = xload1(C, o + V);
+    const Coef<T>& c = C.c;
+    T au[V], ad[V];
+    vld(c.au + (live ? k0 : 1), au);
+    vld(c.ad + (live ? k0 : 1), ad);
+    const T sij = -ld(c.ae + i) - ld(c.aw + i) - ld(c.an + j) - ld(c.as + j);
+    const T ae = ld(c.ae + i), aw = ld(c.aw + i), an = ld(c.an + j), as = ld(c.as + j);
+    T ap[V], Ax[V];
+#pragma unroll
+    for (int q = 0; q < V; q++) {
+        const int kk = k0 + q;
+        T xd = q == 0 ? prev : xc[q - 1];
+        T xu = q == V - 1 ? next : xc[q + 1];
+        xd = kk == 1 ? xc[q] : xd;
+        xu = kk == kp ? xc[q] : xu;
+        ap[q] = sij - au[q] - ad[q];  // a_p, dynamics.f90:93-95 (same order)
+        // mat_ax, dynamics.f90:219-222 (a_c = 0)
+        Ax[q] = aw * xw[q] + ae * xe[q] + as * xs[q] + an * xn[q] + ad[q] * xd + au[q] * xu +
+                ap[q] * xc[q] + T(0);
     }
+    const SolverBufs& B = C.B;
+    T* __restrict__ out = (T*)B.out;
+    T res[V];
+    if (OP == OP_SETUP) {
+        T bv[V], res3[V];
+        vld((const T*)B.b + o, bv);
+#pragma unroll
+        for (int q = 0; q < V; q++) {
+            res[q] = bv[q] - Ax[q];  // :377
+            res3[q] = res[q] / ap[q];
+            if (q < nvalid) {
+                acc[0] += (double)bv[q] * (double)bv[q];
+                acc[NV - 1] += (double)res[q] * (double)res[q];
+            }
+        }
+        vst(out + o, res, nvalid);
+        vst((T*)B.out2 + o, res, nvalid);
+        vst((T*)B.out3 + o, res3, nvalid);
+    } else if (OP == OP_MATP) {
+        T cr[V], res3[V];
+        vld((const T*)B.cr + o, cr);
+#pragma unroll
+        for (int q = 0; q < V; q++) {
+            res3[q] = Ax[q] / ap[q];
+            if (q < nvalid) acc[0] += (double)cr[q] * (double)Ax[q];
+        }
+        vst(out + o, Ax, nvalid);
+        vst((T*)B.out3 + o, res3, nvalid);
+    } else if (OP == OP_MATC) {
+        T r[V], v1[V];
+        vld((const T*)B.r + o, r);
+        vld((const T*)B.v1 + o, v1);
+#pragma unroll
+        for (int q = 0; q < V; q++) {
+            const T sv = r[q] - C.alf * v1[q];  // s of :404
+            if (q < nvalid) {
+                acc[0] += (double)Ax[q] * (double)Ax[q];
+                acc[NV - 1] += (double)Ax[q] * (double)sv;
+            }
+        }
+        vst(out + o, Ax, nvalid);
+    } else {
+        // precondition, dynamics.f90:260-264:
+        //   s_new = s + (q - A s)/a_p = s + q/a_p - (A s)/a_p
+        T s0[V];
+        if (OP == OP_SW1) {
+#pragma unroll
+            for (int q = 0; q < V; q++) s0[q] = xc[q];
+        } else {
+            StenCtx<T, OP_SW1, MODE> C1;
+            C1.rh = C.rh; C1.vh = C.vh; C1.bet = C.bet; C1.omg = C.omg; C1.alf = C.alf;
+            C1.first = C.first;
+            xload(C1, o, s0);
+        }
+#pragma unroll
+        for (int q = 0; q < V; q++) res[q] = xc[q] + s0[q] - Ax[q] / ap[q];
+        if (OP == OP_SW3P) {
+            T pold[V];
+            if (C.first) {
+#pragma unroll
+                for (int q = 0; q < V; q++) res[q] = res[q] + C.bet * T(0);  // :397
+            } else {
+                vld_rw(out + o, pold);
+#pragma unroll
+                for (int q = 0; q < V; q++) res[q] = res[q] + C.bet * pold[q];
+            }
+        }
+        if (live) vst(out + o, res, nvalid);
+    }
+}
+
+// block and grid reduction of a reducing stencil kernel, then the scalar
+// recurrences in the last block
+template <int OP, int NV>
+__device__ __forceinline__ void reduce_tail(const SolverArgs& a, double (&acc)[NV], const Red2& R,
+                                            double* smem, SolverScalars* S) {
     block_reduce<R_SUM, NV>(acc, smem);
     double s[NV];
     if (reduce2<NV>(acc, R, smem, s) && threadIdx.x == 0 && threadIdx.y == 0) {
         if (OP == OP_SETUP) {
             double sc = sqrt(s[0]);
-            sc = sc > 0.01 ? sc : 0.01;  // dynamics.f90:370-371
-            const double err = sqrt(s[NV - 1]) / sc;
+            sc = sc > a.sc_floor ? sc : a.sc_floor;  // dynamics.f90:370-371
+            const double err = sc > 0.0 ? sqrt(s[NV - 1]) / sc : 0.0;
             S->sc_err = sc;
             S->err = err;
             S->it = 0;
@@ -250,6 +387,43 @@ __global__ void __launch_bounds__(256) k_sten(SolverArgs a, Coef<T> c, SolverBuf
     }
 }
 
+// Sweeps (no reduction): one warp task per warp, grid (k-chunks, j/8, i).
+// Reducing kernels: persistent blocks, each warp strides over the warp tasks
+// and the block publishes one partial.
+template <typename T, int OP, int MODE>
+__global__ void __launch_bounds__(256) k_sten(SolverArgs a, Coef<T> c, SolverBufs B, Red2 R,
+                                              SolverScalars* S) {
+    constexpr int NV = (OP == OP_SETUP || OP == OP_MATC) ? 2 : 1;
+    constexpr bool RED = OP == OP_SETUP || OP == OP_MATC || OP == OP_MATP;
+    __shared__ double smem[64];
+    if (OP != OP_SETUP && (S->done || S->pause)) return;
+    StenCtx<T, OP, MODE> C;
+    C.d = a.d;
+    C.c = c;
+    C.gx = (const T*)(OP == OP_SETUP ? B.x : B.sin);
+    C.rh = (const T*)B.rh;
+    C.vh = (const T*)B.vh;
+    C.B = B;
+    C.bet = (T)S->bet;
+    C.omg = (T)S->omg;
+    C.alf = (T)S->alf;
+    C.first = S->it == 0;
+    const Dims& d = a.d;
+    double acc[NV];
+#pragma unroll
+    for (int q = 0; q < NV; q++) acc[q] = 0.0;
+    if constexpr (!RED) {
+        const int j = 1 + blockIdx.y * BY + threadIdx.y;
+        if (j <= d.jp) sten_task<T, OP, MODE, NV>(C, blockIdx.x, j, 1 + blockIdx.z, acc);
+    } else {
+        for (TaskIter t(blockIdx.x * blockDim.y + threadIdx.y, gridDim.x * blockDim.y, a.nkt,
+                        d.jp);
+             t.i <= d.ip; t.next())
+            sten_task<T, OP, MODE, NV>(C, t.kt, 1 + t.jr, t.i, acc);
+        reduce_tail<OP, NV>(a, acc, R, smem, S);
+    }
+}
+
 // --- D: x, r updates, (r,r), (r,cr) -> err, next rho and bet -----------------
 template <typename T>
 __global__ void __launch_bounds__(256) k_bicg_update(SolverArgs a, Coef<T> c,
@@ -263,29 +437,44 @@ __global__ void __launch_bounds__(256) k_bicg_update(SolverArgs a, Coef<T> c,
                                                      T* __restrict__ rh, Red2 R,
                                                      SolverScalars* S) {
     __shared__ double smem[64];
-    if (S->done) return;
+    if (S->done || S->pause) return;
     const Dims& d = a.d;
     const T alf = (T)S->alf, omg = (T)S->omg;
     double acc[2] = {0.0, 0.0};
-    const int nkt = a.nkt;
-    const long long ntask = (long long)nkt * d.jp * d.ip;
-    const int warps = blockDim.y;
-    for (long long tk = (long long)blockIdx.x * warps + threadIdx.y; tk < ntask;
-         tk += (long long)gridDim.x * warps) {
-        const int kt = (int)(tk % nkt);
-        const long long r2 = tk / nkt;
-        const int j = 1 + (int)(r2 % d.jp);
-        const int i = 1 + (int)(r2 / d.jp);
-        const int k = 1 + kt * BX + threadIdx.x;
-        if (k > d.kp) continue;
-        const int o = d.at(k, j, i);
-        const T sv = r[o] - alf * v1[o];
-        x[o] = x[o] + alf * p[o] + omg * cs[o];  // :419
-        const T rn = sv - omg * t[o];             // :420
-        r[o] = rn;
-        rh[o] = rn / diag_ap(c, k, j, i);
-        acc[0] += (double)rn * (double)rn;
-        acc[1] += (double)rn * (double)cr[o];
+    constexpr int V = KVec<T>::V;
+    const int lane = threadIdx.x;
+    for (TaskIter tk(blockIdx.x * blockDim.y + threadIdx.y, gridDim.x * blockDim.y, a.nkt, d.jp);
+         tk.i <= d.ip; tk.next()) {
+        const int k0 = 1 + V * (tk.kt * BX + lane);
+        if (k0 > d.kp) continue;
+        const int nvalid = min(V, d.kp - k0 + 1);
+        const int j = 1 + tk.jr, i = tk.i;
+        const int o = d.at(k0, j, i);
+        T xv[V], pv[V], csv[V], rv[V], v1v[V], tv[V], crv[V], au[V], ad[V], rhv[V];
+        vld_rw(x + o, xv);
+        vld(p + o, pv);
+        vld(cs + o, csv);
+        vld_rw(r + o, rv);
+        vld(v1 + o, v1v);
+        vld(t + o, tv);
+        vld(cr + o, crv);
+        vld(c.au + k0, au);
+        vld(c.ad + k0, ad);
+        const T sij = -ld(c.ae + i) - ld(c.aw + i) - ld(c.an + j) - ld(c.as + j);
+#pragma unroll
+        for (int q = 0; q < V; q++) {
+            const T sv = rv[q] - alf * v1v[q];
+            xv[q] = xv[q] + alf * pv[q] + omg * csv[q];  // :419
+            rv[q] = sv - omg * tv[q];                    // :420
+            rhv[q] = rv[q] / (sij - au[q] - ad[q]);
+            if (q < nvalid) {
+                acc[0] += (double)rv[q] * (double)rv[q];
+                acc[1] += (double)rv[q] * (double)crv[q];
+            }
+        }
+        vst(x + o, xv, nvalid);
+        vst(r + o, rv, nvalid);
+        vst(rh + o, rhv, nvalid);
     }
     block_reduce<R_SUM, 2>(acc, smem);
     double s[2];
@@ -295,7 +484,12 @@ __global__ void __launch_bounds__(256) k_bicg_update(SolverArgs a, Coef<T> c,
         const double err = sqrt(s[0]) / S->sc_err;  // :423
         S->err = err;
         S->nrm = S->rho;  // :425
-        if (err < a.tol) {  // :428
+        if (S->ru && (err < a.tol || sqrt(s[0]) < S->delta * S->ru_norm)) {
+            // reliable update (mixed-precision form): the host replaces r by
+            // the FP64 residual before the iteration continues
+            S->pause = 1;
+            S->rho = s[1];
+        } else if (err < a.tol) {  // :428
             S->done = 1;
         } else if (!(err == err)) {
             S->status = DCM_E_NONFINITE;
@@ -313,9 +507,9 @@ __global__ void __launch_bounds__(256) k_bicg_update(SolverArgs a, Coef<T> c,
 // --- after the solve: halo rows of x (dynamics.f90:437-442 or, after the
 //     early return, mat_ax's rows :203-211) and the driver's
 //     exchange_along_dim_wo(p) (driver_code.f90:506)
-template <typename T>
+template <typename T, typename TS>
 __global__ void __launch_bounds__(256) k_bicg_post(Dims d, T* __restrict__ x,
-                                                   const T* __restrict__ sw,
+                                                   const TS* __restrict__ sw,
                                                    const T* __restrict__ dzn,
                                                    const SolverScalars* S, int wo) {
     const int k = 1 + blockIdx.x * BX + threadIdx.x;
@@ -339,7 +533,7 @@ __global__ void __launch_bounds__(256) k_bicg_post(Dims d, T* __restrict__ x,
         for (int b3 = 0; b3 < nj; b3++)
             for (int c3 = 0; c3 < ni; c3++) {
                 const int jj = js[b3], ii = is[c3];
-                x[d.at(0, jj, ii)] = v - sw[d.at(0, jj, ii)] * dz0;
+                x[d.at(0, jj, ii)] = v - (T)sw[d.at(0, jj, ii)] * dz0;
             }
     }
 }
@@ -370,6 +564,12 @@ static int persistent_grid(K kernel) {
     return sm_count() * (per > 0 ? per : 1);
 }
 
+// Warp tasks: (k-chunk of 32 V levels, j, i).
+template <typename T>
+static int kchunks(const Dims& d) {
+    return (d.kp + KVec<T>::V * BX - 1) / (KVec<T>::V * BX);
+}
+
 template <typename T, int OP, int MODE>
 static void sten(const SolverArgs& a, const Coef<T>& c, const SolverBufs& B, SolverWork<T>& w,
                  cudaStream_t st, int cat) {
@@ -380,8 +580,8 @@ static void sten(const SolverArgs& a, const Coef<T>& c, const SolverBufs& B, Sol
         if (!g) g = persistent_grid(k_sten<T, OP, MODE>);
         k_sten<T, OP, MODE><<<g, dim3(BX, BY), 0, st>>>(a, c, B, w.red, w.S);
     } else {
-        k_sten<T, OP, MODE><<<interior_grid(a.d, a.d.kp), dim3(BX, BY), 0, st>>>(a, c, B, w.red,
-                                                                                   w.S);
+        const dim3 grid(a.nkt, (a.d.jp + BY - 1) / BY, a.d.ip);
+        k_sten<T, OP, MODE><<<grid, dim3(BX, BY), 0, st>>>(a, c, B, w.red, w.S);
     }
 }
 
@@ -430,20 +630,16 @@ static void launch_iteration(const SolverArgs& a, const Coef<T>& c, SolverWork<T
     }
 }
 
-int solver_ich = 16;  // i-planes per tile
-
 template <typename T>
 int solver_run(SolverWork<T>& w, const Dims& d, T* x, const T* b, const T* sw, const T* dzn,
                double tol, int itmax, int wo, int chunk, cudaStream_t st, SolverScalars* host_S,
-               int* launched_iters) {
+               int* launched_iters, double sc_floor, bool post) {
     SolverArgs a;
     a.d = d;
     a.itmax = itmax;
     a.tol = tol;
-    a.ich = solver_ich;
-    a.nkt = (d.kp + BX - 1) / BX;
-    a.njt = (d.jp + BY - 1) / BY;
-    a.ntiles = a.nkt * a.njt * ((d.ip + a.ich - 1) / a.ich);
+    a.sc_floor = sc_floor;
+    a.nkt = kchunks<T>(d);
     const Coef<T> c = coef_of(w);
     SolverBufs B{};
     B.x = x;
@@ -463,9 +659,9 @@ int solver_run(SolverWork<T>& w, const Dims& d, T* x, const T* b, const T* sw, c
             launch_iteration<T>(a, c, w, x, st);
         if (cudaGetLastError() != cudaSuccess) return DCM_E_CUDA;
     }
-    {
+    if (post) {
         ProfScope ps(P_POST, st);
-        k_bicg_post<T><<<interior_grid(d, d.kp), dim3(BX, BY), 0, st>>>(d, x, sw, dzn, w.S, wo);
+        k_bicg_post<T, T><<<interior_grid(d, d.kp), dim3(BX, BY), 0, st>>>(d, x, sw, dzn, w.S, wo);
     }
     cudaMemcpyAsync(host_S, w.S, sizeof(SolverScalars), cudaMemcpyDeviceToHost, st);
     if (cudaStreamSynchronize(st) != cudaSuccess) return DCM_E_CUDA;
@@ -475,6 +671,207 @@ int solver_run(SolverWork<T>& w, const Dims& d, T* x, const T* b, const T* sw, c
 
 template int solver_run<double>(SolverWork<double>&, const Dims&, double*, const double*,
                                 const double*, const double*, double, int, int, int,
-                                cudaStream_t, SolverScalars*, int*);
+                                cudaStream_t, SolverScalars*, int*, double, bool);
+template int solver_run<float>(SolverWork<float>&, const Dims&, float*, const float*,
+                               const float*, const float*, double, int, int, int, cudaStream_t,
+                               SolverScalars*, int*, double, bool);
+
+// =============================================================================
+// Mixed precision: FP32 BiCGSTAB with FP64 reliable updates
+// =============================================================================
+// The pressure x and the residual that decides convergence are FP64; every
+// vector of the BiCGSTAB recursion and every stencil sweep is FP32, and all
+// dot products are summed in FP64.  One Krylov iteration runs from start to
+// convergence; whenever its recursive FP32 residual has fallen by `delta`
+// since the last FP64 residual (or below the tolerance), the iteration pauses
+// and the host performs an FP64 refinement step:
+//     x64 += dx32, dx32 = 0;   r = b - A x64 (FP64);   r32 = r, r32/a_p
+// and the recursion resumes from the replaced residual with
+// rho = (r, cr) -- iterative refinement that keeps the Krylov space
+// (reliable updates, Sleijpen & van der Vorst 1996).  Convergence is the
+// reference's ||r|| / max(||b||, 0.01) < ptol on the FP64 residual
+// (dynamics.f90:370-428).
+
+// r = b - A x (FP64) -> r32, r32/a_p; FIRST also cr = r32 and (b,b).
+template <bool FIRST>
+__global__ void __launch_bounds__(256) k_ru_residual(SolverArgs a, Coef<double> c,
+                                                     Coef<float> cf,
+                                                     const double* __restrict__ x,
+                                                     const double* __restrict__ b,
+                                                     float* __restrict__ r32,
+                                                     float* __restrict__ rh32,
+                                                     float* __restrict__ cr32, Red2 R,
+                                                     SolverScalars* S) {
+    __shared__ double smem[96];
+    const Dims& d = a.d;
+    const int ip = d.ip, jp = d.jp, kp = d.kp;
+    double acc[3] = {0.0, 0.0, 0.0};
+    const int lane = threadIdx.x;
+    for (TaskIter t(blockIdx.x * blockDim.y + threadIdx.y, gridDim.x * blockDim.y, a.nkt, jp);
+         t.i <= ip; t.next()) {
+        const int j = 1 + t.jr, i = t.i;
+        const int k = 1 + t.kt * BX + lane;
+        const int km = min(k, kp);
+        const double xc = x[d.at(km, j, i)];
+        double xd = __shfl_up_sync(0xffffffffu, xc, 1);
+        double xu = __shfl_down_sync(0xffffffffu, xc, 1);
+        if (lane == 0) xd = x[d.at(max(km - 1, 1), j, i)];
+        if (lane == BX - 1) xu = x[d.at(min(km + 1, kp), j, i)];
+        if (k > kp) continue;
+        const double xm = x[d.at(k, j, i == 1 ? ip : i - 1)], xp = x[d.at(k, j, i == ip ? 1 : i + 1)];
+        const double xs = x[d.at(k, j == 1 ? jp : j - 1, i)], xn = x[d.at(k, j == jp ? 1 : j + 1, i)];
+        const double ae = ld(c.ae + i), aw = ld(c.aw + i), an = ld(c.an + j), as = ld(c.as + j),
+                     au = ld(c.au + k), ad = ld(c.ad + k);
+        const double ap = -ae - aw - an - as - au - ad;
+        const double Ax = aw * xm + ae * xp + as * xs + an * xn + ad * xd + au * xu + ap * xc;
+        const int o = d.at(k, j, i);
+        const double bv = b[o];
+        const double rv = bv - Ax;
+        const float rf = (float)rv;
+        r32[o] = rf;
+        rh32[o] = rf / diag_ap(cf, k, j, i);
+        float crf;
+        if (FIRST) {
+            cr32[o] = rf;
+            crf = rf;
+        } else {
+            crf = cr32[o];
+        }
+        acc[0] += bv * bv;
+        acc[1] += rv * rv;
+        acc[2] += (double)rf * (double)crf;
+    }
+    block_reduce<R_SUM, 3>(acc, smem);
+    double s[3];
+    if (reduce2<3>(acc, R, smem, s) && threadIdx.x == 0 && threadIdx.y == 0) {
+        if (FIRST) {
+            double sc = sqrt(s[0]);
+            sc = sc > 0.01 ? sc : 0.01;  // dynamics.f90:370-371
+            S->sc_err = sc;
+            S->it = 0;
+            S->status = 0;
+            S->updates = 0;
+            S->alf = 1.0;  // :385-387
+            S->omg = 1.0;
+            S->nrm = 1.0;
+        }
+        const double err = sqrt(s[1]) / S->sc_err;
+        S->err = err;
+        S->ru_norm = sqrt(s[1]);
+        S->pause = 0;
+        S->done = 0;
+        S->early = 0;
+        if (err < a.tol) {
+            S->done = 1;
+            S->early = FIRST ? 1 : 0;
+        } else if (!(err == err)) {
+            S->status = DCM_E_NONFINITE;
+            S->done = 1;
+        } else {
+            S->rho = s[2];  // (r, cr) of the replaced residual
+            S->bet = (S->rho / S->nrm) * (S->alf / S->omg);
+            if (!FIRST) S->updates = S->updates + 1;
+        }
+    }
+}
+
+// x (FP64) += dx (FP32); dx = 0 (interior)
+__global__ void __launch_bounds__(256) k_ru_add(Dims d, double* __restrict__ x,
+                                                float* __restrict__ dx) {
+    const int k = 1 + blockIdx.x * BX + threadIdx.x;
+    const int j = 1 + blockIdx.y * BY + threadIdx.y;
+    const int i = 1 + blockIdx.z;
+    if (k > d.kp || j > d.jp) return;
+    const int o = d.at(k, j, i);
+    x[o] = x[o] + (double)dx[o];
+    dx[o] = 0.0f;
+}
+
+int refine_run(SolverWork<float>& wf, SolverWork<double>& wd, const Dims& d, double* x,
+               const double* b, const float* sw, const double* dzn, float* dx, double tol,
+               double delta, int itmax, int max_updates, cudaStream_t st,
+               SolverScalars* hS_out, SolverScalars* hS_in, RefineStats* rs) {
+    SolverArgs a;
+    a.d = d;
+    a.itmax = itmax;
+    a.tol = tol;
+    a.sc_floor = 0.01;
+    a.nkt = (d.kp + BX - 1) / BX;  // scalar warp tasks of the FP64 residual
+    SolverArgs af = a;             // vector warp tasks of the FP32 iterations
+    af.nkt = kchunks<float>(d);
+    Coef<double> cd;
+    cd.ae = wd.ae; cd.aw = wd.aw; cd.an = wd.an; cd.as = wd.as; cd.au = wd.au; cd.ad = wd.ad;
+    const Coef<float> cf = coef_of(wf);
+    static int g = 0;
+    if (!g) g = persistent_grid(k_ru_residual<false>);
+    const dim3 gi = interior_grid(d, d.kp), bl(BX, BY);
+    if (cudaMemsetAsync(dx, 0, d.n() * sizeof(float), st) != cudaSuccess) return DCM_E_CUDA;
+    // reliable-update controls live in the FP32 solve's scalars
+    hS_in->ru = 1;
+    hS_in->delta = delta;
+    cudaMemcpyAsync(&wf.S->ru, &hS_in->ru, sizeof(int), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(&wf.S->delta, &hS_in->delta, sizeof(double), cudaMemcpyHostToDevice, st);
+    {
+        ProfScope ps(P_SETUP, st);
+        k_ru_residual<true><<<g, bl, 0, st>>>(a, cd, cf, x, b, wf.r, wf.rh, wf.cr, wd.red, wf.S);
+    }
+    int launched = 0, status = DCM_OK;
+    for (;;) {
+        cudaMemcpyAsync(hS_in, wf.S, sizeof(SolverScalars), cudaMemcpyDeviceToHost, st);
+        if (cudaStreamSynchronize(st) != cudaSuccess) return DCM_E_CUDA;
+        if (hS_in->done) break;
+        if (hS_in->pause) {
+            if (hS_in->updates >= max_updates) {
+                status = DCM_E_NOCONV;
+                break;
+            }
+            {
+                ProfScope ps(P_UPDATE, st);
+                k_ru_add<<<gi, bl, 0, st>>>(d, x, dx);
+            }
+            {
+                ProfScope ps(P_SETUP, st);
+                k_ru_residual<false><<<g, bl, 0, st>>>(a, cd, cf, x, b, wf.r, wf.rh, wf.cr, wd.red,
+                                                       wf.S);
+            }
+            if (std::getenv("DCM_DEBUG")) {
+                cudaMemcpyAsync(hS_in, wf.S, sizeof(SolverScalars), cudaMemcpyDeviceToHost, st);
+                cudaStreamSynchronize(st);
+                std::fprintf(stderr, "reliable update %d at it %d: FP64 err %.3e\n",
+                             hS_in->updates, hS_in->it, hS_in->err);
+            }
+            continue;
+        }
+        if (launched >= itmax) {
+            status = DCM_E_NOCONV;
+            break;
+        }
+        for (int q = 0; q < 4 && launched < itmax; q++, launched++)
+            launch_iteration<float>(af, cf, wf, dx, st);
+        if (cudaGetLastError() != cudaSuccess) return DCM_E_CUDA;
+    }
+    if (status == DCM_OK) status = hS_in->status;
+    // the correction accumulated since the last update (zero after one)
+    k_ru_add<<<gi, bl, 0, st>>>(d, x, dx);
+    // leave the FP32 scalars in plain mode for any later use
+    hS_in->ru = 0;
+    cudaMemcpyAsync(&wf.S->ru, &hS_in->ru, sizeof(int), cudaMemcpyHostToDevice, st);
+    hS_out->early = hS_in->early;
+    hS_out->status = status;
+    hS_out->it = hS_in->it;
+    hS_out->err = hS_in->err;
+    cudaMemcpyAsync(wd.S, hS_out, sizeof(SolverScalars), cudaMemcpyHostToDevice, st);
+    {
+        ProfScope ps(P_POST, st);
+        k_bicg_post<double, float><<<gi, bl, 0, st>>>(d, x, sw, dzn, wd.S, 1);
+    }
+    if (cudaStreamSynchronize(st) != cudaSuccess) return DCM_E_CUDA;
+    if (rs) {
+        rs->outer = hS_in->updates;
+        rs->inner = hS_in->it;
+        rs->err = hS_in->err;
+    }
+    return status;
+}
 
 }  // namespace dcm

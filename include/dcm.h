@@ -171,7 +171,14 @@ typedef struct {
     int moisture, nq, ncat; /* q categories advected by mpdata_vec_3d      */
     const int *c_s, *c_e;   /* 1-based category bounds (ncat each)         */
     double thbase, thtop;   /* lbc / ubc of scheme 2                       */
-    int precision;          /* 0 = FP64 (the reference's VAR_TYPE=1)      */
+    int precision;          /* 0 = FP64 (the reference's VAR_TYPE=1);
+                               1 = FP32 fields; FP32 BiCGSTAB iterations on
+                               an FP64 pressure with FP64 reliable updates,
+                               converged to ptol on the FP64 residual      */
+    double inner_tol;       /* precision 1: reliable-update factor: the FP32
+                               recursion stops for an FP64 update of p and
+                               of the true residual when its residual has
+                               fallen by this factor (0 -> 0.1)            */
     dcm_forcing forcing;
 } dcm_config;
 
