@@ -9,6 +9,12 @@ of the run from the initial state (a warm-up run of W steps precedes them on
 the same handle, then the initial state is uploaded again), so every arm
 times the same time steps with the same solver iteration counts.
 
+The headline `value` is the mixed-precision form (FP32 fields and BiCGSTAB
+iterations, FP64 pressure, residual and dot products); the plain FP64 path
+is timed on the same steps (`fp64`), and the per-field max / RMS errors of
+the mixed form against the FP64 path after 1, 10 and --accuracy-steps steps
+go in `accuracy_vs_fp64`.
+
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
 N > 1 (torchrun, one process per GPU): the single domain does not shard
@@ -107,11 +113,15 @@ class ClockSampler:
 
 # algorithmic field passes per launch of each kernel class (reads + writes of
 # an N-point field; stencil neighbours come from cache).  Jacobi sweeps:
-# B1 3, B2 4, B3 5, C1 3, C2 4, C3 4 -> 23/6; matvecs: B4 3, C4 4 -> 3.5;
-# update 9.  Other classes per launch at this configuration.
-PASSES = {"jacobi": 23.0 / 6.0, "matvec": 3.5, "update": 9.0, "setup": 4.0,
+# B1 3, B2 4, B3 5, C1 3, C2 4, C3 4 -> 23/6; matvecs: B4 (p, cr -> v1, vh) 4,
+# C4 (cs, r, v1 -> t) 4; update (x p cs r v1 t cr -> x r rh) 10.  Other
+# classes per launch at this configuration.
+PASSES = {"jacobi": 23.0 / 6.0, "matvec": 4.0, "update": 10.0, "setup": 4.0,
           "means": 5.0, "sources": 7.0, "rhs": 4.0, "adv_ref": 3.0, "mp_shift": 1.0,
           "upwind": 5.0, "antidiff": 7.0, "beta": 7.0, "limit": 8.0, "momentum": 16.0}
+# field passes of one BiCGSTAB iteration and of the rest of a step
+ITER_PASSES = 41.0
+STEP_PASSES = 60.0
 
 
 def make_case(pkg, name):
@@ -136,6 +146,37 @@ def pinned_like(a):
     return v, t
 
 
+def live_mask_p(g):
+    """Cells of p the reference computes and later reads (all but the halo
+    rings of the top/bottom rows and the vertical halo edges)."""
+    m = np.ones((g.kp + 2, g.jp + 2, g.ip + 2), dtype=bool, order="F")
+    jh = np.zeros(g.jp + 2, dtype=bool)
+    jh[[0, g.jp + 1]] = True
+    ih = np.zeros(g.ip + 2, dtype=bool)
+    ih[[0, g.ip + 1]] = True
+    ring = jh[:, None] | ih[None, :]
+    m[0][ring] = False
+    m[g.kp + 1][ring] = False
+    m[1:g.kp + 1][:, jh[:, None] & ih[None, :]] = False
+    return m
+
+
+def field_errors(g, ref, got):
+    """Per-field max and RMS error of `got` relative to max|ref| (p on its
+    live cells)."""
+    out = {}
+    for n in ("u", "v", "w", "th", "p"):
+        a, b = np.asarray(got[n]), np.asarray(ref[n])
+        if n == "p":
+            m = live_mask_p(g)
+            a, b = a[m], b[m]
+        den = float(np.max(np.abs(b))) or 1.0
+        d = a - b
+        out[n] = {"max": float(np.max(np.abs(d)) / den),
+                  "rms": float(np.sqrt(np.mean(d * d)) / den)}
+    return out
+
+
 def run_b200(args, rank, world, local_rank, dist):
     pkg = load_pkg()
     case = make_case(pkg, args.case)
@@ -143,15 +184,11 @@ def run_b200(args, rank, world, local_rank, dist):
     N = g.npoints
     core = pkg.DynamicalCore(g, device=local_rank)
     kw = dict(ptol=case.ptol, kord=case.kord, monotone=case.monotone)
+    peak, peak_kind = peaks()
 
-    def fresh():
-        core.upload_state(case.state, case.dt, **kw)
+    def fresh(prec):
+        core.upload_state(case.state, case.dt, precision=prec, **kw)
         core.driver_start()
-
-    # warm-up run (allocations, first launches), then restart from step 1
-    fresh()
-    if args.warmup:
-        core.step(args.warmup)
 
     def barrier():
         if dist is not None:
@@ -167,43 +204,72 @@ def run_b200(args, rank, world, local_rank, dist):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    # ---- timed region (device time from CUDA events on the library stream)
-    fresh()
-    core.profile(False)  # reset the launch counters, event timing off
-    clocks = ClockSampler(local_rank)
-    barrier()
-    clocks.start()
-    st = core.step(args.steps)
-    clk = clocks.stop()
-    barrier()
-    ms = max_over_ranks(st.ms_total)
-    launches = sum(c for _, c in core.profile_read().values())
-    iters = st.iters_total
-    value = world * N * args.steps / (ms / 1e3)
+    def measure(prec):
+        """Steps 1..K of one precision: device time (CUDA events on the
+        library stream, max over ranks), launches, clocks, then the same
+        steps again with per-kernel-class events for the roofline."""
+        fresh(prec)  # warm-up run (allocations, first launches)
+        if args.warmup:
+            core.step(args.warmup)
+        fresh(prec)
+        core.profile(False)  # reset the launch counters, event timing off
+        clocks = ClockSampler(local_rank)
+        barrier()
+        clocks.start()
+        st = core.step(args.steps)
+        clk = clocks.stop()
+        barrier()
+        ms = max_over_ranks(st.ms_total)
+        launches = sum(c for _, c in core.profile_read().values())
+        fresh(prec)
+        core.profile(True)
+        core.step(args.steps)
+        prof = core.profile_read()
+        core.profile(False)
+        classes = {k: v for k, v in prof.items() if v[1] > 0}
+        return dict(ms=ms, iters=st.iters_total, launches=launches, clocks=clk,
+                    classes=classes, value=world * N * args.steps / (ms / 1e3))
 
-    # ---- per-kernel-class timing (same steps again, events around launches)
-    fresh()
-    core.profile(True)
-    st2 = core.step(args.steps)
-    prof = core.profile_read()
-    core.profile(False)
-    peak, peak_kind = peaks()
-    classes = {k: v for k, v in prof.items() if v[1] > 0}
+    m32 = measure(1)
+    m64 = measure(0)
+
+    # roofline of the dominant kernel class of the headline (mixed) form
+    w32 = 4.0
+    classes = m32["classes"]
     dom = max(classes, key=lambda k: classes[k][0])
     dom_ms, dom_n = classes[dom]
-    dom_bytes = PASSES.get(dom, 0.0) * N * 8.0
+    dom_bytes = PASSES.get(dom, 0.0) * N * w32
     achieved = dom_bytes / (dom_ms / dom_n / 1e3) / 1e9 if dom_n else None
     traffic = None
     tp = os.path.join(ROOT, "profiles", "dram_traffic.json")
     if os.path.exists(tp):
         with open(tp) as f:
-            tr = json.load(f).get(args.case, {})
-        if dom in tr:
-            traffic = tr[dom]
-    step_bytes = (60.0 + 39.0 * iters / args.steps) * N * 8.0
-    step_gbs = step_bytes / (ms / args.steps / 1e3) / 1e9
+            tr = json.load(f).get(args.case, {}).get("fp32", {})
+        traffic = tr.get(dom)
 
-    # ---- end to end through the C-ABI with host buffers (pinned)
+    def step_model(m, w):
+        it = m["iters"] / args.steps
+        b = (STEP_PASSES + ITER_PASSES * it) * N * w
+        gbs = b / (m["ms"] / args.steps / 1e3) / 1e9
+        return {"bytes_per_step": b, "GBs": gbs, "frac": gbs / peak, "iters_per_step": it}
+
+    # ---- accuracy: mixed against the FP64 path after the timed steps and
+    #      after args.accuracy_steps
+    acc = {}
+    if args.accuracy_steps:
+        cores = [core, pkg.DynamicalCore(g, device=local_rank)]
+        for prec, c in zip((0, 1), cores):
+            c.upload_state(case.state, case.dt, precision=prec, **kw)
+            c.driver_start()
+        done = 0
+        for n in sorted({1, 10, args.accuracy_steps}):
+            for c in cores:
+                c.step(n - done)
+            done = n
+            acc[str(n)] = field_errors(g, cores[0].download_state(), cores[1].download_state())
+        cores[1].close()
+
+    # ---- end to end through the C-ABI with host buffers (pinned), mixed form
     host = {n: pinned_like(getattr(case.state, n)) for n in
             ("u", "v", "w", "zu", "zv", "zw", "tu", "tv", "tw", "th", "p")}
     st_host = case.state.copy()
@@ -211,7 +277,7 @@ def run_b200(args, rank, world, local_rank, dist):
         setattr(st_host, n, v)
     barrier()
     t0 = time.perf_counter()
-    core.upload_state(st_host, case.dt, **kw)
+    core.upload_state(st_host, case.dt, precision=1, **kw)
     core.driver_start()
     core.step(args.steps)
     out = core.download_state()
@@ -223,7 +289,8 @@ def run_b200(args, rank, world, local_rank, dist):
     d2h = sum(a.nbytes for a in out.values() if isinstance(a, np.ndarray))
     e2e = {"value": world * N * args.steps / e2e_s, "unit": "grid-pt-steps/s",
            "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
-           "note": "upload of the state, K steps, download of the state per K-step call"}
+           "note": "mixed form: upload of the FP64 host state, K steps, download of the "
+                   "state, per K-step call"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -232,24 +299,34 @@ def run_b200(args, rank, world, local_rank, dist):
     if rank != 0:
         return None
     return {
-        "metric": METRIC, "value": value, "unit": "grid-pt-steps/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "metric": METRIC, "value": m32["value"], "unit": "grid-pt-steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": m32["ms"] / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64 (FP32 fields and BiCGSTAB, FP64 pressure, residual and dots)",
         "data": "synthetic (seeded warm bubble, numpy PCG64 seed %d)" % case.seed,
-        "config": {"workload": case.name, "precision": "fp64", "grid": [g.ip, g.jp, g.kp],
-                   "dt": case.dt, "kord": case.kord, "monotone": bool(case.monotone),
-                   "ptol": case.ptol, "timed_steps": "1..%d from the initial state" % args.steps,
-                   "bicgstab_iters_per_step": iters / args.steps,
-                   "l2": "inputs larger than L2 (20 fields x 69 MB resident)",
+        "config": {"workload": case.name + " mixed precision (FP32 + FP64 reliable updates)",
+                   "grid": [g.ip, g.jp, g.kp], "dt": case.dt, "kord": case.kord,
+                   "monotone": bool(case.monotone), "ptol": case.ptol,
+                   "timed_steps": "1..%d from the initial state" % args.steps,
+                   "bicgstab_iters_per_step": m32["iters"] / args.steps,
+                   "l2": "inputs larger than L2 (about 40 fields of 34-69 MB resident)",
                    "parallelism": "replicas" if world > 1 else "single GPU"},
+        "fp64": {"value": m64["value"], "ms_per_step": m64["ms"] / args.steps,
+                 "bicgstab_iters_per_step": m64["iters"] / args.steps,
+                 "gpu_launches": m64["launches"], "clocks": m64["clocks"],
+                 "step_model": step_model(m64, 8.0),
+                 "kernel_ms": {k: round(v[0], 3) for k, v in m64["classes"].items()}},
+        "speedup_vs_fp64": m32["value"] / m64["value"],
+        "accuracy_vs_fp64": acc,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
                      "traffic": traffic, "peak_kind": peak_kind,
                      "bytes_per_launch": dom_bytes, "launches": dom_n,
                      "avg_launch_us": dom_ms / dom_n * 1e3 if dom_n else None,
-                     "step_model_GBs": step_gbs, "step_model_frac": step_gbs / peak},
+                     "step_model": step_model(m32, w32)},
         "kernel_ms": {k: round(v[0], 3) for k, v in classes.items()},
-        "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
+        "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": m32["launches"],
+        "clocks": m32["clocks"],
     }
 
 
@@ -306,6 +383,7 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--cpu-budget", type=float, default=60.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--accuracy-steps", type=int, default=100)
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
