@@ -109,6 +109,7 @@ def library():
             "dcm_horizontal_means_noalloc": [C.c_int, C.c_int, C.c_int, P, P, P, P, P, P],
             "dcm_profile_enable": [P, C.c_int],
             "dcm_profile_read": [P, _dp, C.POINTER(C.c_longlong), C.c_int],
+            "dcm_solver_graphs": [P, C.c_int],
         }
         for name, args in sig.items():
             f = getattr(lib, name)
@@ -125,7 +126,7 @@ EXPORTS = ("dcm_create", "dcm_destroy", "dcm_status_string", "dcm_last_error",
            "dcm_divergence_calc", "dcm_advance_scalar_fields_3d", "dcm_exchange_full",
            "dcm_exchange_along_dim", "dcm_exchange_along_dim_wo", "dcm_state_upload",
            "dcm_driver_start", "dcm_step", "dcm_state_download", "dcm_profile_enable",
-           "dcm_profile_read", "dcm_horizontal_means_noalloc")
+           "dcm_profile_read", "dcm_horizontal_means_noalloc", "dcm_solver_graphs")
 
 PROF_CLASSES = ("setup", "jacobi", "matvec", "update", "post", "means", "sources", "rhs",
                 "adv_ref", "mp_shift", "upwind", "antidiff", "beta", "limit", "restore",
@@ -368,6 +369,10 @@ class DynamicalCore:
         stats = StepStats()
         self._check(self.lib.dcm_step(self.h, int(nsteps), C.byref(stats)))
         return stats
+
+    def solver_graphs(self, on=True):
+        """Graph-driven pressure solves (default) or the host-polled loop."""
+        self._check(self.lib.dcm_solver_graphs(self.h, int(bool(on))))
 
     def profile(self, on=True):
         """Enable (and reset) or disable per-kernel-class event timing."""

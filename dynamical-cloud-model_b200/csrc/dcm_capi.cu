@@ -79,6 +79,10 @@ struct dcm_handle {
     std::vector<float*> fslots;
     SolverScalars* S2 = nullptr;   // scalars of the inner (FP32) solve
     SolverScalars* hS2 = nullptr;  // pinned
+    // captured pressure solves (FP64 and mixed), rebuilt when their
+    // arguments change
+    SolveGraph g64, g32;
+    bool graphs = true;  // graph-driven solver loops (else host-polled)
 
     // ---- resident state -------------------------------------------------------
     bool resident = false;
@@ -199,6 +203,7 @@ SolverWork<double> solver_work(dcm_handle* h) {
     w.partials = h->partials; w.ticket = h->ticket; w.S = h->S;
     w.red.partials = h->partials; w.red.gpartials = h->gpartials; w.red.gtick = h->gtick;
     w.red.ticket = h->ticket2;
+    w.graph = h->graphs ? &h->g64 : nullptr;
     return w;
 }
 
@@ -406,6 +411,8 @@ extern "C" int dcm_create(const dcm_grid* g, int device, dcm_handle** out) {
 }
 
 static void free_state(dcm_handle* h) {
+    h->g64.release();  // captured solves hold the old field pointers
+    h->g32.release();
     for (void* p : h->owned) cudaFree(p);
     h->owned.clear();
     h->s64 = State<double>();
@@ -859,6 +866,7 @@ SolverWork<float> solver_work_f(dcm_handle* h) {
     w.partials = h->partials; w.ticket = h->ticket; w.S = h->S2;
     w.red.partials = h->partials; w.red.gpartials = h->gpartials; w.red.gtick = h->gtick;
     w.red.ticket = h->ticket2;
+    w.graph = h->graphs ? &h->g32 : nullptr;
     return w;
 }
 
@@ -1222,6 +1230,12 @@ extern "C" int dcm_state_download(dcm_handle* h, dcm_fields* f) {
 // =============================================================================
 // diagnostics
 // =============================================================================
+extern "C" int dcm_solver_graphs(dcm_handle* h, int on) {
+    CHECK_H();
+    h->graphs = on != 0;
+    return DCM_OK;
+}
+
 extern "C" int dcm_profile_enable(dcm_handle* h, int on) {
     CHECK_H();
     h->prof.reset();

@@ -19,6 +19,40 @@ struct SolverScalars {
     // residual (ru_norm) or below the tolerance
     double ru_norm, delta;
     int ru, pause, updates, pad;
+    int rounds;  // loop rounds of a graph-driven solve (bounded, see k_loop_cond)
+    int pad2;
+};
+
+// One pressure solve captured as a CUDA graph: the iteration loop is a
+// conditional WHILE node whose condition a device kernel sets, so the host
+// neither polls nor launches per iteration.  Rebuilt when any captured
+// argument changes (key).
+struct SolveGraph {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaStream_t side[2] = {nullptr, nullptr};  // capture streams of the loop bodies
+    // key: everything the captured launches depend on
+    const void* key_ptr[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    double key_d[3] = {0, 0, 0};
+    int key_i[6] = {0, 0, 0, 0, 0, 0};
+    bool matches(const void* const* p, const double* dv, const int* iv) const {
+        for (int q = 0; q < 6; q++)
+            if (key_ptr[q] != p[q] || key_i[q] != iv[q]) return false;
+        for (int q = 0; q < 3; q++)
+            if (key_d[q] != dv[q]) return false;
+        return exec != nullptr;
+    }
+    void release() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
+    }
+    ~SolveGraph() {
+        release();
+        for (cudaStream_t& s : side)
+            if (s) cudaStreamDestroy(s);
+    }
 };
 
 template <typename T>
@@ -30,6 +64,7 @@ struct SolverWork {
     unsigned int* ticket;
     Red2 red;
     SolverScalars* S;
+    SolveGraph* graph = nullptr;  // null: host-driven loop
 };
 
 // per-field scalars of one MPDATA call
@@ -53,6 +88,10 @@ struct MpdataWork {
     MpScalars* Mzero;  // all zero
 };
 
+// Jacobi-preconditioned BiCGSTAB (dynamics.f90:293-444) on x, b in the
+// pitched layout.  With w.graph set (and event profiling off) the whole solve
+// runs as one CUDA graph; otherwise the host launches iterations in chunks
+// and polls the device scalars between chunks.
 template <typename T>
 int solver_run(SolverWork<T>& w, const Dims& d, T* x, const T* b, const T* sw,
                const T* dzn, double tol, int itmax, int wo, int chunk,

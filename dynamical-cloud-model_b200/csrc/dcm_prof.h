@@ -15,6 +15,7 @@ enum ProfCat {
 
 struct Profiler {
     bool on = false;
+    bool capturing = false;  // launches are being captured into a graph
     std::vector<cudaEvent_t> pool;
     size_t used = 0;
     struct Rec { int cat; size_t e0, e1; };
@@ -43,6 +44,8 @@ struct Profiler {
         recs.clear();
         used = 0;
     }
+    // launches that ran inside a graph, counted from the device scalars
+    void add(int cat, long long n) { count[cat] += n; }
     void reset() {
         for (int c = 0; c < P_NCAT; c++) { ms[c] = 0; launches[c] = 0; count[c] = 0; }
         recs.clear();
@@ -61,8 +64,9 @@ struct ProfScope {
     size_t e0 = 0;
     cudaStream_t st;
     bool timed;
-    ProfScope(int c, cudaStream_t s) : cat(c), st(s), timed(g_prof && g_prof->on) {
-        if (g_prof) g_prof->count[c] += 1;  // launches are always counted
+    ProfScope(int c, cudaStream_t s)
+        : cat(c), st(s), timed(g_prof && g_prof->on && !g_prof->capturing) {
+        if (g_prof && !g_prof->capturing) g_prof->count[c] += 1;  // launches are always counted
         if (timed) {
             e0 = g_prof->used;
             cudaEventRecord(g_prof->get(), st);

@@ -56,6 +56,7 @@ struct SolverArgs {
     double tol;
     double sc_floor;  // max(||b||, sc_floor) scales the residual (0.01, :371)
     int nkt;          // k-chunks of a warp task
+    int max_updates;  // mixed form: reliable updates before DCM_E_NOCONV
 };
 
 // a_p exactly as set_mat_a forms it (dynamics.f90:93-95)
@@ -357,6 +358,7 @@ __device__ __forceinline__ void reduce_tail(const SolverArgs& a, double (&acc)[N
             S->status = 0;
             S->early = 0;
             S->done = 0;
+            S->rounds = 0;
             if (err < a.tol) {  // :382-383 early return
                 S->early = 1;
                 S->done = 1;
@@ -630,6 +632,93 @@ static void launch_iteration(const SolverArgs& a, const Coef<T>& c, SolverWork<T
     }
 }
 
+// ---- graph-driven loops ------------------------------------------------------
+// Condition of the WHILE node: one more round while the solve has not set
+// `done`.  The round budget bounds the loop whatever the scalars do: past it
+// the solve stops with DCM_E_TIMEOUT.
+__global__ void k_loop_cond(cudaGraphConditionalHandle h, SolverScalars* S, int max_rounds) {
+    unsigned go = S->done ? 0u : 1u;
+    if (go) {
+        if (S->rounds >= max_rounds) {
+            S->status = DCM_E_TIMEOUT;
+            S->done = 1;
+            go = 0u;
+        } else {
+            S->rounds = S->rounds + 1;
+        }
+    }
+    cudaGraphSetConditional(h, go);
+}
+
+// Condition of the IF/ELSE node of the mixed solve: reliable update or
+// another FP32 iteration.
+__global__ void k_branch_pause(cudaGraphConditionalHandle h, const SolverScalars* S) {
+    cudaGraphSetConditional(h, S->pause ? 1u : 0u);
+}
+
+namespace {
+
+bool ok(cudaError_t e) { return e == cudaSuccess; }
+
+// Add a conditional node after the work captured so far on `st` (which must
+// be capturing); the handle is created on the capturing graph first so that
+// kernels captured before the node can set it.
+bool capture_cond_handle(cudaStream_t st, cudaGraphConditionalHandle* h, unsigned dflt) {
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t cg = nullptr;
+    if (!ok(cudaStreamGetCaptureInfo(st, &cs, nullptr, &cg, nullptr, nullptr)) ||
+        cs != cudaStreamCaptureStatusActive)
+        return false;
+    return ok(cudaGraphConditionalHandleCreate(h, cg, dflt, 0));
+}
+bool capture_cond_node(cudaStream_t st, cudaGraphConditionalHandle h,
+                       cudaGraphConditionalNodeType type, unsigned size, cudaGraph_t* bodies) {
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t cg = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    if (!ok(cudaStreamGetCaptureInfo(st, &cs, nullptr, &cg, &deps, &nd)) ||
+        cs != cudaStreamCaptureStatusActive)
+        return false;
+    cudaGraphNodeParams p = {};
+    p.type = cudaGraphNodeTypeConditional;
+    p.conditional.handle = h;
+    p.conditional.type = type;
+    p.conditional.size = size;
+    cudaGraphNode_t node;
+    if (!ok(cudaGraphAddNode(&node, cg, deps, nd, &p))) return false;
+    for (unsigned q = 0; q < size; q++) bodies[q] = p.conditional.phGraph_out[q];
+    return ok(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
+}
+
+// capture launches into an existing (body) graph on a side stream
+template <typename F>
+bool capture_into(cudaStream_t side, cudaGraph_t body, F&& launches) {
+    if (!ok(cudaStreamBeginCaptureToGraph(side, body, nullptr, nullptr, 0,
+                                          cudaStreamCaptureModeRelaxed)))
+        return false;
+    launches(side);
+    cudaGraph_t out = body;
+    return ok(cudaStreamEndCapture(side, &out));
+}
+
+struct CaptureGuard {  // launches inside a capture are counted per run instead
+    CaptureGuard() {
+        if (g_prof) g_prof->capturing = true;
+    }
+    ~CaptureGuard() {
+        if (g_prof) g_prof->capturing = false;
+    }
+};
+
+bool side_streams(SolveGraph& G) {
+    for (cudaStream_t& s : G.side)
+        if (!s && !ok(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking))) return false;
+    return true;
+}
+
+}  // namespace
+
 template <typename T>
 int solver_run(SolverWork<T>& w, const Dims& d, T* x, const T* b, const T* sw, const T* dzn,
                double tol, int itmax, int wo, int chunk, cudaStream_t st, SolverScalars* host_S,
@@ -640,6 +729,7 @@ int solver_run(SolverWork<T>& w, const Dims& d, T* x, const T* b, const T* sw, c
     a.tol = tol;
     a.sc_floor = sc_floor;
     a.nkt = kchunks<T>(d);
+    a.max_updates = 0;
     const Coef<T> c = coef_of(w);
     SolverBufs B{};
     B.x = x;
@@ -647,6 +737,67 @@ int solver_run(SolverWork<T>& w, const Dims& d, T* x, const T* b, const T* sw, c
     B.out = w.r;
     B.out2 = w.cr;
     B.out3 = w.rh;
+    const int max_rounds = itmax + 1;
+    auto post_launch = [&](cudaStream_t s) {
+        if (post) {
+            ProfScope ps(P_POST, s);
+            k_bicg_post<T, T><<<interior_grid(d, d.kp), dim3(BX, BY), 0, s>>>(d, x, sw, dzn, w.S,
+                                                                              wo);
+        }
+    };
+    const bool use_graph = w.graph && !(g_prof && g_prof->on);
+    if (use_graph) {
+        SolveGraph& G = *w.graph;
+        const void* kp[6] = {x, b, sw, dzn, w.r, w.S};
+        const double kd[3] = {tol, sc_floor, 0.0};
+        const int ki[6] = {itmax, wo, post ? 1 : 0, (int)sizeof(T), d.ip * 4096 + d.jp, d.kp};
+        if (!G.matches(kp, kd, ki)) {
+            G.release();
+            if (!side_streams(G)) return DCM_E_CUDA;
+            CaptureGuard cg;
+            bool good = ok(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
+            cudaGraphConditionalHandle hw{};
+            cudaGraph_t body[1] = {nullptr};
+            if (good) {
+                sten<T, OP_SETUP, 0>(a, c, B, w, st, P_SETUP);
+                good = capture_cond_handle(st, &hw, 0);
+                if (good) k_loop_cond<<<1, 1, 0, st>>>(hw, w.S, max_rounds);
+                good = good && capture_cond_node(st, hw, cudaGraphCondTypeWhile, 1, body);
+                good = good && capture_into(G.side[0], body[0], [&](cudaStream_t s) {
+                           launch_iteration<T>(a, c, w, x, s);
+                           k_loop_cond<<<1, 1, 0, s>>>(hw, w.S, max_rounds);
+                       });
+                post_launch(st);
+            }
+            cudaGraph_t gr = nullptr;
+            const bool ended = ok(cudaStreamEndCapture(st, &gr));
+            G.graph = gr;
+            if (!good || !ended || !ok(cudaGraphInstantiate(&G.exec, gr, 0))) {
+                G.release();
+                cudaGetLastError();
+                return DCM_E_CUDA;
+            }
+            for (int q = 0; q < 6; q++) {
+                G.key_ptr[q] = kp[q];
+                G.key_i[q] = ki[q];
+            }
+            for (int q = 0; q < 3; q++) G.key_d[q] = kd[q];
+        }
+        if (!ok(cudaGraphLaunch(G.exec, st))) return DCM_E_CUDA;
+        cudaMemcpyAsync(host_S, w.S, sizeof(SolverScalars), cudaMemcpyDeviceToHost, st);
+        if (cudaStreamSynchronize(st) != cudaSuccess) return DCM_E_CUDA;
+        const long long r = host_S->rounds;
+        if (g_prof) {
+            g_prof->add(P_SETUP, 1);
+            g_prof->add(P_JACOBI, 6 * r);
+            g_prof->add(P_MATVEC, 2 * r);
+            g_prof->add(P_UPDATE, r);
+            g_prof->add(P_OTHER, r + 1);
+            if (post) g_prof->add(P_POST, 1);
+        }
+        if (launched_iters) *launched_iters = (int)r;
+        return host_S->status;
+    }
     sten<T, OP_SETUP, 0>(a, c, B, w, st, P_SETUP);
     if (cudaGetLastError() != cudaSuccess) return DCM_E_CUDA;
     int launched = 0;
@@ -659,10 +810,7 @@ int solver_run(SolverWork<T>& w, const Dims& d, T* x, const T* b, const T* sw, c
             launch_iteration<T>(a, c, w, x, st);
         if (cudaGetLastError() != cudaSuccess) return DCM_E_CUDA;
     }
-    if (post) {
-        ProfScope ps(P_POST, st);
-        k_bicg_post<T, T><<<interior_grid(d, d.kp), dim3(BX, BY), 0, st>>>(d, x, sw, dzn, w.S, wo);
-    }
+    post_launch(st);
     cudaMemcpyAsync(host_S, w.S, sizeof(SolverScalars), cudaMemcpyDeviceToHost, st);
     if (cudaStreamSynchronize(st) != cudaSuccess) return DCM_E_CUDA;
     if (launched_iters) *launched_iters = launched;
@@ -751,6 +899,7 @@ __global__ void __launch_bounds__(256) k_ru_residual(SolverArgs a, Coef<double> 
             S->it = 0;
             S->status = 0;
             S->updates = 0;
+            S->rounds = 0;
             S->alf = 1.0;  // :385-387
             S->omg = 1.0;
             S->nrm = 1.0;
@@ -766,6 +915,9 @@ __global__ void __launch_bounds__(256) k_ru_residual(SolverArgs a, Coef<double> 
             S->early = FIRST ? 1 : 0;
         } else if (!(err == err)) {
             S->status = DCM_E_NONFINITE;
+            S->done = 1;
+        } else if (!FIRST && S->updates >= a.max_updates) {
+            S->status = DCM_E_NOCONV;
             S->done = 1;
         } else {
             S->rho = s[2];  // (r, cr) of the replaced residual
@@ -787,6 +939,23 @@ __global__ void __launch_bounds__(256) k_ru_add(Dims d, double* __restrict__ x,
     dx[o] = 0.0f;
 }
 
+// reliable-update controls of the FP32 scalars (start of a mixed solve)
+__global__ void k_ru_begin(SolverScalars* S, double delta) {
+    S->ru = 1;
+    S->delta = delta;
+    S->pause = 0;
+}
+
+// end of a mixed solve: the FP32 scalars back to plain mode, the outcome into
+// the FP64 scalars that the halo fix-up (k_bicg_post) reads
+__global__ void k_ru_end(SolverScalars* Sin, SolverScalars* Sout) {
+    Sin->ru = 0;
+    Sout->early = Sin->early;
+    Sout->status = Sin->status;
+    Sout->it = Sin->it;
+    Sout->err = Sin->err;
+}
+
 int refine_run(SolverWork<float>& wf, SolverWork<double>& wd, const Dims& d, double* x,
                const double* b, const float* sw, const double* dzn, float* dx, double tol,
                double delta, int itmax, int max_updates, cudaStream_t st,
@@ -797,6 +966,7 @@ int refine_run(SolverWork<float>& wf, SolverWork<double>& wd, const Dims& d, dou
     a.tol = tol;
     a.sc_floor = 0.01;
     a.nkt = (d.kp + BX - 1) / BX;  // scalar warp tasks of the FP64 residual
+    a.max_updates = max_updates;
     SolverArgs af = a;             // vector warp tasks of the FP32 iterations
     af.nkt = kchunks<float>(d);
     Coef<double> cd;
@@ -805,67 +975,112 @@ int refine_run(SolverWork<float>& wf, SolverWork<double>& wd, const Dims& d, dou
     static int g = 0;
     if (!g) g = persistent_grid(k_ru_residual<false>);
     const dim3 gi = interior_grid(d, d.kp), bl(BX, BY);
-    if (cudaMemsetAsync(dx, 0, d.n() * sizeof(float), st) != cudaSuccess) return DCM_E_CUDA;
-    // reliable-update controls live in the FP32 solve's scalars
-    hS_in->ru = 1;
-    hS_in->delta = delta;
-    cudaMemcpyAsync(&wf.S->ru, &hS_in->ru, sizeof(int), cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(&wf.S->delta, &hS_in->delta, sizeof(double), cudaMemcpyHostToDevice, st);
-    {
-        ProfScope ps(P_SETUP, st);
-        k_ru_residual<true><<<g, bl, 0, st>>>(a, cd, cf, x, b, wf.r, wf.rh, wf.cr, wd.red, wf.S);
-    }
-    int launched = 0, status = DCM_OK;
-    for (;;) {
-        cudaMemcpyAsync(hS_in, wf.S, sizeof(SolverScalars), cudaMemcpyDeviceToHost, st);
-        if (cudaStreamSynchronize(st) != cudaSuccess) return DCM_E_CUDA;
-        if (hS_in->done) break;
-        if (hS_in->pause) {
-            if (hS_in->updates >= max_updates) {
-                status = DCM_E_NOCONV;
-                break;
-            }
-            {
-                ProfScope ps(P_UPDATE, st);
-                k_ru_add<<<gi, bl, 0, st>>>(d, x, dx);
-            }
-            {
-                ProfScope ps(P_SETUP, st);
-                k_ru_residual<false><<<g, bl, 0, st>>>(a, cd, cf, x, b, wf.r, wf.rh, wf.cr, wd.red,
-                                                       wf.S);
-            }
-            if (std::getenv("DCM_DEBUG")) {
-                cudaMemcpyAsync(hS_in, wf.S, sizeof(SolverScalars), cudaMemcpyDeviceToHost, st);
-                cudaStreamSynchronize(st);
-                std::fprintf(stderr, "reliable update %d at it %d: FP64 err %.3e\n",
-                             hS_in->updates, hS_in->it, hS_in->err);
-            }
-            continue;
+    auto begin = [&](cudaStream_t s) {
+        cudaMemsetAsync(dx, 0, d.n() * sizeof(float), s);
+        k_ru_begin<<<1, 1, 0, s>>>(wf.S, delta);
+        ProfScope ps(P_SETUP, s);
+        k_ru_residual<true><<<g, bl, 0, s>>>(a, cd, cf, x, b, wf.r, wf.rh, wf.cr, wd.red, wf.S);
+    };
+    auto update = [&](cudaStream_t s) {  // x64 += dx32; FP64 residual
+        {
+            ProfScope ps(P_UPDATE, s);
+            k_ru_add<<<gi, bl, 0, s>>>(d, x, dx);
         }
-        if (launched >= itmax) {
-            status = DCM_E_NOCONV;
-            break;
+        ProfScope ps(P_SETUP, s);
+        k_ru_residual<false><<<g, bl, 0, s>>>(a, cd, cf, x, b, wf.r, wf.rh, wf.cr, wd.red, wf.S);
+    };
+    auto finish = [&](cudaStream_t s) {
+        {
+            // the correction accumulated since the last update (zero after one)
+            ProfScope ps(P_UPDATE, s);
+            k_ru_add<<<gi, bl, 0, s>>>(d, x, dx);
         }
-        for (int q = 0; q < 4 && launched < itmax; q++, launched++)
-            launch_iteration<float>(af, cf, wf, dx, st);
-        if (cudaGetLastError() != cudaSuccess) return DCM_E_CUDA;
+        k_ru_end<<<1, 1, 0, s>>>(wf.S, wd.S);
+        ProfScope ps(P_POST, s);
+        k_bicg_post<double, float><<<gi, bl, 0, s>>>(d, x, sw, dzn, wd.S, 1);
+    };
+    const int max_rounds = itmax + max_updates + 1;
+    const bool use_graph = wf.graph && !(g_prof && g_prof->on);
+    if (use_graph) {
+        SolveGraph& G = *wf.graph;
+        const void* kp[6] = {x, b, sw, dzn, dx, wf.S};
+        const double kd[3] = {tol, delta, 0.0};
+        const int ki[6] = {itmax, max_updates, 1, 0, d.ip * 4096 + d.jp, d.kp};
+        if (!G.matches(kp, kd, ki)) {
+            G.release();
+            if (!side_streams(G)) return DCM_E_CUDA;
+            CaptureGuard cgd;
+            bool good = ok(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
+            cudaGraphConditionalHandle hw{};
+            cudaGraph_t body[1] = {nullptr};
+            if (good) {
+                begin(st);
+                good = capture_cond_handle(st, &hw, 0);
+                if (good) k_loop_cond<<<1, 1, 0, st>>>(hw, wf.S, max_rounds);
+                good = good && capture_cond_node(st, hw, cudaGraphCondTypeWhile, 1, body);
+                // loop body: branch on pause -> reliable update | FP32 iteration
+                good = good && capture_into(G.side[0], body[0], [&](cudaStream_t s) {
+                           cudaGraphConditionalHandle hb{};
+                           cudaGraph_t br[2] = {nullptr, nullptr};
+                           bool g2 = capture_cond_handle(s, &hb, 0);
+                           if (g2) k_branch_pause<<<1, 1, 0, s>>>(hb, wf.S);
+                           g2 = g2 && capture_cond_node(s, hb, cudaGraphCondTypeIf, 2, br);
+                           g2 = g2 && capture_into(G.side[1], br[0], update);
+                           g2 = g2 && capture_into(G.side[1], br[1], [&](cudaStream_t s2) {
+                                    launch_iteration<float>(af, cf, wf, dx, s2);
+                                });
+                           k_loop_cond<<<1, 1, 0, s>>>(hw, wf.S, max_rounds);
+                           if (!g2) good = false;
+                       });
+                finish(st);
+            }
+            cudaGraph_t gr = nullptr;
+            const bool ended = ok(cudaStreamEndCapture(st, &gr));
+            G.graph = gr;
+            if (!good || !ended || !ok(cudaGraphInstantiate(&G.exec, gr, 0))) {
+                G.release();
+                cudaGetLastError();
+                return DCM_E_CUDA;
+            }
+            for (int q = 0; q < 6; q++) {
+                G.key_ptr[q] = kp[q];
+                G.key_i[q] = ki[q];
+            }
+            for (int q = 0; q < 3; q++) G.key_d[q] = kd[q];
+        }
+        if (!ok(cudaGraphLaunch(G.exec, st))) return DCM_E_CUDA;
+    } else {
+        begin(st);
+        int launched = 0;
+        for (int round = 0;; round++) {
+            cudaMemcpyAsync(hS_in, wf.S, sizeof(SolverScalars), cudaMemcpyDeviceToHost, st);
+            if (cudaStreamSynchronize(st) != cudaSuccess) return DCM_E_CUDA;
+            if (hS_in->done || round > max_rounds) break;
+            if (hS_in->pause) {
+                update(st);
+                continue;
+            }
+            if (launched >= itmax) break;
+            for (int q = 0; q < 4 && launched < itmax; q++, launched++)
+                launch_iteration<float>(af, cf, wf, dx, st);
+            if (cudaGetLastError() != cudaSuccess) return DCM_E_CUDA;
+        }
+        finish(st);
     }
-    if (status == DCM_OK) status = hS_in->status;
-    // the correction accumulated since the last update (zero after one)
-    k_ru_add<<<gi, bl, 0, st>>>(d, x, dx);
-    // leave the FP32 scalars in plain mode for any later use
-    hS_in->ru = 0;
-    cudaMemcpyAsync(&wf.S->ru, &hS_in->ru, sizeof(int), cudaMemcpyHostToDevice, st);
-    hS_out->early = hS_in->early;
-    hS_out->status = status;
-    hS_out->it = hS_in->it;
-    hS_out->err = hS_in->err;
-    cudaMemcpyAsync(wd.S, hS_out, sizeof(SolverScalars), cudaMemcpyHostToDevice, st);
-    {
-        ProfScope ps(P_POST, st);
-        k_bicg_post<double, float><<<gi, bl, 0, st>>>(d, x, sw, dzn, wd.S, 1);
-    }
+    cudaMemcpyAsync(hS_in, wf.S, sizeof(SolverScalars), cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(hS_out, wd.S, sizeof(SolverScalars), cudaMemcpyDeviceToHost, st);
     if (cudaStreamSynchronize(st) != cudaSuccess) return DCM_E_CUDA;
+    int status = hS_out->status;
+    if (status == DCM_OK && !hS_in->done) status = DCM_E_NOCONV;  // host loop ran out
+    if (use_graph && g_prof) {
+        const long long r = hS_in->rounds, u = hS_in->updates, itr = r - u;
+        g_prof->add(P_SETUP, u + 1);
+        g_prof->add(P_JACOBI, 6 * itr);
+        g_prof->add(P_MATVEC, 2 * itr);
+        g_prof->add(P_UPDATE, itr + u + 1);
+        g_prof->add(P_POST, 1);
+        g_prof->add(P_OTHER, 2 * r + 3);
+    }
     if (rs) {
         rs->outer = hS_in->updates;
         rs->inner = hS_in->it;

@@ -243,6 +243,15 @@ int dcm_horizontal_means_noalloc(int ip, int jp, int kp, const double *u,
 #define DCM_PROF_NCAT 17
 int dcm_profile_enable(dcm_handle *h, int on);
 int dcm_profile_read(dcm_handle *h, double *ms, long long *launches, int ncat);
+/* Pressure-solve driver (default 1).  1: each solve is one CUDA graph whose
+ * iteration loop is a conditional WHILE node driven by the device scalars
+ * (and, in the mixed form, an IF/ELSE node choosing an FP64 reliable update
+ * or an FP32 iteration), captured once and relaunched while its arguments
+ * stay the same.  0: the host launches iterations in chunks of 4 and polls
+ * the device scalars between chunks.  Both launch the same kernels in the
+ * same order and give bit-identical results; while event timing is enabled
+ * the host-driven loop is used. */
+int dcm_solver_graphs(dcm_handle *h, int on);
 
 #ifdef __cplusplus
 }

@@ -63,3 +63,25 @@ def test_mixed_tracers(dcm, orc):
     print("tracers", {k: f"{v:.2e}" for k, v in e.items()})
     bad = {k: v for k, v in e.items() if not v <= MIXED_TOL}
     assert not bad, bad
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_graph_and_host_loops_agree(dcm, precision):
+    """The graph-driven solve (conditional WHILE / IF nodes) and the
+    host-polled loop launch the same kernels in the same order: identical
+    fields and iteration counts, step after step."""
+    c = small_bubble()
+    out = []
+    for graphs in (True, False):
+        core = dcm.DynamicalCore(c.grid)
+        core.solver_graphs(graphs)
+        core.upload_state(c.state, c.dt, ptol=c.ptol, kord=c.kord, monotone=c.monotone,
+                          precision=precision)
+        core.driver_start()
+        its = [core.step(1).iters_last for _ in range(3)]
+        out.append((its, core.download_state()))
+        core.close()
+    (ia, fa), (ib, fb) = out
+    assert ia == ib
+    for n in ("u", "v", "w", "th", "p", "psrc"):
+        assert np.array_equal(fa[n], fb[n]), n
