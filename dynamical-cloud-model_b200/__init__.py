@@ -63,7 +63,8 @@ class _Fields(C.Structure):
 
 class StepStats(C.Structure):
     _fields_ = [("steps", C.c_int), ("iters_last", C.c_int), ("iters_total", C.c_longlong),
-                ("err_last", C.c_double), ("ms_total", C.c_double)]
+                ("err_last", C.c_double), ("ms_total", C.c_double),
+                ("updates_last", C.c_int), ("restarts_last", C.c_int)]
 
 
 _lib = None

@@ -153,7 +153,13 @@ class State:
     extra: dict = field(default_factory=dict)
 
     def copy(self):
-        c = State(**{k: (None if getattr(self, k) is None else getattr(self, k).copy(order="K"))
+        def cp(a):
+            if a is None:
+                return None
+            if isinstance(a, list):
+                return [x.copy(order="K") for x in a]
+            return a.copy(order="K")
+        c = State(**{k: cp(getattr(self, k))
                      for k in ("u", "v", "w", "zu", "zv", "zw", "tu", "tv", "tw", "th", "p",
                                "q")})
         c.extra = dict(self.extra)

@@ -1217,6 +1217,8 @@ extern "C" int dcm_step(dcm_handle* h, int nsteps, dcm_step_stats* stats) {
         stats->iters_total = tot;
         stats->err_last = h->last_err;
         stats->ms_total = ms;
+        stats->updates_last = h->prec ? h->last_refine.outer : 0;
+        stats->restarts_last = h->prec ? h->last_refine.restarts : 0;
     }
     return rc;
 }

@@ -18,9 +18,16 @@ struct SolverScalars {
     // iteration when its residual has fallen by `delta` since the last FP64
     // residual (ru_norm) or below the tolerance
     double ru_norm, delta;
-    int ru, pause, updates, pad;
-    int rounds;  // loop rounds of a graph-driven solve (bounded, see k_loop_cond)
-    int pad2;
+    int ru, pause, updates;
+    // breakdown of the FP32 recursion in the mixed form: 1 = restart from the
+    // FP64 residual keeping the FP32 correction, 2 = its vectors went
+    // non-finite, drop the correction since the last update
+    int restart;
+    int rounds;    // loop rounds of a graph-driven solve (bounded, see k_loop_cond)
+    int fresh;     // the next iteration starts a recursion (p = v1 = 0)
+    int restarts;  // restarts of this solve
+    int cycle_it;  // FP32 iterations since the last FP64 update
+    double crnorm;  // (cr, cr) of the shadow residual
 };
 
 // One pressure solve captured as a CUDA graph: the iteration loop is a
@@ -99,7 +106,7 @@ int solver_run(SolverWork<T>& w, const Dims& d, T* x, const T* b, const T* sw,
                double sc_floor = 0.01, bool post = true);
 
 struct RefineStats {
-    int outer, inner;
+    int outer, inner, restarts;
     double err;
 };
 

@@ -37,6 +37,7 @@
 // moves 41 field passes instead of 39.
 #include <cstdio>
 #include <cstdlib>
+#include <type_traits>
 
 #include "dcm_internal.h"
 #include "dcm_prof.h"
@@ -57,6 +58,7 @@ struct SolverArgs {
     double sc_floor;  // max(||b||, sc_floor) scales the residual (0.01, :371)
     int nkt;          // k-chunks of a warp task
     int max_updates;  // mixed form: reliable updates before DCM_E_NOCONV
+    int max_cycle;    // mixed form: FP32 iterations between updates before a restart
 };
 
 // a_p exactly as set_mat_a forms it (dynamics.f90:93-95)
@@ -265,9 +267,21 @@ __device__ __forceinline__ void sten_task(const StenCtx<T, OP, MODE>& C, int kc,
         xd = kk == 1 ? xc[q] : xd;
         xu = kk == kp ? xc[q] : xu;
         ap[q] = sij - au[q] - ad[q];  // a_p, dynamics.f90:93-95 (same order)
-        // mat_ax, dynamics.f90:219-222 (a_c = 0)
-        Ax[q] = aw * xw[q] + ae * xe[q] + as * xs[q] + an * xn[q] + ad[q] * xd + au[q] * xu +
-                ap[q] * xc[q] + T(0);
+        if constexpr (std::is_same<T, double>::value) {
+            // mat_ax, dynamics.f90:219-222 (a_c = 0), in the reference's form
+            Ax[q] = aw * xw[q] + ae * xe[q] + as * xs[q] + an * xn[q] + ad[q] * xd +
+                    au[q] * xu + ap[q] * xc[q] + T(0);
+        } else {
+            // FP32 (mixed form): the same operator as differences to the
+            // centre.  a_p rounded in FP32 no longer cancels its neighbours
+            // exactly, which would give the singular (Neumann / periodic)
+            // operator a spurious eigenvalue ~1e-7 a_p along the constants;
+            // the Krylov recursion then stalls and drifts in p's constant.
+            // In difference form constants are an exact null vector.
+            const T c0 = xc[q];
+            Ax[q] = aw * (xw[q] - c0) + ae * (xe[q] - c0) + as * (xs[q] - c0) +
+                    an * (xn[q] - c0) + ad[q] * (xd - c0) + au[q] * (xu - c0);
+        }
     }
     const SolverBufs& B = C.B;
     T* __restrict__ out = (T*)B.out;
@@ -375,12 +389,19 @@ __device__ __forceinline__ void reduce_tail(const SolverArgs& a, double (&acc)[N
         } else if (OP == OP_MATP) {
             S->nrm = s[0];             // :401
             S->alf = S->rho / S->nrm;  // :403
+            if (S->ru && !(isfinite(S->alf) && S->nrm != 0.0)) {
+                S->restart = isfinite(s[0]) ? 1 : 2;  // FP32 breakdown: restart
+                S->pause = 1;
+            }
         } else if (OP == OP_MATC) {
             S->tt = s[0];
             S->ts = s[NV - 1];
             S->omg = S->ts / S->tt;               // :412
             const double tiny = (double)1.e-16f;  // default-real literal, :321
-            if (fabs(S->omg) < tiny) {            // :414-417
+            if (S->ru && !(fabs(S->omg) >= tiny)) {
+                S->restart = (isfinite(s[0]) && isfinite(s[NV - 1])) ? 1 : 2;
+                S->pause = 1;
+            } else if (fabs(S->omg) < tiny) {     // :414-417
                 S->status = DCM_E_BREAKDOWN;
                 S->it = S->it + 1;
                 S->done = 1;
@@ -409,7 +430,7 @@ __global__ void __launch_bounds__(256) k_sten(SolverArgs a, Coef<T> c, SolverBuf
     C.bet = (T)S->bet;
     C.omg = (T)S->omg;
     C.alf = (T)S->alf;
-    C.first = S->it == 0;
+    C.first = S->it == 0 || S->fresh;
     const Dims& d = a.d;
     double acc[NV];
 #pragma unroll
@@ -486,7 +507,18 @@ __global__ void __launch_bounds__(256) k_bicg_update(SolverArgs a, Coef<T> c,
         const double err = sqrt(s[0]) / S->sc_err;  // :423
         S->err = err;
         S->nrm = S->rho;  // :425
-        if (S->ru && (err < a.tol || sqrt(s[0]) < S->delta * S->ru_norm)) {
+        S->fresh = 0;
+        if (S->ru && !(isfinite(s[0]) && isfinite(s[1]))) {
+            S->restart = 2;  // the FP32 vectors went non-finite
+            S->pause = 1;
+        } else if (S->ru && !(err < a.tol) &&
+                   (!(fabs(s[1]) > 1e-10 * sqrt(s[0] * S->crnorm)) ||
+                    ++S->cycle_it > a.max_cycle)) {
+            // (r, cr) collapsed, or the FP32 recursion stagnated: restart
+            // from the FP64 residual with cr = r
+            S->restart = 1;
+            S->pause = 1;
+        } else if (S->ru && (err < a.tol || sqrt(s[0]) < S->delta * S->ru_norm)) {
             // reliable update (mixed-precision form): the host replaces r by
             // the FP64 residual before the iteration continues
             S->pause = 1;
@@ -730,6 +762,7 @@ int solver_run(SolverWork<T>& w, const Dims& d, T* x, const T* b, const T* sw, c
     a.sc_floor = sc_floor;
     a.nkt = kchunks<T>(d);
     a.max_updates = 0;
+    a.max_cycle = 0;
     const Coef<T> c = coef_of(w);
     SolverBufs B{};
     B.x = x;
@@ -855,6 +888,8 @@ __global__ void __launch_bounds__(256) k_ru_residual(SolverArgs a, Coef<double> 
     const int ip = d.ip, jp = d.jp, kp = d.kp;
     double acc[3] = {0.0, 0.0, 0.0};
     const int lane = threadIdx.x;
+    // a first residual, or a restart after a breakdown: cr = r
+    const bool reset = FIRST || S->restart != 0;
     for (TaskIter t(blockIdx.x * blockDim.y + threadIdx.y, gridDim.x * blockDim.y, a.nkt, jp);
          t.i <= ip; t.next()) {
         const int j = 1 + t.jr, i = t.i;
@@ -879,7 +914,7 @@ __global__ void __launch_bounds__(256) k_ru_residual(SolverArgs a, Coef<double> 
         r32[o] = rf;
         rh32[o] = rf / diag_ap(cf, k, j, i);
         float crf;
-        if (FIRST) {
+        if (reset) {
             cr32[o] = rf;
             crf = rf;
         } else {
@@ -900,9 +935,8 @@ __global__ void __launch_bounds__(256) k_ru_residual(SolverArgs a, Coef<double> 
             S->status = 0;
             S->updates = 0;
             S->rounds = 0;
-            S->alf = 1.0;  // :385-387
-            S->omg = 1.0;
-            S->nrm = 1.0;
+            S->restarts = 0;
+            S->fresh = 0;
         }
         const double err = sqrt(s[1]) / S->sc_err;
         S->err = err;
@@ -910,6 +944,7 @@ __global__ void __launch_bounds__(256) k_ru_residual(SolverArgs a, Coef<double> 
         S->pause = 0;
         S->done = 0;
         S->early = 0;
+        S->cycle_it = 0;
         if (err < a.tol) {
             S->done = 1;
             S->early = FIRST ? 1 : 0;
@@ -920,22 +955,38 @@ __global__ void __launch_bounds__(256) k_ru_residual(SolverArgs a, Coef<double> 
             S->status = DCM_E_NOCONV;
             S->done = 1;
         } else {
+            if (reset) {
+                // BiCGSTAB from r with cr = r: alf = omg = nrm = 1 (:385-387);
+                // after a breakdown the next iteration also starts with p = v1 = 0
+                S->alf = 1.0;
+                S->omg = 1.0;
+                S->nrm = 1.0;
+                S->crnorm = s[2];
+                if (!FIRST) {
+                    S->restarts = S->restarts + 1;
+                    S->fresh = 1;
+                }
+            }
             S->rho = s[2];  // (r, cr) of the replaced residual
             S->bet = (S->rho / S->nrm) * (S->alf / S->omg);
             if (!FIRST) S->updates = S->updates + 1;
         }
+        S->restart = 0;
     }
 }
 
 // x (FP64) += dx (FP32); dx = 0 (interior)
 __global__ void __launch_bounds__(256) k_ru_add(Dims d, double* __restrict__ x,
-                                                float* __restrict__ dx) {
+                                                float* __restrict__ dx,
+                                                const SolverScalars* S) {
     const int k = 1 + blockIdx.x * BX + threadIdx.x;
     const int j = 1 + blockIdx.y * BY + threadIdx.y;
     const int i = 1 + blockIdx.z;
     if (k > d.kp || j > d.jp) return;
     const int o = d.at(k, j, i);
-    x[o] = x[o] + (double)dx[o];
+    // after a non-finite breakdown the correction since the last update is
+    // dropped (x64 keeps its last FP64-checked value)
+    if (S->restart != 2) x[o] = x[o] + (double)dx[o];
     dx[o] = 0.0f;
 }
 
@@ -967,6 +1018,7 @@ int refine_run(SolverWork<float>& wf, SolverWork<double>& wd, const Dims& d, dou
     a.sc_floor = 0.01;
     a.nkt = (d.kp + BX - 1) / BX;  // scalar warp tasks of the FP64 residual
     a.max_updates = max_updates;
+    a.max_cycle = 250;
     SolverArgs af = a;             // vector warp tasks of the FP32 iterations
     af.nkt = kchunks<float>(d);
     Coef<double> cd;
@@ -984,7 +1036,7 @@ int refine_run(SolverWork<float>& wf, SolverWork<double>& wd, const Dims& d, dou
     auto update = [&](cudaStream_t s) {  // x64 += dx32; FP64 residual
         {
             ProfScope ps(P_UPDATE, s);
-            k_ru_add<<<gi, bl, 0, s>>>(d, x, dx);
+            k_ru_add<<<gi, bl, 0, s>>>(d, x, dx, wf.S);
         }
         ProfScope ps(P_SETUP, s);
         k_ru_residual<false><<<g, bl, 0, s>>>(a, cd, cf, x, b, wf.r, wf.rh, wf.cr, wd.red, wf.S);
@@ -993,7 +1045,7 @@ int refine_run(SolverWork<float>& wf, SolverWork<double>& wd, const Dims& d, dou
         {
             // the correction accumulated since the last update (zero after one)
             ProfScope ps(P_UPDATE, s);
-            k_ru_add<<<gi, bl, 0, s>>>(d, x, dx);
+            k_ru_add<<<gi, bl, 0, s>>>(d, x, dx, wf.S);
         }
         k_ru_end<<<1, 1, 0, s>>>(wf.S, wd.S);
         ProfScope ps(P_POST, s);
@@ -1084,6 +1136,7 @@ int refine_run(SolverWork<float>& wf, SolverWork<double>& wd, const Dims& d, dou
     if (rs) {
         rs->outer = hS_in->updates;
         rs->inner = hS_in->it;
+        rs->restarts = hS_in->restarts;
         rs->err = hS_in->err;
     }
     return status;

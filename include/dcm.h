@@ -198,6 +198,10 @@ typedef struct {
     long long iters_total;  /* summed over the call                       */
     double err_last;        /* final relative residual of the last solve  */
     double ms_total;        /* device time of the call (CUDA events)      */
+    int updates_last;       /* precision 1: FP64 reliable updates of the
+                               last solve (0 for FP64)                     */
+    int restarts_last;      /* precision 1: of those, restarts after a
+                               breakdown of the FP32 recursion             */
 } dcm_step_stats;
 
 /* Upload the driver state; roles as in dcm_fields. */
