@@ -36,6 +36,8 @@ __device__ __forceinline__ float small_of<float>() { return 1e-30f; }
 // ---- positive-definite shift: min over the whole array or the interior ---
 // mpdata_3d takes minval over the whole array including halos (:275);
 // mpdata_vec_3d over the interior only (:1307).
+// Each block strides over the i-planes (blockIdx.z, step gridDim.z), so the
+// grid has a few thousand blocks rather than one per plane.
 template <typename T, bool INTERIOR>
 __global__ void __launch_bounds__(256) k_min(Dims d, const T* __restrict__ a,
                                              double lbc, double ubc,
@@ -46,9 +48,14 @@ __global__ void __launch_bounds__(256) k_min(Dims d, const T* __restrict__ a,
     double v[1] = {1e300};
     const int k = (INTERIOR ? 1 : 0) + blockIdx.x * BX + threadIdx.x;
     const int j = (INTERIOR ? 1 : 0) + blockIdx.y * BY + threadIdx.y;
-    const int i = (INTERIOR ? 1 : 0) + blockIdx.z;
     const int kmax = INTERIOR ? d.kp : d.kp + 1, jmax = INTERIOR ? d.jp : d.jp + 1;
-    if (k <= kmax && j <= jmax) v[0] = (double)a[d.at(k, j, i)];
+    const int imax = INTERIOR ? d.ip : d.ip + 1;
+    if (k <= kmax && j <= jmax) {
+        T m = a[d.at(k, j, (INTERIOR ? 1 : 0) + blockIdx.z)];
+        for (int i = (INTERIOR ? 1 : 0) + blockIdx.z + gridDim.z; i <= imax; i += gridDim.z)
+            m = fmin(m, a[d.at(k, j, i)]);
+        v[0] = (double)m;
+    }
     block_reduce<R_MIN, 1>(v, smem);
     const unsigned int nb = gridDim.x * gridDim.y * gridDim.z;
     if (publish_partials<1>(v, partials, ticket, nb)) {
@@ -169,7 +176,7 @@ __global__ void __launch_bounds__(256) k_upwind(Dims d, Metrics<T> mt, T dt,
 
 // ---- antidiffusive velocities (:320-505) ------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(256) k_antidiff(Dims d, Metrics<T> mt, T dt,
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_antidiff(Dims d, Metrics<T> mt, T dt,
                                                   Vel<T> Vt,
                                                   const T* __restrict__ pso,
                                                   VelOut<T> out,
@@ -417,13 +424,13 @@ int mpdata_run(MpdataWork<T>& w, const Dims& d, const Metrics<T>& mt, T dt,
     for (int q = 0; q < nq; q++) {
         if (vec)
             { ProfScope ps_(P_MPMIN, st);
-            k_min<T, true><<<g, b, 0, st>>>(d, psi_in[q], lbc[q], ubc[q], w.partials, w.ticket,
-                                            w.M + q);
+            k_min<T, true><<<dim3(g.x, g.y, min(g.z, 16u)), b, 0, st>>>(
+                d, psi_in[q], lbc[q], ubc[q], w.partials, w.ticket, w.M + q);
             }
         else
             { ProfScope ps_(P_MPMIN, st);
-            k_min<T, false><<<gf, b, 0, st>>>(d, psi_in[q], lbc[q], ubc[q], w.partials, w.ticket,
-                                              w.M + q);
+            k_min<T, false><<<dim3(gf.x, gf.y, min(gf.z, 16u)), b, 0, st>>>(
+                d, psi_in[q], lbc[q], ubc[q], w.partials, w.ticket, w.M + q);
             }
     }
     const MpScalars* gate = w.M;
