@@ -61,6 +61,11 @@ class _Fields(C.Structure):
                                    "vbar", "wbar", "thbar", "qbar")]
 
 
+class EnsembleStats(C.Structure):
+    _fields_ = [("steps", C.c_int), ("iters_total", C.c_longlong), ("iters_max_last", C.c_int),
+                ("ms_total", C.c_double)]
+
+
 class StepStats(C.Structure):
     _fields_ = [("steps", C.c_int), ("iters_last", C.c_int), ("iters_total", C.c_longlong),
                 ("err_last", C.c_double), ("ms_total", C.c_double),
@@ -111,11 +116,18 @@ def library():
             "dcm_profile_enable": [P, C.c_int],
             "dcm_profile_read": [P, _dp, C.POINTER(C.c_longlong), C.c_int],
             "dcm_solver_graphs": [P, C.c_int],
+            "dcm_tune": [P, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)],
+            "dcm_ensemble_create": [C.c_int, C.c_void_p, C.c_int, C.POINTER(C.c_void_p)],
+            "dcm_ensemble_destroy": [P],
+            "dcm_ensemble_member": [P, C.c_int, C.POINTER(C.c_void_p)],
+            "dcm_ensemble_step": [P, C.c_int, C.POINTER(EnsembleStats)],
+            "dcm_ensemble_last_error": [P],
         }
         for name, args in sig.items():
             f = getattr(lib, name)
             f.argtypes = args
-            f.restype = C.c_char_p if name in ("dcm_status_string", "dcm_last_error") else C.c_int
+            f.restype = C.c_char_p if name in ("dcm_status_string", "dcm_last_error",
+                                               "dcm_ensemble_last_error") else C.c_int
         _lib = lib
     return _lib
 
@@ -127,7 +139,9 @@ EXPORTS = ("dcm_create", "dcm_destroy", "dcm_status_string", "dcm_last_error",
            "dcm_divergence_calc", "dcm_advance_scalar_fields_3d", "dcm_exchange_full",
            "dcm_exchange_along_dim", "dcm_exchange_along_dim_wo", "dcm_state_upload",
            "dcm_driver_start", "dcm_step", "dcm_state_download", "dcm_profile_enable",
-           "dcm_profile_read", "dcm_horizontal_means_noalloc", "dcm_solver_graphs")
+           "dcm_profile_read", "dcm_horizontal_means_noalloc", "dcm_solver_graphs", "dcm_tune",
+           "dcm_ensemble_create", "dcm_ensemble_destroy", "dcm_ensemble_member",
+           "dcm_ensemble_step", "dcm_ensemble_last_error")
 
 PROF_CLASSES = ("setup", "jacobi", "matvec", "update", "post", "means", "sources", "rhs",
                 "adv_ref", "mp_shift", "upwind", "antidiff", "beta", "limit", "restore",
@@ -152,6 +166,13 @@ def _field(a, shape):
     return a.ctypes.data_as(_dp)
 
 
+def _grid_struct(grid):
+    keep = [np.ascontiguousarray(getattr(grid, n), dtype=np.float64)
+            for n in ("dx", "dxn", "dy", "dyn", "dz", "dzn", "rhoa", "rhoan", "theta", "thetan",
+                      "x", "y", "z")]
+    return keep, _Grid(grid.ip, grid.jp, grid.kp, *[a.ctypes.data_as(_dp) for a in keep])
+
+
 def check_decomposition(dims):
     """mpi_cart_initialise check: only a 1 x 1 x 1 process grid runs here."""
     d = (C.c_int * 3)(*dims)
@@ -164,25 +185,35 @@ class DynamicalCore:
     """One device handle for one grid (the module state of d_solver lives
     here: the stencil coefficients and the bicgstab first-call flag)."""
 
-    def __init__(self, grid, device=0):
+    def __init__(self, grid, device=0, _handle=None):
         self.lib = library()
         self.grid = grid
         self.shape = (grid.kp + 2, grid.jp + 2, grid.ip + 2)
-        self._keep = [np.ascontiguousarray(getattr(grid, n), dtype=np.float64)
-                      for n in ("dx", "dxn", "dy", "dyn", "dz", "dzn", "rhoa", "rhoan", "theta",
-                                "thetan", "x", "y", "z")]
-        g = _Grid(grid.ip, grid.jp, grid.kp, *[a.ctypes.data_as(_dp) for a in self._keep])
+        self._state_keep = None
+        self._owned = _handle is None
+        if _handle is not None:  # a member handle owned by an Ensemble
+            self.h = _handle
+            return
+        self._keep, g = _grid_struct(grid)
         h = C.c_void_p()
         st = self.lib.dcm_create(C.byref(g), device, C.byref(h))
         if st:
             raise DCMError(st, self.lib.dcm_status_string(st).decode())
         self.h = h
-        self._state_keep = None
 
     def close(self):
         if getattr(self, "h", None):
-            self.lib.dcm_destroy(self.h)
+            if self._owned:
+                self.lib.dcm_destroy(self.h)
             self.h = None
+
+    def tune(self, precision=1, use_cache=True):
+        """Autotune the solver launch shape for this grid (dcm_tune);
+        returns (warps per sweep block, warp tasks per warp)."""
+        by, tasks = C.c_int(), C.c_int()
+        self._check(self.lib.dcm_tune(self.h, int(precision), int(bool(use_cache)), C.byref(by),
+                                      C.byref(tasks)))
+        return by.value, tasks.value
 
     def __del__(self):
         try:
@@ -366,6 +397,11 @@ class DynamicalCore:
     def driver_start(self):
         self._check(self.lib.dcm_driver_start(self.h))
 
+    def last_iters(self):
+        """Solver iterations of the last step taken (by step or by an
+        Ensemble): dcm_step with zero steps reports the last values."""
+        return self.step(0).iters_last
+
     def step(self, nsteps=1):
         stats = StepStats()
         self._check(self.lib.dcm_step(self.h, int(nsteps), C.byref(stats)))
@@ -423,3 +459,50 @@ def fortran_stack(fields):
     for q, a in enumerate(fields):
         out[q][...] = a
     return out
+
+
+class Ensemble:
+    """Independent domains on one device advanced together, one CUDA graph
+    launch per time step (dcm_ensemble_*).  `members[m]` is a DynamicalCore
+    view of member m's handle: upload_state / driver_start / download_state /
+    tune / step (alone) work on it as on a standalone core."""
+
+    def __init__(self, grids, device=0):
+        self.lib = library()
+        keeps, structs = zip(*[_grid_struct(g) for g in grids])
+        self._keep = keeps
+        arr = (_Grid * len(grids))(*structs)
+        e = C.c_void_p()
+        st = self.lib.dcm_ensemble_create(len(grids), C.cast(arr, C.c_void_p), device, C.byref(e))
+        if st:
+            raise DCMError(st, self.lib.dcm_status_string(st).decode())
+        self.e = e
+        self.members = []
+        for m, g in enumerate(grids):
+            h = C.c_void_p()
+            self._check(self.lib.dcm_ensemble_member(self.e, m, C.byref(h)))
+            self.members.append(DynamicalCore(g, device, _handle=h))
+
+    def _check(self, st):
+        if st:
+            msg = self.lib.dcm_ensemble_last_error(self.e)
+            raise DCMError(st, (msg or b"").decode() or
+                           self.lib.dcm_status_string(st).decode())
+
+    def step(self, nsteps=1):
+        stats = EnsembleStats()
+        self._check(self.lib.dcm_ensemble_step(self.e, int(nsteps), C.byref(stats)))
+        return stats
+
+    def close(self):
+        if getattr(self, "e", None):
+            for m in self.members:
+                m.h = None
+            self.lib.dcm_ensemble_destroy(self.e)
+            self.e = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

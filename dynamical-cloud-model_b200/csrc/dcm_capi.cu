@@ -2,6 +2,9 @@
 // per-call drop-ins for the reference subroutines, and the device-resident
 // time loop of model_driver (driver_code.f90:304-676).
 #include <cmath>
+#include <cstdlib>
+#include <fstream>
+#include <sstream>
 #include <cstdio>
 #include <cstring>
 #include <type_traits>
@@ -83,6 +86,12 @@ struct dcm_handle {
     // arguments change
     SolveGraph g64, g32;
     bool graphs = true;  // graph-driven solver loops (else host-polled)
+    // launch shape of the solver kernels (dcm_tune): warps per sweep block,
+    // warp tasks per warp of the reducing kernels (0 = fill the GPU)
+    int tune_by = 8, tune_tasks = 0;
+    // bumped whenever captured pointers or launch shapes change (state
+    // upload, tuning); an ensemble rebuilds its step graphs when it moves
+    unsigned generation = 0;
 
     // ---- resident state -------------------------------------------------------
     bool resident = false;
@@ -204,6 +213,19 @@ SolverWork<double> solver_work(dcm_handle* h) {
     w.red.partials = h->partials; w.red.gpartials = h->gpartials; w.red.gtick = h->gtick;
     w.red.ticket = h->ticket2;
     w.graph = h->graphs ? &h->g64 : nullptr;
+    w.by = h->tune_by;
+    w.tasks = h->tune_tasks;
+    return w;
+}
+
+// The FP64 side of a mixed solve: scalars, reductions and coefficients only
+// (the FP64 residual is formed from x and b directly, no FP64 work vectors).
+SolverWork<double> solver_scalars(dcm_handle* h) {
+    SolverWork<double> w{};
+    w.ae = h->ae; w.aw = h->aw; w.an = h->an; w.as = h->as; w.au = h->au; w.ad = h->ad;
+    w.partials = h->partials; w.ticket = h->ticket; w.S = h->S;
+    w.red.partials = h->partials; w.red.gpartials = h->gpartials; w.red.gtick = h->gtick;
+    w.red.ticket = h->ticket2;
     return w;
 }
 
@@ -777,13 +799,14 @@ T* alloc_owned(dcm_handle* h, size_t n = 0) {
 
 // velocity roles after n steps: (u, zu, tu) -> buffers (0,1,2), (2,0,1),
 // (1,2,0) for n mod 3 = 0, 1, 2 (driver_code.f90:281-283, :634-646)
-void roles(const dcm_handle* h, int& cu, int& cz, int& ct) {
+void roles_of(int phase, int& cu, int& cz, int& ct) {
     static const int RU[3] = {0, 2, 1}, RZ[3] = {1, 0, 2}, RT[3] = {2, 1, 0};
-    const int m = h->nstep % 3;
+    const int m = phase % 3;
     cu = RU[m];
     cz = RZ[m];
     ct = RT[m];
 }
+void roles(const dcm_handle* h, int& cu, int& cz, int& ct) { roles_of(h->nstep, cu, cz, ct); }
 
 template <typename T>
 __global__ void k_driver_start(Dims d, T* zu, T* zv, T* zw) {
@@ -867,6 +890,8 @@ SolverWork<float> solver_work_f(dcm_handle* h) {
     w.red.partials = h->partials; w.red.gpartials = h->gpartials; w.red.gtick = h->gtick;
     w.red.ticket = h->ticket2;
     w.graph = h->graphs ? &h->g32 : nullptr;
+    w.by = h->tune_by;
+    w.tasks = h->tune_tasks;
     return w;
 }
 
@@ -901,17 +926,21 @@ Forcing<float> forcing_t<float>(dcm_handle* h) {
     return F;
 }
 
-// one pass of the time loop (driver_code.f90:304-676) with fields in T and
-// the pressure in FP64
+// One pass of the time loop (driver_code.f90:304-676) with fields in T and
+// the pressure in FP64, on stream `st` with the velocity roles of `phase`
+// (= steps taken mod 3).  emit = false: run it (the pressure solve as its own
+// graph, host reads of the solver scalars).  emit = true: `st` is capturing
+// a larger graph (an ensemble time step) and the step, its solve included,
+// is only recorded into it: no host synchronisation, no host state changes.
 template <typename T>
-int one_step(dcm_handle* h) {
+int step_body(dcm_handle* h, cudaStream_t st, int phase, bool emit) {
     const Dims& d = h->d;
     const dcm_config& c = h->cfg;
     State<T>& S = state_of<T>(h);
     const Metrics<T>& mt = metrics_of<T>(h);
     const size_t K2 = d.kp + 2;
     int cu, cz, ct;
-    roles(h, cu, cz, ct);
+    roles_of(phase, cu, cz, ct);
     T *u = S.U[cu], *v = S.V[cu], *w = S.W[cu];
     T *zu = S.U[cz], *zv = S.V[cz], *zw = S.W[cz];
     T *tu = S.U[ct], *tv = S.V[ct], *tw = S.W[ct];
@@ -919,81 +948,97 @@ int one_step(dcm_handle* h) {
     const T dt = (T)c.dt;
     // horizontal_means + divergence_calc (FP64 divergence), driver_code.f90:433-444
     launch_means_div<T, double>(d, h->mt, u, v, w, S.th, S.q.data(), nqq, S.means, h->div,
-                                h->partials, h->ticket, h->st);
+                                h->partials, h->ticket, st);
     // sources (sth = 0 first, :340) + exchange_along_dim_wo(psrc), :455-487
     const Forcing<T> F = forcing_t<T>(h);
     const T* ubar = S.means;
     launch_sources<T, double>(d, mt, h->mt, F, ubar, ubar + K2, ubar + 2 * K2, ubar + 3 * K2, zu,
                               zv, zw, u, v, w, S.th, S.su, S.sv, S.sw, S.sth, h->psrc, 1, 1,
-                              h->st);
+                              st);
     CK(cudaGetLastError());
     // pressure: bicgstab + exchange_along_dim_wo(p), :496-507
-    SolverWork<double> swd = solver_work(h);
-    NEED(swd.r); NEED(swd.sB); NEED(swd.rh); NEED(swd.vh);
-    h->first_call = 0;
-    int st;
+    if (!emit) h->first_call = 0;
+    int rc;
     if constexpr (std::is_same<T, double>::value) {
-        st = solver_run<double>(swd, d, h->p, h->psrc, S.sw, h->mt.dzn, c.ptol, c.itmax, 1, 4,
-                                h->st, h->hS, nullptr);
-        h->last_iters = h->hS->it;
-        h->last_err = h->hS->err;
+        SolverWork<double> swd = solver_work(h);
+        NEED(swd.r); NEED(swd.sB); NEED(swd.rh); NEED(swd.vh);
+        if (emit) {
+            swd.graph = &h->g64;
+            swd.emit = true;
+        }
+        rc = solver_run<double>(swd, d, h->p, h->psrc, S.sw, h->mt.dzn, c.ptol, c.itmax, 1, 4,
+                                st, h->hS, nullptr);
+        if (!emit) {
+            h->last_iters = h->hS->it;
+            h->last_err = h->hS->err;
+        }
     } else {
+        SolverWork<double> swd = solver_scalars(h);
         SolverWork<float> swf = solver_work_f(h);
         NEED(swf.r); NEED(swf.sB); NEED(swf.rh); NEED(swf.vh);
+        if (emit) {
+            swf.graph = &h->g32;
+            swf.emit = true;
+        }
         float* dx = fslot(h, S_B);
         NEED(dx);
-        st = refine_run(swf, swd, d, h->p, h->psrc, S.sw, h->mt.dzn, dx, c.ptol,
-                        c.inner_tol > 0 ? c.inner_tol : 0.1, c.itmax, 1000, h->st, h->hS,
+        rc = refine_run(swf, swd, d, h->p, h->psrc, S.sw, h->mt.dzn, dx, c.ptol,
+                        c.inner_tol > 0 ? c.inner_tol : 0.1, c.itmax, 1000, st, h->hS,
                         h->hS2, &h->last_refine);
-        h->last_iters = h->last_refine.inner;
-        h->last_err = h->last_refine.err;
-        h->refine_outer_total += h->last_refine.outer;
+        if (!emit) {
+            h->last_iters = h->last_refine.inner;
+            h->last_err = h->last_refine.err;
+            h->refine_outer_total += h->last_refine.outer;
+        }
     }
-    if (st != DCM_OK) {
-        h->err = dcm_status_string(st);
-        return st;
+    if (rc != DCM_OK) {
+        h->err = dcm_status_string(rc);
+        return rc;
     }
     // scalar advection, :514-560, with advance_scalar_fields_3d (:601) fused
     MpBufsT<T> mb;
     if (!mpdata_work_t<T>(h, std::max(1, nqq), mb))
         return fail(h, DCM_E_CUDA, "device allocation");
     if (c.advection_scheme == 0 || c.advection_scheme == 1)
-        launch_adv_ref_state<T>(d, mt, dt, w, S.th, S.th2, mt.thetan, 1, h->st);
+        launch_adv_ref_state<T>(d, mt, dt, w, S.th, S.th2, mt.thetan, 1, st);
     if (c.advection_scheme == 1) {
         double lb = h->t1, ub = h->t2;
         T* pin = S.th2;
         T* pout = S.th;
         const T* sadd = S.sth;
         RC(mpdata_run<T>(mb.w, d, mt, dt, u, v, w, &pin, &pout, 1, &lb, &ub, c.kord, c.monotone,
-                         0, c.limiter, false, &sadd, dt, h->st));
+                         0, c.limiter, false, &sadd, dt, st));
         // t1, t2 return as (t - m) + m, which is exactly t when t = 0
         if (h->t1 != 0.0 || h->t2 != 0.0) {
-            CK(cudaMemcpyAsync(h->hM, h->M, sizeof(MpScalars), cudaMemcpyDeviceToHost, h->st));
+            if (emit) return fail(h, DCM_E_UNSUPPORTED, "captured step: t1, t2 must be 0");
+            CK(cudaMemcpyAsync(h->hM, h->M, sizeof(MpScalars), cudaMemcpyDeviceToHost, st));
             RC(sync(h));
             h->t1 = h->hM[0].lbc + h->hM[0].m;
             h->t2 = h->hM[0].ubc + h->hM[0].m;
         }
     } else if (c.advection_scheme == 0) {
         // donor cell + exchange_full(th, t1, t2), :539-545, then th += sth*dt
-        CK(cudaMemcpyAsync(S.th, S.th2, h->n * sizeof(T), cudaMemcpyDeviceToDevice, h->st));
-        RC(upwind_run<T>(mb.w, d, mt, dt, u, v, w, S.th2, S.th, 0, h->st));
-        launch_exchange<T>(d, S.th, HALO_FULL, (T)h->t1, (T)h->t2, h->st);
-        launch_advance_scalar<T>(d, dt, S.th, S.sth, h->st);
+        CK(cudaMemcpyAsync(S.th, S.th2, h->n * sizeof(T), cudaMemcpyDeviceToDevice, st));
+        RC(upwind_run<T>(mb.w, d, mt, dt, u, v, w, S.th2, S.th, 0, st));
+        launch_exchange<T>(d, S.th, HALO_FULL, (T)h->t1, (T)h->t2, st);
+        launch_advance_scalar<T>(d, dt, S.th, S.sth, st);
     } else if (c.advection_scheme == 2) {
+        if (emit) return fail(h, DCM_E_UNSUPPORTED, "captured step: advection_scheme 2");
         // mpdata_3d_add with thetan, thbase, thtop, :552-556
         double lb = c.thbase, ub = c.thtop;
-        launch_add_profile<T>(d, S.th, mt.thetan, T(1), h->st);
+        launch_add_profile<T>(d, S.th, mt.thetan, T(1), st);
         T* pin = S.th;
         T* pout = S.th2;
         RC(mpdata_run<T>(mb.w, d, mt, dt, u, v, w, &pin, &pout, 1, &lb, &ub, c.kord, c.monotone,
-                         0, c.limiter, false, nullptr, T(0), h->st));
-        launch_add_profile<T>(d, S.th2, mt.thetan, T(-1), h->st);
-        launch_advance_scalar<T>(d, dt, S.th2, S.sth, h->st);
+                         0, c.limiter, false, nullptr, T(0), st));
+        launch_add_profile<T>(d, S.th2, mt.thetan, T(-1), st);
+        launch_advance_scalar<T>(d, dt, S.th2, S.sth, st);
         std::swap(S.th, S.th2);
     } else {
         return fail(h, DCM_E_UNSUPPORTED, "advection_scheme");
     }
     // q categories, :568-585, then q += sq*dt
+    if (nqq && emit) return fail(h, DCM_E_UNSUPPORTED, "captured step: moisture");
     if (nqq) {
         for (int cat = 0; cat < c.ncat; cat++) {
             const int a = h->cs[cat] - 1, b = h->ce[cat] - 1;
@@ -1010,13 +1055,19 @@ int one_step(dcm_handle* h) {
             }
             RC(mpdata_run<T>(mb.w, d, mt, dt, u, v, w, qin.data(), qout.data(), nc,
                              h->q1.data() + a, h->q2.data() + a, c.kord, c.monotone, 0, c.limiter,
-                             true, sadd.data(), dt, h->st));
+                             true, sadd.data(), dt, st));
         }
     }
     // advance_momentum(2dt) + time filter + rotation + exchange + rows, :592-674
     launch_momentum_step<T, double>(d, mt, h->mt, (T)(2.0 * c.dt), u, v, w, zu, zv, zw, tu, tv,
-                                    tw, S.su, S.sv, S.sw, h->p, h->st);
+                                    tw, S.su, S.sv, S.sw, h->p, st);
     CK(cudaGetLastError());
+    return DCM_OK;
+}
+
+template <typename T>
+int one_step(dcm_handle* h) {
+    RC(step_body<T>(h, h->st, h->nstep % 3, false));
     h->nstep += 1;
     return DCM_OK;
 }
@@ -1173,6 +1224,7 @@ extern "C" int dcm_state_upload(dcm_handle* h, const dcm_config* cfg, const dcm_
     h->t1 = h->t2 = 0.0;  // saved locals, :260
     h->refine_outer_total = 0;
     h->resident = true;
+    h->generation += 1;
     return sync(h);
 }
 
@@ -1253,4 +1305,317 @@ extern "C" int dcm_profile_read(dcm_handle* h, double* ms, long long* launches, 
         launches[c] = h->prof.count[c];
     }
     return DCM_OK;
+}
+
+// =============================================================================
+// solver launch-shape autotuner (no counterpart in the reference)
+// =============================================================================
+namespace {
+
+std::string tune_cache_path() {
+    if (const char* p = std::getenv("DCM_TUNE_CACHE")) return p;
+    const char* home = std::getenv("HOME");
+    return std::string(home ? home : ".") + "/.cache/dcm_b200_solver_tune.txt";
+}
+
+// cache lines: "<sms> <ip> <jp> <kp> <precision> <by> <tasks> <ms per iteration>"
+bool tune_lookup(int sms, const Dims& d, int prec, int* by, int* tasks) {
+    std::ifstream f(tune_cache_path());
+    std::string line;
+    bool found = false;
+    while (std::getline(f, line)) {
+        std::istringstream is(line);
+        int a[7];
+        double ms;
+        if (!(is >> a[0] >> a[1] >> a[2] >> a[3] >> a[4] >> a[5] >> a[6] >> ms)) continue;
+        if (a[0] == sms && a[1] == d.ip && a[2] == d.jp && a[3] == d.kp && a[4] == prec) {
+            *by = a[5];
+            *tasks = a[6];
+            found = true;  // the last entry wins
+        }
+    }
+    return found;
+}
+
+void tune_store(int sms, const Dims& d, int prec, int by, int tasks, double ms) {
+    std::ofstream f(tune_cache_path(), std::ios::app);
+    if (f) f << sms << ' ' << d.ip << ' ' << d.jp << ' ' << d.kp << ' ' << prec << ' ' << by << ' '
+             << tasks << ' ' << ms << '\n';
+}
+
+template <typename T>
+__global__ void k_tune_rhs(Dims d, T* b, T* x) {
+    const int k = 1 + blockIdx.x * BX + threadIdx.x;
+    const int j = 1 + blockIdx.y * BY + threadIdx.y;
+    const int i = 1 + blockIdx.z;
+    if (k > d.kp || j > d.jp) return;
+    // a smooth zero-mean right-hand side; x starts at zero
+    const double pi = 3.141592653589793;
+    b[d.at(k, j, i)] = (T)(sin(2.0 * pi * i / d.ip) * cos(2.0 * pi * j / d.jp) *
+                           cos(pi * (k - 0.5) / d.kp));
+    x[d.at(k, j, i)] = T(0);
+}
+
+// device time of `iters` iterations of the solver in precision T with the
+// given launch shape (graph-driven, tolerance unreachable, itmax = iters)
+template <typename T>
+double tune_time(dcm_handle* h, int by, int tasks, int iters) {
+    SolverWork<T> w;
+    T *x, *b;
+    if constexpr (std::is_same<T, double>::value) {
+        w = solver_work(h);
+        x = slot(h, S_X);
+        b = slot(h, S_RHS);
+    } else {
+        w = solver_work_f(h);
+        x = fslot(h, S_X);
+        b = fslot(h, S_RHS);
+    }
+    if (!x || !b || !w.r || !w.sB || !w.rh || !w.vh) return -1.0;
+    SolveGraph G;
+    w.graph = &G;
+    w.by = by;
+    w.tasks = tasks;
+    const Metrics<T>& mt = metrics_of<T>(h);
+    double best = 1e30;
+    for (int rep = 0; rep < 3; rep++) {
+        k_tune_rhs<T><<<interior_grid(h->d, h->d.kp), dim3(BX, BY), 0, h->st>>>(h->d, b, x);
+        cudaEventRecord(h->ev0, h->st);
+        // tolerance out of reach: exactly `iters` iterations, ending NOCONV
+        const int rc = solver_run<T>(w, h->d, x, b, x, mt.dzn, 1e-300, iters, 0, 4, h->st, h->hS,
+                                     nullptr, 0.01, false);
+        if (rc != DCM_E_NOCONV || h->hS->it != iters) return -1.0;
+        cudaEventRecord(h->ev1, h->st);
+        cudaEventSynchronize(h->ev1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+        if (rep > 0) best = std::min(best, (double)ms / iters);  // rep 0 builds the graph
+    }
+    return cudaGetLastError() == cudaSuccess ? best : -1.0;
+}
+
+}  // namespace
+
+extern "C" int dcm_tune(dcm_handle* h, int precision, int use_cache, int* by, int* tasks) {
+    CHECK_H();
+    if (precision != 0 && precision != 1) return fail(h, DCM_E_ARG, "tune: precision");
+    int sms = 0;
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
+    int b0 = 8, t0 = 0;
+    if (!(use_cache && tune_lookup(sms, h->d, precision, &b0, &t0))) {
+        static const int BYS[3] = {2, 4, 8}, TASKS[4] = {0, 1, 2, 4};
+        double best = 1e30;
+        for (int bi = 0; bi < 3; bi++)
+            for (int ti = 0; ti < 4; ti++) {
+                const double ms = precision == 0 ? tune_time<double>(h, BYS[bi], TASKS[ti], 12)
+                                                 : tune_time<float>(h, BYS[bi], TASKS[ti], 12);
+                if (ms < 0) return fail(h, DCM_E_CUDA, "tune: a candidate launch shape failed");
+                if (ms < best) {
+                    best = ms;
+                    b0 = BYS[bi];
+                    t0 = TASKS[ti];
+                }
+            }
+        tune_store(sms, h->d, precision, b0, t0, best);
+    }
+    h->tune_by = b0;
+    h->tune_tasks = t0;
+    h->generation += 1;
+    if (by) *by = b0;
+    if (tasks) *tasks = t0;
+    return DCM_OK;
+}
+
+// =============================================================================
+// batched ensemble (no counterpart in the reference)
+// =============================================================================
+struct dcm_ensemble {
+    int device = 0;
+    std::vector<dcm_handle*> m;
+    cudaStream_t st = nullptr;
+    std::vector<cudaStream_t> mst;
+    cudaEvent_t fork = nullptr, ev0 = nullptr, ev1 = nullptr;
+    std::vector<cudaEvent_t> join;
+    cudaGraph_t graph[3] = {nullptr, nullptr, nullptr};
+    cudaGraphExec_t exec[3] = {nullptr, nullptr, nullptr};
+    std::vector<unsigned> gen[3];  // member generations each graph was built for
+    std::string err;
+};
+
+namespace {
+
+void ens_release(dcm_ensemble* e, int p) {
+    if (e->exec[p]) cudaGraphExecDestroy(e->exec[p]);
+    if (e->graph[p]) cudaGraphDestroy(e->graph[p]);
+    e->exec[p] = nullptr;
+    e->graph[p] = nullptr;
+    e->gen[p].clear();
+}
+
+int ens_fail(dcm_ensemble* e, int code, const std::string& what) {
+    e->err = what;
+    return code;
+}
+
+// one CUDA graph for a time step of every member at velocity phase p: a
+// fork into one capture stream per member, each member's whole step (its
+// pressure solve as its own WHILE loop: converged members stop iterating
+// while the others continue), the solver scalars copied to pinned host
+// memory, and a join
+int ens_build(dcm_ensemble* e, int p) {
+    ens_release(e, p);
+    if (cudaStreamBeginCapture(e->st, cudaStreamCaptureModeRelaxed) != cudaSuccess)
+        return ens_fail(e, DCM_E_CUDA, "ensemble: begin capture");
+    int rc = DCM_OK;
+    cudaEventRecord(e->fork, e->st);
+    Profiler* saved = g_prof;
+    g_prof = nullptr;
+    for (size_t q = 0; q < e->m.size() && rc == DCM_OK; q++) {
+        dcm_handle* h = e->m[q];
+        cudaStream_t s = e->mst[q];
+        cudaStreamWaitEvent(s, e->fork, 0);
+        rc = h->prec == 0 ? step_body<double>(h, s, p, true) : step_body<float>(h, s, p, true);
+        if (rc != DCM_OK) {
+            e->err = "member " + std::to_string(q) + ": " + h->err;
+            break;
+        }
+        cudaMemcpyAsync(h->hS, h->S, sizeof(SolverScalars), cudaMemcpyDeviceToHost, s);
+        if (h->prec) cudaMemcpyAsync(h->hS2, h->S2, sizeof(SolverScalars), cudaMemcpyDeviceToHost, s);
+        cudaEventRecord(e->join[q], s);
+        cudaStreamWaitEvent(e->st, e->join[q], 0);
+    }
+    g_prof = saved;
+    cudaGraph_t g = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(e->st, &g);
+    e->graph[p] = g;
+    if (rc != DCM_OK || ce != cudaSuccess || !g ||
+        cudaGraphInstantiate(&e->exec[p], g, 0) != cudaSuccess) {
+        ens_release(e, p);
+        cudaGetLastError();
+        return rc != DCM_OK ? rc : ens_fail(e, DCM_E_CUDA, "ensemble: capture / instantiate");
+    }
+    for (dcm_handle* h : e->m) e->gen[p].push_back(h->generation);
+    return DCM_OK;
+}
+
+}  // namespace
+
+extern "C" int dcm_ensemble_create(int nmembers, const dcm_grid* grids, int device,
+                                   dcm_ensemble** out) {
+    if (!out || !grids || nmembers < 1) return DCM_E_ARG;
+    *out = nullptr;
+    dcm_ensemble* e = new dcm_ensemble();
+    e->device = device;
+    for (int q = 0; q < nmembers; q++) {
+        dcm_handle* h = nullptr;
+        const int rc = dcm_create(&grids[q], device, &h);
+        if (rc != DCM_OK) {
+            for (dcm_handle* x : e->m) dcm_destroy(x);
+            delete e;
+            return rc;
+        }
+        e->m.push_back(h);
+    }
+    bool good = cudaSetDevice(device) == cudaSuccess &&
+                cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking) == cudaSuccess &&
+                cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming) == cudaSuccess &&
+                cudaEventCreate(&e->ev0) == cudaSuccess && cudaEventCreate(&e->ev1) == cudaSuccess;
+    e->mst.assign(nmembers, nullptr);
+    e->join.assign(nmembers, nullptr);
+    for (int q = 0; q < nmembers && good; q++)
+        good = cudaStreamCreateWithFlags(&e->mst[q], cudaStreamNonBlocking) == cudaSuccess &&
+               cudaEventCreateWithFlags(&e->join[q], cudaEventDisableTiming) == cudaSuccess;
+    *out = e;
+    return good ? DCM_OK : DCM_E_CUDA;
+}
+
+extern "C" int dcm_ensemble_destroy(dcm_ensemble* e) {
+    if (!e) return DCM_OK;
+    cudaSetDevice(e->device);
+    if (e->st) cudaStreamSynchronize(e->st);
+    for (int p = 0; p < 3; p++) ens_release(e, p);
+    for (cudaStream_t s : e->mst)
+        if (s) cudaStreamDestroy(s);
+    for (cudaEvent_t v : e->join)
+        if (v) cudaEventDestroy(v);
+    if (e->fork) cudaEventDestroy(e->fork);
+    if (e->ev0) cudaEventDestroy(e->ev0);
+    if (e->ev1) cudaEventDestroy(e->ev1);
+    if (e->st) cudaStreamDestroy(e->st);
+    for (dcm_handle* h : e->m) dcm_destroy(h);
+    delete e;
+    return DCM_OK;
+}
+
+extern "C" int dcm_ensemble_member(dcm_ensemble* e, int member, dcm_handle** h) {
+    if (!e || !h || member < 0 || member >= (int)e->m.size()) return DCM_E_ARG;
+    *h = e->m[member];
+    return DCM_OK;
+}
+
+extern "C" const char* dcm_ensemble_last_error(const dcm_ensemble* e) {
+    return e ? e->err.c_str() : "";
+}
+
+extern "C" int dcm_ensemble_step(dcm_ensemble* e, int nsteps, dcm_ensemble_stats* stats) {
+    if (!e || nsteps < 0) return DCM_E_ARG;
+    if (cudaSetDevice(e->device) != cudaSuccess) return ens_fail(e, DCM_E_CUDA, "set device");
+    const int n0 = e->m[0]->nstep;
+    for (dcm_handle* h : e->m) {
+        if (!h->resident) return ens_fail(e, DCM_E_ARG, "ensemble: a member has no state");
+        if (h->nstep != n0) return ens_fail(e, DCM_E_ARG, "ensemble: members at different steps");
+    }
+    long long iters = 0;
+    int imax = 0, done = 0, rc = DCM_OK;
+    float ms_total = 0.f;
+    for (; done < nsteps; done++) {
+        const int p = (n0 + done) % 3;
+        bool fresh = e->exec[p] != nullptr && e->gen[p].size() == e->m.size();
+        for (size_t q = 0; fresh && q < e->m.size(); q++) fresh = e->gen[p][q] == e->m[q]->generation;
+        if (!fresh && (rc = ens_build(e, p)) != DCM_OK) break;
+        cudaEventRecord(e->ev0, e->st);
+        if (cudaGraphLaunch(e->exec[p], e->st) != cudaSuccess) {
+            rc = ens_fail(e, DCM_E_CUDA, "ensemble: graph launch");
+            break;
+        }
+        cudaEventRecord(e->ev1, e->st);
+        if (cudaEventSynchronize(e->ev1) != cudaSuccess) {
+            rc = ens_fail(e, DCM_E_CUDA, std::string("ensemble: ") +
+                                             cudaGetErrorString(cudaGetLastError()));
+            break;
+        }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e->ev0, e->ev1);
+        ms_total += ms;
+        imax = 0;
+        for (size_t q = 0; q < e->m.size(); q++) {
+            dcm_handle* h = e->m[q];
+            const SolverScalars* S = h->prec ? h->hS2 : h->hS;
+            const int st = h->hS->status;  // the mixed solve copies its outcome there
+            h->last_iters = S->it;
+            h->last_err = S->err;
+            if (h->prec) {
+                h->last_refine.outer = S->updates;
+                h->last_refine.inner = S->it;
+                h->last_refine.restarts = S->restarts;
+                h->last_refine.err = S->err;
+            }
+            h->nstep += 1;
+            iters += S->it;
+            imax = std::max(imax, S->it);
+            if (st != DCM_OK && rc == DCM_OK)
+                rc = ens_fail(e, st, "member " + std::to_string(q) + ": " + dcm_status_string(st));
+        }
+        if (rc != DCM_OK) {
+            done++;
+            break;
+        }
+    }
+    if (stats) {
+        stats->steps = done;
+        stats->iters_total = iters;
+        stats->iters_max_last = imax;
+        stats->ms_total = ms_total;
+    }
+    return rc;
 }

@@ -72,6 +72,14 @@ struct SolverWork {
     Red2 red;
     SolverScalars* S;
     SolveGraph* graph = nullptr;  // null: host-driven loop
+    // emit the solve into the graph being captured on the caller's stream
+    // (a whole time step captured with other work) instead of running it
+    bool emit = false;
+    // launch shape (tuning): warps per block of the non-reducing sweeps, and
+    // warp tasks per warp of the persistent reducing kernels (0 = as many
+    // resident blocks as the occupancy allows)
+    int by = 8;
+    int tasks = 0;
 };
 
 // per-field scalars of one MPDATA call

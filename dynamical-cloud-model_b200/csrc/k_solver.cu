@@ -35,6 +35,7 @@
 // a_p once.  The result agrees with the reference's order of operations to a
 // few ulp per sweep, far below the 1e-10 parity bar.  The iteration then
 // moves 41 field passes instead of 39.
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <type_traits>
@@ -59,6 +60,8 @@ struct SolverArgs {
     int nkt;          // k-chunks of a warp task
     int max_updates;  // mixed form: reliable updates before DCM_E_NOCONV
     int max_cycle;    // mixed form: FP32 iterations between updates before a restart
+    int by;           // warps per block of the non-reducing sweeps
+    int tasks;        // warp tasks per warp of the reducing kernels (0: fill the GPU)
 };
 
 // a_p exactly as set_mat_a forms it (dynamics.f90:93-95)
@@ -436,7 +439,7 @@ __global__ void __launch_bounds__(256) k_sten(SolverArgs a, Coef<T> c, SolverBuf
 #pragma unroll
     for (int q = 0; q < NV; q++) acc[q] = 0.0;
     if constexpr (!RED) {
-        const int j = 1 + blockIdx.y * BY + threadIdx.y;
+        const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
         if (j <= d.jp) sten_task<T, OP, MODE, NV>(C, blockIdx.x, j, 1 + blockIdx.z, acc);
     } else {
         for (TaskIter t(blockIdx.x * blockDim.y + threadIdx.y, gridDim.x * blockDim.y, a.nkt,
@@ -604,18 +607,30 @@ static int kchunks(const Dims& d) {
     return (d.kp + KVec<T>::V * BX - 1) / (KVec<T>::V * BX);
 }
 
+// blocks of a persistent reducing kernel: all resident blocks (tasks = 0),
+// or enough blocks for `tasks` warp tasks per warp
+static int red_grid(const SolverArgs& a, int full, int nkt) {
+    if (a.tasks <= 0) return full;
+    const long long ntask = (long long)nkt * a.d.jp * a.d.ip;
+    const long long want = (ntask + (long long)BY * a.tasks - 1) / ((long long)BY * a.tasks);
+    return (int)std::max(1LL, std::min((long long)full, want));
+}
+
 template <typename T, int OP, int MODE>
 static void sten(const SolverArgs& a, const Coef<T>& c, const SolverBufs& B, SolverWork<T>& w,
                  cudaStream_t st, int cat) {
     ProfScope ps(cat, st);
     constexpr bool RED = OP == OP_SETUP || OP == OP_MATC || OP == OP_MATP;
     if (RED) {
-        static int g = 0;
-        if (!g) g = persistent_grid(k_sten<T, OP, MODE>);
-        k_sten<T, OP, MODE><<<g, dim3(BX, BY), 0, st>>>(a, c, B, w.red, w.S);
+        static int full = 0;
+        if (!full) full = persistent_grid(k_sten<T, OP, MODE>);
+        k_sten<T, OP, MODE><<<red_grid(a, full, a.nkt), dim3(BX, BY), 0, st>>>(a, c, B, w.red,
+                                                                                w.S);
     } else {
-        const dim3 grid(a.nkt, (a.d.jp + BY - 1) / BY, a.d.ip);
-        k_sten<T, OP, MODE><<<grid, dim3(BX, BY), 0, st>>>(a, c, B, w.red, w.S);
+        // at most 256 threads: the kernels are compiled with __launch_bounds__(256)
+        const int by = a.by >= 1 && a.by <= 256 / BX ? a.by : BY;
+        const dim3 grid(a.nkt, (a.d.jp + by - 1) / by, a.d.ip);
+        k_sten<T, OP, MODE><<<grid, dim3(BX, by), 0, st>>>(a, c, B, w.red, w.S);
     }
 }
 
@@ -657,9 +672,9 @@ static void launch_iteration(const SolverArgs& a, const Coef<T>& c, SolverWork<T
     // phase D
     {
         ProfScope ps(P_UPDATE, st);
-        static int g = 0;
-        if (!g) g = persistent_grid(k_bicg_update<T>);
-        k_bicg_update<T><<<g, dim3(BX, BY), 0, st>>>(a, c, x, w.p, w.sA, w.r, w.v1, w.t, w.cr,
+        static int full = 0;
+        if (!full) full = persistent_grid(k_bicg_update<T>);
+        k_bicg_update<T><<<red_grid(a, full, a.nkt), dim3(BX, BY), 0, st>>>(a, c, x, w.p, w.sA, w.r, w.v1, w.t, w.cr,
                                                      w.rh, w.red, w.S);
     }
 }
@@ -730,8 +745,9 @@ bool capture_into(cudaStream_t side, cudaGraph_t body, F&& launches) {
                                           cudaStreamCaptureModeRelaxed)))
         return false;
     launches(side);
+    const bool launched = cudaPeekAtLastError() == cudaSuccess;
     cudaGraph_t out = body;
-    return ok(cudaStreamEndCapture(side, &out));
+    return ok(cudaStreamEndCapture(side, &out)) && launched;
 }
 
 struct CaptureGuard {  // launches inside a capture are counted per run instead
@@ -763,6 +779,8 @@ int solver_run(SolverWork<T>& w, const Dims& d, T* x, const T* b, const T* sw, c
     a.nkt = kchunks<T>(d);
     a.max_updates = 0;
     a.max_cycle = 0;
+    a.by = w.by;
+    a.tasks = w.tasks;
     const Coef<T> c = coef_of(w);
     SolverBufs B{};
     B.x = x;
@@ -778,30 +796,36 @@ int solver_run(SolverWork<T>& w, const Dims& d, T* x, const T* b, const T* sw, c
                                                                               wo);
         }
     };
+    // the whole solve into the graph being captured on `s`: setup, the
+    // WHILE loop of iterations, the halo fix-up
+    auto emit = [&](cudaStream_t s, SolveGraph& G) {
+        if (!side_streams(G)) return false;
+        CaptureGuard cg;
+        cudaGraphConditionalHandle hw{};
+        cudaGraph_t body[1] = {nullptr};
+        sten<T, OP_SETUP, 0>(a, c, B, w, s, P_SETUP);
+        bool good = capture_cond_handle(s, &hw, 0);
+        if (good) k_loop_cond<<<1, 1, 0, s>>>(hw, w.S, max_rounds);
+        good = good && capture_cond_node(s, hw, cudaGraphCondTypeWhile, 1, body);
+        good = good && capture_into(G.side[0], body[0], [&](cudaStream_t s2) {
+                   launch_iteration<T>(a, c, w, x, s2);
+                   k_loop_cond<<<1, 1, 0, s2>>>(hw, w.S, max_rounds);
+               });
+        post_launch(s);
+        return good && cudaPeekAtLastError() == cudaSuccess;
+    };
+    if (w.graph && w.emit) return emit(st, *w.graph) ? DCM_OK : DCM_E_CUDA;
     const bool use_graph = w.graph && !(g_prof && g_prof->on);
     if (use_graph) {
         SolveGraph& G = *w.graph;
         const void* kp[6] = {x, b, sw, dzn, w.r, w.S};
         const double kd[3] = {tol, sc_floor, 0.0};
-        const int ki[6] = {itmax, wo, post ? 1 : 0, (int)sizeof(T), d.ip * 4096 + d.jp, d.kp};
+        const int ki[6] = {itmax, wo, post ? 1 : 0, (int)sizeof(T), d.ip * 4096 + d.jp,
+                           d.kp + 65536 * (a.by + 64 * a.tasks)};
         if (!G.matches(kp, kd, ki)) {
             G.release();
-            if (!side_streams(G)) return DCM_E_CUDA;
-            CaptureGuard cg;
             bool good = ok(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
-            cudaGraphConditionalHandle hw{};
-            cudaGraph_t body[1] = {nullptr};
-            if (good) {
-                sten<T, OP_SETUP, 0>(a, c, B, w, st, P_SETUP);
-                good = capture_cond_handle(st, &hw, 0);
-                if (good) k_loop_cond<<<1, 1, 0, st>>>(hw, w.S, max_rounds);
-                good = good && capture_cond_node(st, hw, cudaGraphCondTypeWhile, 1, body);
-                good = good && capture_into(G.side[0], body[0], [&](cudaStream_t s) {
-                           launch_iteration<T>(a, c, w, x, s);
-                           k_loop_cond<<<1, 1, 0, s>>>(hw, w.S, max_rounds);
-                       });
-                post_launch(st);
-            }
+            if (good) good = emit(st, G);
             cudaGraph_t gr = nullptr;
             const bool ended = ok(cudaStreamEndCapture(st, &gr));
             G.graph = gr;
@@ -1019,13 +1043,16 @@ int refine_run(SolverWork<float>& wf, SolverWork<double>& wd, const Dims& d, dou
     a.nkt = (d.kp + BX - 1) / BX;  // scalar warp tasks of the FP64 residual
     a.max_updates = max_updates;
     a.max_cycle = 250;
+    a.by = wf.by;
+    a.tasks = wf.tasks;
     SolverArgs af = a;             // vector warp tasks of the FP32 iterations
     af.nkt = kchunks<float>(d);
     Coef<double> cd;
     cd.ae = wd.ae; cd.aw = wd.aw; cd.an = wd.an; cd.as = wd.as; cd.au = wd.au; cd.ad = wd.ad;
     const Coef<float> cf = coef_of(wf);
-    static int g = 0;
-    if (!g) g = persistent_grid(k_ru_residual<false>);
+    static int gfull = 0;
+    if (!gfull) gfull = persistent_grid(k_ru_residual<false>);
+    const int g = red_grid(a, gfull, a.nkt);
     const dim3 gi = interior_grid(d, d.kp), bl(BX, BY);
     auto begin = [&](cudaStream_t s) {
         cudaMemsetAsync(dx, 0, d.n() * sizeof(float), s);
@@ -1052,40 +1079,45 @@ int refine_run(SolverWork<float>& wf, SolverWork<double>& wd, const Dims& d, dou
         k_bicg_post<double, float><<<gi, bl, 0, s>>>(d, x, sw, dzn, wd.S, 1);
     };
     const int max_rounds = itmax + max_updates + 1;
+    // the whole mixed solve into the graph being captured on `s0`
+    auto emit = [&](cudaStream_t s0, SolveGraph& G) {
+        if (!side_streams(G)) return false;
+        CaptureGuard cgd;
+        cudaGraphConditionalHandle hw{};
+        cudaGraph_t body[1] = {nullptr};
+        begin(s0);
+        bool good = capture_cond_handle(s0, &hw, 0);
+        if (good) k_loop_cond<<<1, 1, 0, s0>>>(hw, wf.S, max_rounds);
+        good = good && capture_cond_node(s0, hw, cudaGraphCondTypeWhile, 1, body);
+        // loop body: branch on pause -> reliable update | FP32 iteration
+        good = good && capture_into(G.side[0], body[0], [&](cudaStream_t s) {
+                   cudaGraphConditionalHandle hb{};
+                   cudaGraph_t br[2] = {nullptr, nullptr};
+                   bool g2 = capture_cond_handle(s, &hb, 0);
+                   if (g2) k_branch_pause<<<1, 1, 0, s>>>(hb, wf.S);
+                   g2 = g2 && capture_cond_node(s, hb, cudaGraphCondTypeIf, 2, br);
+                   g2 = g2 && capture_into(G.side[1], br[0], update);
+                   g2 = g2 && capture_into(G.side[1], br[1], [&](cudaStream_t s2) {
+                            launch_iteration<float>(af, cf, wf, dx, s2);
+                        });
+                   k_loop_cond<<<1, 1, 0, s>>>(hw, wf.S, max_rounds);
+                   if (!g2) good = false;
+               });
+        finish(s0);
+        return good && cudaPeekAtLastError() == cudaSuccess;
+    };
+    if (wf.graph && wf.emit) return emit(st, *wf.graph) ? DCM_OK : DCM_E_CUDA;
     const bool use_graph = wf.graph && !(g_prof && g_prof->on);
     if (use_graph) {
         SolveGraph& G = *wf.graph;
         const void* kp[6] = {x, b, sw, dzn, dx, wf.S};
         const double kd[3] = {tol, delta, 0.0};
-        const int ki[6] = {itmax, max_updates, 1, 0, d.ip * 4096 + d.jp, d.kp};
+        const int ki[6] = {itmax, max_updates, 1, 0, d.ip * 4096 + d.jp,
+                           d.kp + 65536 * (af.by + 64 * af.tasks)};
         if (!G.matches(kp, kd, ki)) {
             G.release();
-            if (!side_streams(G)) return DCM_E_CUDA;
-            CaptureGuard cgd;
             bool good = ok(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
-            cudaGraphConditionalHandle hw{};
-            cudaGraph_t body[1] = {nullptr};
-            if (good) {
-                begin(st);
-                good = capture_cond_handle(st, &hw, 0);
-                if (good) k_loop_cond<<<1, 1, 0, st>>>(hw, wf.S, max_rounds);
-                good = good && capture_cond_node(st, hw, cudaGraphCondTypeWhile, 1, body);
-                // loop body: branch on pause -> reliable update | FP32 iteration
-                good = good && capture_into(G.side[0], body[0], [&](cudaStream_t s) {
-                           cudaGraphConditionalHandle hb{};
-                           cudaGraph_t br[2] = {nullptr, nullptr};
-                           bool g2 = capture_cond_handle(s, &hb, 0);
-                           if (g2) k_branch_pause<<<1, 1, 0, s>>>(hb, wf.S);
-                           g2 = g2 && capture_cond_node(s, hb, cudaGraphCondTypeIf, 2, br);
-                           g2 = g2 && capture_into(G.side[1], br[0], update);
-                           g2 = g2 && capture_into(G.side[1], br[1], [&](cudaStream_t s2) {
-                                    launch_iteration<float>(af, cf, wf, dx, s2);
-                                });
-                           k_loop_cond<<<1, 1, 0, s>>>(hw, wf.S, max_rounds);
-                           if (!g2) good = false;
-                       });
-                finish(st);
-            }
+            if (good) good = emit(st, G);
             cudaGraph_t gr = nullptr;
             const bool ended = ok(cudaStreamEndCapture(st, &gr));
             G.graph = gr;

@@ -257,6 +257,47 @@ int dcm_profile_read(dcm_handle *h, double *ms, long long *launches, int ncat);
  * the host-driven loop is used. */
 int dcm_solver_graphs(dcm_handle *h, int on);
 
+/* ---- solver launch-shape autotuner (no counterpart in the reference) ---- */
+/* Chooses, for this handle's grid shape and the given precision (0 FP64,
+ * 1 the FP32 iterations of the mixed form), the warps per block of the
+ * Jacobi sweeps (2, 4, 8) and the warp tasks per warp of the persistent
+ * reducing kernels (0 = fill the GPU, 1, 2, 4) by timing 12 BiCGSTAB
+ * iterations of each pair on a synthetic right-hand side, then applies them
+ * to the handle.  With use_cache the result is looked up first in, and
+ * otherwise appended to, a text file: $DCM_TUNE_CACHE, or
+ * $HOME/.cache/dcm_b200_solver_tune.txt (one line per SM count, grid shape
+ * and precision).  Uses the handle's scratch fields; call it before
+ * dcm_state_upload or between steps, not concurrently with other calls on
+ * the handle. */
+int dcm_tune(dcm_handle *h, int precision, int use_cache, int *by, int *tasks);
+
+/* ---- batched ensemble (no counterpart in the reference) ------------------ */
+/* Independent domains of possibly different sizes on one device.  Each
+ * member is a full handle (dcm_ensemble_member): upload its state with
+ * dcm_state_upload + dcm_driver_start, optionally dcm_tune it, read it back
+ * with dcm_state_download.  dcm_ensemble_step advances every member by one
+ * time step per launch of ONE CUDA graph: a fork into one branch per member
+ * holding that member's whole step; each member's pressure solve is its own
+ * conditional WHILE loop, so a converged member stops iterating while the
+ * others continue (per-member convergence masks).  Three graphs (the
+ * velocity-role phases of the leapfrog rotation) are captured on first use
+ * and recaptured after a member's state upload or tuning.  Members must be
+ * at the same step count and use advection_scheme 0 or 1 without moisture
+ * and with t1 = t2 = 0 (the dry configurations). */
+typedef struct dcm_ensemble dcm_ensemble;
+typedef struct {
+    int steps;              /* ensemble steps taken in this call           */
+    long long iters_total;  /* solver iterations, all members and steps    */
+    int iters_max_last;     /* most iterations of any member, last step    */
+    double ms_total;        /* device time of the graph launches           */
+} dcm_ensemble_stats;
+int dcm_ensemble_create(int nmembers, const dcm_grid *grids, int device,
+                        dcm_ensemble **e);
+int dcm_ensemble_destroy(dcm_ensemble *e);
+int dcm_ensemble_member(dcm_ensemble *e, int member, dcm_handle **h);
+int dcm_ensemble_step(dcm_ensemble *e, int nsteps, dcm_ensemble_stats *stats);
+const char *dcm_ensemble_last_error(const dcm_ensemble *e);
+
 #ifdef __cplusplus
 }
 #endif
