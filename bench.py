@@ -196,6 +196,8 @@ def run_b200(args, rank, world, local_rank, dist):
     g = case.grid
     N = g.npoints
     core = pkg.DynamicalCore(g, device=local_rank)
+    if args.host_loop:
+        core.solver_graphs(False)
     kw = dict(ptol=case.ptol, kord=case.kord, monotone=case.monotone)
     if case.nq:
         kw.update(nq=case.nq, c_s=case.c_s, c_e=case.c_e)
@@ -345,6 +347,111 @@ def run_b200(args, rank, world, local_rank, dist):
     }
 
 
+def run_ensemble(args, rank, world, local_rank, dist):
+    """Batched ensemble of seeded dry warm bubbles of uneven sizes (ip, jp
+    from {64, 96, 128, 192}, kp from {48, 64, 96}, amplitude U(1, 3) K),
+    mixed precision, solver launch shapes autotuned per grid shape.  Members
+    are partitioned over ranks (no collective); each rank advances its
+    members with one CUDA graph launch per step and, beside it, the same
+    members one after another (sequential per-member loop)."""
+    pkg = load_pkg()
+    from dcm_b200 import cases
+    spec = cases.ensemble_members(args.members)
+    mine = spec[rank::world]
+    mcases = [cases.warm_bubble(ip=ip, jp=jp, kp=kp, amp=amp, seed=seed)
+              for (ip, jp, kp, amp, seed) in mine]
+    ens = pkg.Ensemble([c.grid for c in mcases], device=local_rank)
+    shapes = {}
+    for core, c in zip(ens.members, mcases):
+        key = (c.grid.ip, c.grid.jp, c.grid.kp)
+        shapes[key] = core.tune(precision=1, use_cache=True)
+        if shapes[key] != core.tune(precision=1, use_cache=True):
+            raise SystemExit("tuner cache is inconsistent")
+
+    def fresh():
+        for core, c in zip(ens.members, mcases):
+            core.upload_state(c.state, c.dt, ptol=c.ptol, kord=c.kord, monotone=c.monotone,
+                              precision=1)
+            core.driver_start()
+
+    def barrier():
+        if dist is not None:
+            import torch
+            torch.cuda.synchronize()
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum_over_ranks(x):
+        if dist is None:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+
+    points = sum(c.grid.npoints for c in mcases)
+    fresh()
+    if args.warmup:
+        ens.step(args.warmup)  # captures the three phase graphs
+    fresh()
+    clocks = ClockSampler(local_rank)
+    barrier()
+    clocks.start()
+    st = ens.step(args.steps)
+    clk = clocks.stop()
+    barrier()
+    ms = max_over_ranks(st.ms_total)
+    iters = st.iters_total
+    # the same steps, one member after another
+    fresh()
+    for core in ens.members:
+        if args.warmup:
+            core.step(args.warmup)
+    fresh()
+    barrier()
+    seq_ms = 0.0
+    seq_iters = 0
+    for core in ens.members:
+        s2 = core.step(args.steps)
+        seq_ms += s2.ms_total
+        seq_iters += s2.iters_total
+    barrier()
+    seq_ms = max_over_ranks(seq_ms)
+    total_points = sum_over_ranks(points)
+    ens.close()
+    if rank != 0:
+        return None
+    value = total_points * args.steps / (ms / 1e3)
+    return {
+        "metric": "aggregate grid-pt-steps/s of a %d-member warm-bubble ensemble" % args.members,
+        "value": value, "unit": "grid-pt-steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak" if world > 1 else "strong", "vs_baseline": None,
+        "dtype": "f32+f64 (FP32 fields and BiCGSTAB, FP64 pressure, residual and dots)",
+        "data": "synthetic (seeded warm bubbles, numpy PCG64 seeds 5000..5063)",
+        "config": {"workload": "ensemble of %d dry warm bubbles, mixed precision" % args.members,
+                   "members_per_rank": len(mine), "points_per_rank": points,
+                   "grid_shapes": sorted(["%dx%dx%d" % k for k in shapes]),
+                   "tuned_launch_shapes": {"%dx%dx%d" % k: list(v) for k, v in shapes.items()},
+                   "timed_steps": "1..%d from the initial states" % args.steps,
+                   "parallelism": "members partitioned over ranks" if world > 1 else
+                   "single GPU"},
+        "sequential": {"value": total_points * args.steps / (seq_ms / 1e3),
+                       "ms_per_step": seq_ms / args.steps,
+                       "note": "the same members, one dcm_step call after another"},
+        "speedup_vs_sequential": seq_ms / ms,
+        "bicgstab_iters": {"ensemble": iters, "sequential": seq_iters},
+        "graph_launches": args.steps, "clocks": clk,
+    }
+
+
 def cpu_baseline(args, case, nsteps):
     """The oracle (CPU restatement of the reference, not the reference
     binary) on the host cores, steps 1..nsteps of the same case."""
@@ -399,6 +506,10 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=60.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--accuracy-steps", type=int, default=100)
+    ap.add_argument("--members", type=int, default=64)
+    ap.add_argument("--host-loop", action="store_true",
+                    help="host-polled solver loop instead of graph-driven solves (same "
+                         "kernels; lets a profiler see every solver launch)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -415,7 +526,10 @@ def main():
             torch.cuda.set_device(local_rank)
             tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
             dist = tdist
-        res = run_b200(args, rank, world, local_rank, dist)
+        if args.case == "ensemble":
+            res = run_ensemble(args, rank, world, local_rank, dist)
+        else:
+            res = run_b200(args, rank, world, local_rank, dist)
         if dist is not None:
             dist.barrier()
             dist.destroy_process_group()
