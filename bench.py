@@ -261,7 +261,7 @@ def run_b200(args, rank, world, local_rank, dist):
     tp = os.path.join(ROOT, "profiles", "dram_traffic.json")
     if os.path.exists(tp):
         with open(tp) as f:
-            tr = json.load(f).get(args.case, {}).get("fp32", {})
+            tr = json.load(f).get(case.name, {}).get("fp32", {})
         traffic = tr.get(dom)
 
     def step_model(m, w):

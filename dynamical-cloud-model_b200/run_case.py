@@ -1,0 +1,76 @@
+"""Run K time steps of a named seeded case through the C-ABI and print the
+solver iterations and device time of each step.  A small driver for
+profiling single kernels (ncu -k ... on a few steps) and for quick checks.
+
+    python dynamical-cloud-model_b200/run_case.py --case warm_bubble \
+        --precision 1 --steps 1 [--host-loop]
+
+Cases: warm_bubble (256x256x128), sheared_convection (512x512x256, 8 tracers),
+kelvin_helmholtz (128x1x64), or warm_bubble_IPxJPxKP /
+sheared_convection_IPxJPxKP for other sizes.  --host-loop drives the
+pressure solve from the host (the same kernels; a profiler sees every
+launch, which it cannot inside the graph-driven solve's conditional loop).
+"""
+import argparse
+import importlib.util
+import os
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def load():
+    if "dcm_b200" in sys.modules:
+        return sys.modules["dcm_b200"]
+    spec = importlib.util.spec_from_file_location(
+        "dcm_b200", os.path.join(HERE, "__init__.py"), submodule_search_locations=[HERE])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["dcm_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def make_case(cases, name):
+    if name == "warm_bubble":
+        return cases.warm_bubble()
+    if name == "sheared_convection":
+        return cases.sheared_convection()
+    if name == "kelvin_helmholtz":
+        return cases.kelvin_helmholtz()
+    for stem, fn in (("warm_bubble_", cases.warm_bubble),
+                     ("sheared_convection_", cases.sheared_convection)):
+        if name.startswith(stem):
+            ip, jp, kp = (int(x) for x in name[len(stem):].split("x"))
+            return fn(ip=ip, jp=jp, kp=kp)
+    raise SystemExit("unknown case " + name)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--case", default="warm_bubble")
+    ap.add_argument("--precision", type=int, default=1, choices=[0, 1])
+    ap.add_argument("--steps", type=int, default=1)
+    ap.add_argument("--host-loop", action="store_true")
+    ap.add_argument("--device", type=int, default=0)
+    args = ap.parse_args()
+    dcm = load()
+    from dcm_b200 import cases
+    c = make_case(cases, args.case)
+    core = dcm.DynamicalCore(c.grid, device=args.device)
+    if args.host_loop:
+        core.solver_graphs(False)
+    kw = dict(nq=c.nq, c_s=c.c_s, c_e=c.c_e) if c.nq else {}
+    core.upload_state(c.state, c.dt, ptol=c.ptol, kord=c.kord, monotone=c.monotone,
+                      precision=args.precision, **kw)
+    core.driver_start()
+    for s in range(args.steps):
+        st = core.step(1)
+        print("%s precision %d step %d: %d iterations (%d updates, %d restarts), "
+              "err %.3e, %.2f ms" % (c.name, args.precision, s + 1, st.iters_last,
+                                     st.updates_last, st.restarts_last, st.err_last,
+                                     st.ms_total), flush=True)
+    core.close()
+
+
+if __name__ == "__main__":
+    main()
