@@ -215,6 +215,7 @@ SolverWork<double> solver_work(dcm_handle* h) {
     w.graph = h->graphs ? &h->g64 : nullptr;
     w.by = h->tune_by;
     w.tasks = h->tune_tasks;
+    w.max_blocks = (int)std::min<size_t>(h->npartials / 3, (size_t)1 << 30);
     return w;
 }
 
@@ -222,6 +223,7 @@ SolverWork<double> solver_work(dcm_handle* h) {
 // (the FP64 residual is formed from x and b directly, no FP64 work vectors).
 SolverWork<double> solver_scalars(dcm_handle* h) {
     SolverWork<double> w{};
+    w.max_blocks = (int)std::min<size_t>(h->npartials / 3, (size_t)1 << 30);
     w.ae = h->ae; w.aw = h->aw; w.an = h->an; w.as = h->as; w.au = h->au; w.ad = h->ad;
     w.partials = h->partials; w.ticket = h->ticket; w.S = h->S;
     w.red.partials = h->partials; w.red.gpartials = h->gpartials; w.red.gtick = h->gtick;
@@ -892,6 +894,7 @@ SolverWork<float> solver_work_f(dcm_handle* h) {
     w.graph = h->graphs ? &h->g32 : nullptr;
     w.by = h->tune_by;
     w.tasks = h->tune_tasks;
+    w.max_blocks = (int)std::min<size_t>(h->npartials / 3, (size_t)1 << 30);
     return w;
 }
 
@@ -1349,10 +1352,14 @@ __global__ void k_tune_rhs(Dims d, T* b, T* x) {
     const int j = 1 + blockIdx.y * BY + threadIdx.y;
     const int i = 1 + blockIdx.z;
     if (k > d.kp || j > d.jp) return;
-    // a smooth zero-mean right-hand side; x starts at zero
-    const double pi = 3.141592653589793;
-    b[d.at(k, j, i)] = (T)(sin(2.0 * pi * i / d.ip) * cos(2.0 * pi * j / d.jp) *
-                           cos(pi * (k - 0.5) / d.kp));
+    // hashed noise in [-1, 1): every mode of the operator is present, so the
+    // solve cannot finish early (a single eigenmode would converge in one
+    // iteration and then break down); x starts at zero
+    unsigned int hsh = (unsigned)k * 73856093u ^ (unsigned)j * 19349663u ^ (unsigned)i * 83492791u;
+    hsh ^= hsh >> 13;
+    hsh *= 0x5bd1e995u;
+    hsh ^= hsh >> 15;
+    b[d.at(k, j, i)] = (T)((double)(hsh & 0xffffffu) / 8388608.0 - 1.0);
     x[d.at(k, j, i)] = T(0);
 }
 

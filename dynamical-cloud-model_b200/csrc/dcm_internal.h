@@ -80,6 +80,9 @@ struct SolverWork {
     // resident blocks as the occupancy allows)
     int by = 8;
     int tasks = 0;
+    // most blocks a reducing kernel may use: the partials buffer holds
+    // 3 values per block (the largest NV of any reducing kernel)
+    int max_blocks = 0;
 };
 
 // per-field scalars of one MPDATA call

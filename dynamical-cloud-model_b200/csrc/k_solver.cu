@@ -62,6 +62,7 @@ struct SolverArgs {
     int max_cycle;    // mixed form: FP32 iterations between updates before a restart
     int by;           // warps per block of the non-reducing sweeps
     int tasks;        // warp tasks per warp of the reducing kernels (0: fill the GPU)
+    int max_blocks;   // blocks a reducing kernel may use (partials capacity)
 };
 
 // a_p exactly as set_mat_a forms it (dynamics.f90:93-95)
@@ -607,13 +608,18 @@ static int kchunks(const Dims& d) {
     return (d.kp + KVec<T>::V * BX - 1) / (KVec<T>::V * BX);
 }
 
-// blocks of a persistent reducing kernel: all resident blocks (tasks = 0),
-// or enough blocks for `tasks` warp tasks per warp
+// blocks of a reducing kernel: all resident blocks (tasks = 0: persistent,
+// each warp strides over many tasks), or enough blocks for `tasks` warp
+// tasks per warp (tasks = 1: one task per warp, as many blocks as tasks / 8),
+// never more than the reduction buffers hold
 static int red_grid(const SolverArgs& a, int full, int nkt) {
-    if (a.tasks <= 0) return full;
-    const long long ntask = (long long)nkt * a.d.jp * a.d.ip;
-    const long long want = (ntask + (long long)BY * a.tasks - 1) / ((long long)BY * a.tasks);
-    return (int)std::max(1LL, std::min((long long)full, want));
+    long long want = full;
+    if (a.tasks > 0) {
+        const long long ntask = (long long)nkt * a.d.jp * a.d.ip;
+        want = (ntask + (long long)BY * a.tasks - 1) / ((long long)BY * a.tasks);
+    }
+    if (a.max_blocks > 0) want = std::min(want, (long long)a.max_blocks);
+    return (int)std::max(1LL, want);
 }
 
 template <typename T, int OP, int MODE>
@@ -781,6 +787,7 @@ int solver_run(SolverWork<T>& w, const Dims& d, T* x, const T* b, const T* sw, c
     a.max_cycle = 0;
     a.by = w.by;
     a.tasks = w.tasks;
+    a.max_blocks = w.max_blocks;
     const Coef<T> c = coef_of(w);
     SolverBufs B{};
     B.x = x;
@@ -1045,6 +1052,7 @@ int refine_run(SolverWork<float>& wf, SolverWork<double>& wd, const Dims& d, dou
     a.max_cycle = 250;
     a.by = wf.by;
     a.tasks = wf.tasks;
+    a.max_blocks = wf.max_blocks;
     SolverArgs af = a;             // vector warp tasks of the FP32 iterations
     af.nkt = kchunks<float>(d);
     Coef<double> cd;
