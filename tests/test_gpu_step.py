@@ -24,8 +24,9 @@ def _run(dcm, orc, c, nsteps, **kw):
     its = [core.step(1).iters_last for _ in range(nsteps)]
     got = core.download_state()
     core.close()
+    okw = {k: v for k, v in kw.items() if k != "precision"}  # the oracle is FP64
     m = orc.OracleModel(c.grid, c.state, c.dt, ptol=c.ptol, kord=c.kord, monotone=c.monotone,
-                        nq=c.nq, c_s=c.c_s, c_e=c.c_e, **kw)
+                        nq=c.nq, c_s=c.c_s, c_e=c.c_e, **okw)
     m.driver_start()
     oits = [m.step(1)[0] for _ in range(nsteps)]
     return got, m.fields(), its, oits
@@ -100,3 +101,32 @@ def test_damping_forcing(dcm, orc):
                    w_subs=-1e-5 * z, forcing_tau=900.0)
     got, ref, its, oits = _run(dcm, orc, c, 2, forcing=forcing)
     _compare(c, got, ref, 1e-10)
+
+
+@pytest.mark.parametrize("shape", [(12, 10, 13), (8, 6, 130), (1, 16, 14), (10, 1, 9)])
+def test_ragged_and_degenerate_shapes(dcm, orc, shape):
+    """Column heights that are not a multiple of the 16-byte vector (13, 9),
+    columns longer than one warp's vector span (130 levels: two k-chunks in
+    both precisions), and the 2-D forms of the reference (ip = 1: y-z,
+    jp = 1: x-z) against the oracle after two steps."""
+    ip, jp, kp = shape
+    c = cases.warm_bubble(ip=ip, jp=jp, kp=kp, dxyz=50.0, radius=200.0, zc=200.0, seed=31)
+    # solved to 1e-13 so that a stopping point one iteration apart (dot
+    # products summed in another order) leaves round-off, not tolerance-sized,
+    # differences: any error at the vector or k-chunk seams would stand out
+    c.ptol = 1e-13
+    got, ref, its, oits = _run(dcm, orc, c, 2)
+    # near the round-off floor the stopping iteration varies by a few
+    assert max(abs(a - b) for a, b in zip(its, oits)) <= 3
+    errs = _compare(c, got, ref, 1e-10)
+    assert errs["p"] <= 1e-10
+
+
+@pytest.mark.parametrize("shape", [(12, 10, 13), (8, 6, 130), (1, 16, 14)])
+def test_ragged_shapes_mixed(dcm, orc, shape):
+    ip, jp, kp = shape
+    c = cases.warm_bubble(ip=ip, jp=jp, kp=kp, dxyz=50.0, radius=200.0, zc=200.0, seed=32)
+    got, ref, _, _ = _run(dcm, orc, c, 2, precision=1)
+    for n in ("u", "v", "w", "th"):
+        assert relerr(got[n], ref[n]) <= 1e-5, n
+    assert relerr(got["p"], ref["p"], live_mask_p(c.grid)) <= 1e-5
