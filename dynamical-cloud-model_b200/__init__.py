@@ -116,7 +116,8 @@ def library():
             "dcm_profile_enable": [P, C.c_int],
             "dcm_profile_read": [P, _dp, C.POINTER(C.c_longlong), C.c_int],
             "dcm_solver_graphs": [P, C.c_int],
-            "dcm_tune": [P, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)],
+            "dcm_tune": [P, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                         C.POINTER(C.c_int)],
             "dcm_ensemble_create": [C.c_int, C.c_void_p, C.c_int, C.POINTER(C.c_void_p)],
             "dcm_ensemble_destroy": [P],
             "dcm_ensemble_member": [P, C.c_int, C.POINTER(C.c_void_p)],
@@ -209,11 +210,11 @@ class DynamicalCore:
 
     def tune(self, precision=1, use_cache=True):
         """Autotune the solver launch shape for this grid (dcm_tune);
-        returns (warps per sweep block, warp tasks per warp)."""
-        by, tasks = C.c_int(), C.c_int()
+        returns (warps per sweep block, warp tasks per warp, marching depth)."""
+        by, tasks, depth = C.c_int(), C.c_int(), C.c_int()
         self._check(self.lib.dcm_tune(self.h, int(precision), int(bool(use_cache)), C.byref(by),
-                                      C.byref(tasks)))
-        return by.value, tasks.value
+                                      C.byref(tasks), C.byref(depth)))
+        return by.value, tasks.value, depth.value
 
     def __del__(self):
         try:

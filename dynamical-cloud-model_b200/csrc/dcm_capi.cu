@@ -88,7 +88,7 @@ struct dcm_handle {
     bool graphs = true;  // graph-driven solver loops (else host-polled)
     // launch shape of the solver kernels (dcm_tune): warps per sweep block,
     // warp tasks per warp of the reducing kernels (0 = fill the GPU)
-    int tune_by = 8, tune_tasks = 0;
+    int tune_by = 8, tune_tasks = 0, tune_ni = 4;
     // bumped whenever captured pointers or launch shapes change (state
     // upload, tuning); an ensemble rebuilds its step graphs when it moves
     unsigned generation = 0;
@@ -215,6 +215,7 @@ SolverWork<double> solver_work(dcm_handle* h) {
     w.graph = h->graphs ? &h->g64 : nullptr;
     w.by = h->tune_by;
     w.tasks = h->tune_tasks;
+    w.ni = h->tune_ni;
     w.max_blocks = (int)std::min<size_t>(h->npartials / 3, (size_t)1 << 30);
     return w;
 }
@@ -894,6 +895,7 @@ SolverWork<float> solver_work_f(dcm_handle* h) {
     w.graph = h->graphs ? &h->g32 : nullptr;
     w.by = h->tune_by;
     w.tasks = h->tune_tasks;
+    w.ni = h->tune_ni;
     w.max_blocks = (int)std::min<size_t>(h->npartials / 3, (size_t)1 << 30);
     return w;
 }
@@ -1321,29 +1323,30 @@ std::string tune_cache_path() {
     return std::string(home ? home : ".") + "/.cache/dcm_b200_solver_tune.txt";
 }
 
-// cache lines: "<sms> <ip> <jp> <kp> <precision> <by> <tasks> <ms per iteration>"
-bool tune_lookup(int sms, const Dims& d, int prec, int* by, int* tasks) {
+// cache lines: "<sms> <ip> <jp> <kp> <precision> <by> <tasks> <depth> <ms per iteration>"
+bool tune_lookup(int sms, const Dims& d, int prec, int* by, int* tasks, int* depth) {
     std::ifstream f(tune_cache_path());
     std::string line;
     bool found = false;
     while (std::getline(f, line)) {
         std::istringstream is(line);
-        int a[7];
+        int a[8];
         double ms;
-        if (!(is >> a[0] >> a[1] >> a[2] >> a[3] >> a[4] >> a[5] >> a[6] >> ms)) continue;
+        if (!(is >> a[0] >> a[1] >> a[2] >> a[3] >> a[4] >> a[5] >> a[6] >> a[7] >> ms)) continue;
         if (a[0] == sms && a[1] == d.ip && a[2] == d.jp && a[3] == d.kp && a[4] == prec) {
             *by = a[5];
             *tasks = a[6];
+            *depth = a[7];
             found = true;  // the last entry wins
         }
     }
     return found;
 }
 
-void tune_store(int sms, const Dims& d, int prec, int by, int tasks, double ms) {
+void tune_store(int sms, const Dims& d, int prec, int by, int tasks, int depth, double ms) {
     std::ofstream f(tune_cache_path(), std::ios::app);
     if (f) f << sms << ' ' << d.ip << ' ' << d.jp << ' ' << d.kp << ' ' << prec << ' ' << by << ' '
-             << tasks << ' ' << ms << '\n';
+             << tasks << ' ' << depth << ' ' << ms << '\n';
 }
 
 template <typename T>
@@ -1366,7 +1369,7 @@ __global__ void k_tune_rhs(Dims d, T* b, T* x) {
 // device time of `iters` iterations of the solver in precision T with the
 // given launch shape (graph-driven, tolerance unreachable, itmax = iters)
 template <typename T>
-double tune_time(dcm_handle* h, int by, int tasks, int iters) {
+double tune_time(dcm_handle* h, int by, int tasks, int depth, int iters) {
     SolverWork<T> w;
     T *x, *b;
     if constexpr (std::is_same<T, double>::value) {
@@ -1383,6 +1386,7 @@ double tune_time(dcm_handle* h, int by, int tasks, int iters) {
     w.graph = &G;
     w.by = by;
     w.tasks = tasks;
+    w.ni = depth;
     const Metrics<T>& mt = metrics_of<T>(h);
     double best = 1e30;
     for (int rep = 0; rep < 3; rep++) {
@@ -1403,33 +1407,40 @@ double tune_time(dcm_handle* h, int by, int tasks, int iters) {
 
 }  // namespace
 
-extern "C" int dcm_tune(dcm_handle* h, int precision, int use_cache, int* by, int* tasks) {
+extern "C" int dcm_tune(dcm_handle* h, int precision, int use_cache, int* by, int* tasks,
+                        int* depth) {
     CHECK_H();
     if (precision != 0 && precision != 1) return fail(h, DCM_E_ARG, "tune: precision");
     int sms = 0;
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
-    int b0 = 8, t0 = 0;
-    if (!(use_cache && tune_lookup(sms, h->d, precision, &b0, &t0))) {
-        static const int BYS[3] = {2, 4, 8}, TASKS[4] = {0, 1, 2, 4};
+    int b0 = 8, t0 = 0, n0 = 4;
+    if (!(use_cache && tune_lookup(sms, h->d, precision, &b0, &t0, &n0))) {
+        static const int BYS[3] = {2, 4, 8}, TASKS[3] = {0, 1, 2}, DEPTHS[4] = {1, 2, 4, 8};
         double best = 1e30;
         for (int bi = 0; bi < 3; bi++)
-            for (int ti = 0; ti < 4; ti++) {
-                const double ms = precision == 0 ? tune_time<double>(h, BYS[bi], TASKS[ti], 12)
-                                                 : tune_time<float>(h, BYS[bi], TASKS[ti], 12);
-                if (ms < 0) return fail(h, DCM_E_CUDA, "tune: a candidate launch shape failed");
-                if (ms < best) {
-                    best = ms;
-                    b0 = BYS[bi];
-                    t0 = TASKS[ti];
+            for (int ti = 0; ti < 3; ti++)
+                for (int ni = 0; ni < 4; ni++) {
+                    const double ms =
+                        precision == 0 ? tune_time<double>(h, BYS[bi], TASKS[ti], DEPTHS[ni], 12)
+                                       : tune_time<float>(h, BYS[bi], TASKS[ti], DEPTHS[ni], 12);
+                    if (ms < 0)
+                        return fail(h, DCM_E_CUDA, "tune: a candidate launch shape failed");
+                    if (ms < best) {
+                        best = ms;
+                        b0 = BYS[bi];
+                        t0 = TASKS[ti];
+                        n0 = DEPTHS[ni];
+                    }
                 }
-            }
-        tune_store(sms, h->d, precision, b0, t0, best);
+        tune_store(sms, h->d, precision, b0, t0, n0, best);
     }
     h->tune_by = b0;
     h->tune_tasks = t0;
+    h->tune_ni = n0;
     h->generation += 1;
     if (by) *by = b0;
     if (tasks) *tasks = t0;
+    if (depth) *depth = n0;
     return DCM_OK;
 }
 

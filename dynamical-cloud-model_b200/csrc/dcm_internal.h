@@ -83,6 +83,8 @@ struct SolverWork {
     // most blocks a reducing kernel may use: the partials buffer holds
     // 3 values per block (the largest NV of any reducing kernel)
     int max_blocks = 0;
+    // i-planes each stencil warp task marches over (tuning)
+    int ni = 4;
 };
 
 // per-field scalars of one MPDATA call

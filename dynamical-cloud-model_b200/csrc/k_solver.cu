@@ -63,6 +63,7 @@ struct SolverArgs {
     int by;           // warps per block of the non-reducing sweeps
     int tasks;        // warp tasks per warp of the reducing kernels (0: fill the GPU)
     int max_blocks;   // blocks a reducing kernel may use (partials capacity)
+    int ni;           // i-planes a stencil warp task marches over
 };
 
 // a_p exactly as set_mat_a forms it (dynamics.f90:93-95)
@@ -227,14 +228,17 @@ __device__ __forceinline__ T xload1(const StenCtx<T, OP, MODE>& C, int o) {
 }
 
 // One warp task: V x 32 consecutive k-levels (lane l holds k0 = 1 +
-// V (32 kc + l) .. k0 + V - 1) of row j, plane i.  k neighbours are the
-// adjacent vector elements, the neighbour lanes' end elements by shuffle, and
-// at the warp's two ends one scalar load each; Neumann mirror at k = 1, kp
-// (dynamics.f90:206-211).  j and i neighbours (periodic) are vector loads of
-// the adjacent columns.
-template <typename T, int OP, int MODE, int NV>
-__device__ __forceinline__ void sten_task(const StenCtx<T, OP, MODE>& C, int kc, int j, int i,
-                                          double (&acc)[NV]) {
+// V (32 kc + l) .. k0 + V - 1) of row j, marching over the planes
+// i0 .. i0 + ni - 1.  k neighbours are the adjacent vector elements, the
+// neighbour lanes' end elements by shuffle, and at the warp's two ends one
+// scalar load each; Neumann mirror at k = 1, kp (dynamics.f90:206-211).  j
+// neighbours (periodic) are vector loads of the adjacent columns; the i
+// neighbours are the previous and the next plane of the march, kept in
+// registers, so each plane loads its i + 1 column and its two j neighbours.
+template <typename T, int OP, int MODE, int NV, bool MARCH>
+__device__ __forceinline__ void sten_task(const StenCtx<T, OP, MODE>& C, int kc, int j, int i0,
+                                          int ni, double (&acc)[NV]) {
+    if (!MARCH) ni = 1;
     constexpr int V = KVec<T>::V;
     const Dims& d = C.d;
     const int lane = threadIdx.x & 31;
@@ -243,25 +247,29 @@ __device__ __forceinline__ void sten_task(const StenCtx<T, OP, MODE>& C, int kc,
     const bool live = k0 <= kp;
     const int nvalid = live ? min(V, kp - k0 + 1) : 0;
     const int K = d.K, KJ = d.K * d.J;
-    const int o = (live ? k0 : 1) + K * j + KJ * i;  // idle lanes read column start
-    const int os = o + (j == 1 ? jp - 1 : -1) * K, on = o + (j == jp ? 1 - jp : 1) * K;
-    const int ow = o + (i == 1 ? ip - 1 : -1) * KJ, oe = o + (i == ip ? 1 - ip : 1) * KJ;
-    T xc[V], xs[V], xn[V], xw[V], xe[V];
-    xload(C, o, xc);
-    xload(C, os, xs);
-    xload(C, on, xn);
-    xload(C, ow, xw);
-    xload(C, oe, xe);
-    T prev = __shfl_up_sync(0xffffffffu, xc[V - 1], 1);
-    T next = __shfl_down_sync(0xffffffffu, xc[0], 1);
-    if (lane == 0 && live && k0 > 1) prev = xload1(C, o - 1);
-    if (lane == BX - 1 && live && k0 + V <= kp) next = xload1(C, o + V);
+    const int col = (live ? k0 : 1) + K * j;  // idle lanes read the column start
+    const int dsj = (j == 1 ? jp - 1 : -1) * K, dnj = (j == jp ? 1 - jp : 1) * K;
     const Coef<T>& c = C.c;
     T au[V], ad[V];
     vld(c.au + (live ? k0 : 1), au);
     vld(c.ad + (live ? k0 : 1), ad);
-    const T sij = -ld(c.ae + i) - ld(c.aw + i) - ld(c.an + j) - ld(c.as + j);
-    const T ae = ld(c.ae + i), aw = ld(c.aw + i), an = ld(c.an + j), as = ld(c.as + j);
+    const T an = ld(c.an + j), as = ld(c.as + j);
+    const int iend = MARCH ? min(i0 + ni - 1, ip) : i0;
+    T xw[V], xc[V], xe[V];
+    xload(C, col + KJ * (i0 == 1 ? ip : i0 - 1), xw);
+    xload(C, col + KJ * i0, xc);
+    for (int i = i0; i <= iend; i++) {
+    const int o = col + KJ * i;
+    T xs[V], xn[V];
+    xload(C, col + KJ * (i == ip ? 1 : i + 1), xe);
+    xload(C, o + dsj, xs);
+    xload(C, o + dnj, xn);
+    T prev = __shfl_up_sync(0xffffffffu, xc[V - 1], 1);
+    T next = __shfl_down_sync(0xffffffffu, xc[0], 1);
+    if (lane == 0 && live && k0 > 1) prev = xload1(C, o - 1);
+    if (lane == BX - 1 && live && k0 + V <= kp) next = xload1(C, o + V);
+    const T ae = ld(c.ae + i), aw = ld(c.aw + i);
+    const T sij = -ae - aw - an - as;
     T ap[V], Ax[V];
 #pragma unroll
     for (int q = 0; q < V; q++) {
@@ -356,6 +364,12 @@ __device__ __forceinline__ void sten_task(const StenCtx<T, OP, MODE>& C, int kc,
         }
         if (live) vst(out + o, res, nvalid);
     }
+#pragma unroll
+    for (int q = 0; q < V; q++) {
+        xw[q] = xc[q];
+        xc[q] = xe[q];
+    }
+    }
 }
 
 // block and grid reduction of a reducing stencil kernel, then the scalar
@@ -439,14 +453,20 @@ __global__ void __launch_bounds__(256) k_sten(SolverArgs a, Coef<T> c, SolverBuf
     double acc[NV];
 #pragma unroll
     for (int q = 0; q < NV; q++) acc[q] = 0.0;
+    // only the first sweep marches: it rebuilds s0 from r/a_p and v1/a_p at
+    // every neighbour, and the march reuses the i-1 and i+1 values; for the
+    // other kernels the extra registers cost more occupancy than they save
+    constexpr bool MARCH = OP == OP_SW1;
+    const int ni = MARCH ? a.ni : 1;
     if constexpr (!RED) {
         const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
-        if (j <= d.jp) sten_task<T, OP, MODE, NV>(C, blockIdx.x, j, 1 + blockIdx.z, acc);
+        if (j <= d.jp)
+            sten_task<T, OP, MODE, NV, MARCH>(C, blockIdx.x, j, 1 + blockIdx.z * ni, ni, acc);
     } else {
         for (TaskIter t(blockIdx.x * blockDim.y + threadIdx.y, gridDim.x * blockDim.y, a.nkt,
                         d.jp);
              t.i <= d.ip; t.next())
-            sten_task<T, OP, MODE, NV>(C, t.kt, 1 + t.jr, t.i, acc);
+            sten_task<T, OP, MODE, NV, false>(C, t.kt, 1 + t.jr, t.i, 1, acc);
         reduce_tail<OP, NV>(a, acc, R, smem, S);
     }
 }
@@ -612,10 +632,10 @@ static int kchunks(const Dims& d) {
 // each warp strides over many tasks), or enough blocks for `tasks` warp
 // tasks per warp (tasks = 1: one task per warp, as many blocks as tasks / 8),
 // never more than the reduction buffers hold
-static int red_grid(const SolverArgs& a, int full, int nkt) {
+static int red_grid(const SolverArgs& a, int full, int nkt, int ni = 1) {
     long long want = full;
     if (a.tasks > 0) {
-        const long long ntask = (long long)nkt * a.d.jp * a.d.ip;
+        const long long ntask = (long long)nkt * a.d.jp * ((a.d.ip + ni - 1) / ni);
         want = (ntask + (long long)BY * a.tasks - 1) / ((long long)BY * a.tasks);
     }
     if (a.max_blocks > 0) want = std::min(want, (long long)a.max_blocks);
@@ -630,12 +650,13 @@ static void sten(const SolverArgs& a, const Coef<T>& c, const SolverBufs& B, Sol
     if (RED) {
         static int full = 0;
         if (!full) full = persistent_grid(k_sten<T, OP, MODE>);
-        k_sten<T, OP, MODE><<<red_grid(a, full, a.nkt), dim3(BX, BY), 0, st>>>(a, c, B, w.red,
-                                                                                w.S);
+        k_sten<T, OP, MODE><<<red_grid(a, full, a.nkt, 1), dim3(BX, BY), 0, st>>>(
+            a, c, B, w.red, w.S);
     } else {
         // at most 256 threads: the kernels are compiled with __launch_bounds__(256)
         const int by = a.by >= 1 && a.by <= 256 / BX ? a.by : BY;
-        const dim3 grid(a.nkt, (a.d.jp + by - 1) / by, a.d.ip);
+        const int ni = OP == OP_SW1 ? a.ni : 1;
+        const dim3 grid(a.nkt, (a.d.jp + by - 1) / by, (a.d.ip + ni - 1) / ni);
         k_sten<T, OP, MODE><<<grid, dim3(BX, by), 0, st>>>(a, c, B, w.red, w.S);
     }
 }
@@ -788,6 +809,7 @@ int solver_run(SolverWork<T>& w, const Dims& d, T* x, const T* b, const T* sw, c
     a.by = w.by;
     a.tasks = w.tasks;
     a.max_blocks = w.max_blocks;
+    a.ni = w.ni >= 1 ? w.ni : 1;
     const Coef<T> c = coef_of(w);
     SolverBufs B{};
     B.x = x;
@@ -828,7 +850,7 @@ int solver_run(SolverWork<T>& w, const Dims& d, T* x, const T* b, const T* sw, c
         const void* kp[6] = {x, b, sw, dzn, w.r, w.S};
         const double kd[3] = {tol, sc_floor, 0.0};
         const int ki[6] = {itmax, wo, post ? 1 : 0, (int)sizeof(T), d.ip * 4096 + d.jp,
-                           d.kp + 65536 * (a.by + 64 * a.tasks)};
+                           d.kp + 65536 * (a.by + 64 * a.tasks + 1024 * a.ni)};
         if (!G.matches(kp, kd, ki)) {
             G.release();
             bool good = ok(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
@@ -1053,8 +1075,10 @@ int refine_run(SolverWork<float>& wf, SolverWork<double>& wd, const Dims& d, dou
     a.by = wf.by;
     a.tasks = wf.tasks;
     a.max_blocks = wf.max_blocks;
+    a.ni = 1;                      // the FP64 residual does not march
     SolverArgs af = a;             // vector warp tasks of the FP32 iterations
     af.nkt = kchunks<float>(d);
+    af.ni = wf.ni >= 1 ? wf.ni : 1;
     Coef<double> cd;
     cd.ae = wd.ae; cd.aw = wd.aw; cd.an = wd.an; cd.as = wd.as; cd.au = wd.au; cd.ad = wd.ad;
     const Coef<float> cf = coef_of(wf);
@@ -1121,7 +1145,7 @@ int refine_run(SolverWork<float>& wf, SolverWork<double>& wd, const Dims& d, dou
         const void* kp[6] = {x, b, sw, dzn, dx, wf.S};
         const double kd[3] = {tol, delta, 0.0};
         const int ki[6] = {itmax, max_updates, 1, 0, d.ip * 4096 + d.jp,
-                           d.kp + 65536 * (af.by + 64 * af.tasks)};
+                           d.kp + 65536 * (af.by + 64 * af.tasks + 1024 * af.ni)};
         if (!G.matches(kp, kd, ki)) {
             G.release();
             bool good = ok(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
