@@ -157,6 +157,47 @@ def pinned_like(a):
     return v, t
 
 
+class Ranks:
+    """The ranks of a torchrun launch (or one process): barrier and max / sum
+    reductions of host scalars over the process group (NCCL on GPUs, gloo in
+    the CPU tests)."""
+
+    def __init__(self, dist=None):
+        self.dist = dist
+        self.rank = dist.get_rank() if dist is not None else 0
+        self.world = dist.get_world_size() if dist is not None else 1
+
+    def _device(self):
+        return "cuda" if self.dist.get_backend() == "nccl" else "cpu"
+
+    def barrier(self):
+        if self.dist is not None:
+            if self._device() == "cuda":
+                import torch
+                torch.cuda.synchronize()
+            self.dist.barrier()
+
+    def _reduce(self, x, op):
+        if self.dist is None:
+            return float(x)
+        import torch
+        t = torch.tensor([float(x)], dtype=torch.float64, device=self._device())
+        self.dist.all_reduce(t, op=op)
+        return float(t.item())
+
+    def max(self, x):
+        return self._reduce(x, self.dist.ReduceOp.MAX if self.dist else None)
+
+    def sum(self, x):
+        return self._reduce(x, self.dist.ReduceOp.SUM if self.dist else None)
+
+
+def partition(items, rank, world):
+    """Ensemble members of one rank: every world-th member from `rank`
+    (members are independent, so no data-path collective)."""
+    return items[rank::world]
+
+
 def live_mask_p(g):
     """Cells of p the reference computes and later reads (all but the halo
     rings of the top/bottom rows and the vertical halo edges)."""
@@ -207,24 +248,15 @@ def run_b200(args, rank, world, local_rank, dist):
         core.upload_state(case.state, case.dt, precision=prec, **kw)
         core.driver_start()
 
-    def barrier():
-        if dist is not None:
-            import torch
-            torch.cuda.synchronize()
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if dist is None:
-            return x
-        import torch
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    R = Ranks(dist)
+    barrier, max_over_ranks = R.barrier, R.max
 
     def measure(prec):
         """Steps 1..K of one precision: device time (CUDA events on the
         library stream, max over ranks), launches, clocks, then the same
-        steps again with per-kernel-class events for the roofline."""
+        steps again with per-kernel-class events for the roofline.  The
+        solver launch shape is the autotuner's for this grid (cached)."""
+        shape = core.tune(precision=prec, use_cache=True)
         fresh(prec)  # warm-up run (allocations, first launches)
         if args.warmup:
             core.step(args.warmup)
@@ -245,7 +277,9 @@ def run_b200(args, rank, world, local_rank, dist):
         core.profile(False)
         classes = {k: v for k, v in prof.items() if v[1] > 0}
         return dict(ms=ms, iters=st.iters_total, launches=launches, clocks=clk,
-                    classes=classes, value=world * N * args.steps / (ms / 1e3))
+                    classes=classes, value=world * N * args.steps / (ms / 1e3),
+                    shape={"warps_per_sweep_block": shape[0], "tasks_per_warp": shape[1],
+                           "march_depth": shape[2]})
 
     m32 = measure(1)
     m64 = measure(0)
@@ -326,9 +360,11 @@ def run_b200(args, rank, world, local_rank, dist):
                    "monotone": bool(case.monotone), "ptol": case.ptol,
                    "timed_steps": "1..%d from the initial state" % args.steps,
                    "bicgstab_iters_per_step": m32["iters"] / args.steps,
+                   "tuned_launch_shape": m32["shape"],
                    "l2": "inputs larger than L2 (about 40 fields of 34-69 MB resident)",
                    "parallelism": "replicas" if world > 1 else "single GPU"},
         "fp64": {"value": m64["value"], "ms_per_step": m64["ms"] / args.steps,
+                 "tuned_launch_shape": m64["shape"],
                  "bicgstab_iters_per_step": m64["iters"] / args.steps,
                  "gpu_launches": m64["launches"], "clocks": m64["clocks"],
                  "step_model": step_model(m64, 8.0),
@@ -357,7 +393,7 @@ def run_ensemble(args, rank, world, local_rank, dist):
     pkg = load_pkg()
     from dcm_b200 import cases
     spec = cases.ensemble_members(args.members)
-    mine = spec[rank::world]
+    mine = partition(spec, rank, world)
     mcases = [cases.warm_bubble(ip=ip, jp=jp, kp=kp, amp=amp, seed=seed)
               for (ip, jp, kp, amp, seed) in mine]
     ens = pkg.Ensemble([c.grid for c in mcases], device=local_rank)
@@ -374,28 +410,8 @@ def run_ensemble(args, rank, world, local_rank, dist):
                               precision=1)
             core.driver_start()
 
-    def barrier():
-        if dist is not None:
-            import torch
-            torch.cuda.synchronize()
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if dist is None:
-            return x
-        import torch
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    def sum_over_ranks(x):
-        if dist is None:
-            return x
-        import torch
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        return float(t.item())
-
+    R = Ranks(dist)
+    barrier, max_over_ranks, sum_over_ranks = R.barrier, R.max, R.sum
     points = sum(c.grid.npoints for c in mcases)
     fresh()
     if args.warmup:

@@ -86,9 +86,10 @@ struct dcm_handle {
     // arguments change
     SolveGraph g64, g32;
     bool graphs = true;  // graph-driven solver loops (else host-polled)
-    // launch shape of the solver kernels (dcm_tune): warps per sweep block,
-    // warp tasks per warp of the reducing kernels (0 = fill the GPU)
-    int tune_by = 8, tune_tasks = 0, tune_ni = 4;
+    // launch shape of the solver kernels per precision (dcm_tune; [0] FP64,
+    // [1] the FP32 iterations of the mixed form): warps per sweep block, warp
+    // tasks per warp of the reducing kernels (0 = fill the GPU), marching depth
+    int tune_by[2] = {8, 8}, tune_tasks[2] = {0, 0}, tune_ni[2] = {4, 4};
     // bumped whenever captured pointers or launch shapes change (state
     // upload, tuning); an ensemble rebuilds its step graphs when it moves
     unsigned generation = 0;
@@ -213,9 +214,9 @@ SolverWork<double> solver_work(dcm_handle* h) {
     w.red.partials = h->partials; w.red.gpartials = h->gpartials; w.red.gtick = h->gtick;
     w.red.ticket = h->ticket2;
     w.graph = h->graphs ? &h->g64 : nullptr;
-    w.by = h->tune_by;
-    w.tasks = h->tune_tasks;
-    w.ni = h->tune_ni;
+    w.by = h->tune_by[0];
+    w.tasks = h->tune_tasks[0];
+    w.ni = h->tune_ni[0];
     w.max_blocks = (int)std::min<size_t>(h->npartials / 3, (size_t)1 << 30);
     return w;
 }
@@ -893,9 +894,9 @@ SolverWork<float> solver_work_f(dcm_handle* h) {
     w.red.partials = h->partials; w.red.gpartials = h->gpartials; w.red.gtick = h->gtick;
     w.red.ticket = h->ticket2;
     w.graph = h->graphs ? &h->g32 : nullptr;
-    w.by = h->tune_by;
-    w.tasks = h->tune_tasks;
-    w.ni = h->tune_ni;
+    w.by = h->tune_by[1];
+    w.tasks = h->tune_tasks[1];
+    w.ni = h->tune_ni[1];
     w.max_blocks = (int)std::min<size_t>(h->npartials / 3, (size_t)1 << 30);
     return w;
 }
@@ -1434,9 +1435,9 @@ extern "C" int dcm_tune(dcm_handle* h, int precision, int use_cache, int* by, in
                 }
         tune_store(sms, h->d, precision, b0, t0, n0, best);
     }
-    h->tune_by = b0;
-    h->tune_tasks = t0;
-    h->tune_ni = n0;
+    h->tune_by[precision] = b0;
+    h->tune_tasks[precision] = t0;
+    h->tune_ni[precision] = n0;
     h->generation += 1;
     if (by) *by = b0;
     if (tasks) *tasks = t0;

@@ -265,7 +265,8 @@ int dcm_solver_graphs(dcm_handle *h, int on);
  * warp striding over many tasks; 1, 2 = that many tasks per warp) and the
  * depth, the number of i-planes each stencil warp task marches over (1, 2,
  * 4, 8), by timing 12 BiCGSTAB iterations of each of the 36 shapes on a
- * synthetic right-hand side, then applies the fastest to the handle.  With
+ * synthetic right-hand side, then applies the fastest to the handle for
+ * that precision (each precision keeps its own launch shape).  With
  * use_cache the result is looked up first in, and otherwise appended to, a
  * text file: $DCM_TUNE_CACHE, or $HOME/.cache/dcm_b200_solver_tune.txt (one
  * line per SM count, grid shape and precision).  Uses the handle's scratch
