@@ -114,6 +114,11 @@ struct StenCtx {
     bool first;
 };
 
+// Ask L2 for the line holding p ahead of its use (no register is written).
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
 // Warp-task iterator of the persistent kernels: task t = kt + nkt*(jr +
 // njr*(i-1)), visited at start, start+stride, ...; the stride is split into
 // its (kt, jr, i) parts once so that each step is a carry chain, not a divide.
@@ -463,10 +468,28 @@ __global__ void __launch_bounds__(256) k_sten(SolverArgs a, Coef<T> c, SolverBuf
         if (j <= d.jp)
             sten_task<T, OP, MODE, NV, MARCH>(C, blockIdx.x, j, 1 + blockIdx.z * ni, ni, acc);
     } else {
+        constexpr int V = KVec<T>::V;
+        const int lane = threadIdx.x & 31;
         for (TaskIter t(blockIdx.x * blockDim.y + threadIdx.y, gridDim.x * blockDim.y, a.nkt,
                         d.jp);
-             t.i <= d.ip; t.next())
+             t.i <= d.ip; t.next()) {
+            // the next task's streamed columns into L2 while this one runs:
+            // a warp's tasks are otherwise serialised by their stores
+            TaskIter u = t;
+            u.next();
+            if (u.i <= d.ip) {
+                const int k0 = min(1 + V * (u.kt * BX + lane), d.kp);
+                const int o = d.at(k0, 1 + u.jr, u.i);
+                prefetch_l2(C.gx + o);
+                if (OP == OP_SETUP) prefetch_l2((const T*)B.b + o);
+                if (OP == OP_MATP) prefetch_l2((const T*)B.cr + o);
+                if (OP == OP_MATC) {
+                    prefetch_l2((const T*)B.r + o);
+                    prefetch_l2((const T*)B.v1 + o);
+                }
+            }
             sten_task<T, OP, MODE, NV, false>(C, t.kt, 1 + t.jr, t.i, 1, acc);
+        }
         reduce_tail<OP, NV>(a, acc, R, smem, S);
     }
 }
@@ -492,6 +515,20 @@ __global__ void __launch_bounds__(256) k_bicg_update(SolverArgs a, Coef<T> c,
     const int lane = threadIdx.x;
     for (TaskIter tk(blockIdx.x * blockDim.y + threadIdx.y, gridDim.x * blockDim.y, a.nkt, d.jp);
          tk.i <= d.ip; tk.next()) {
+        {
+            TaskIter u = tk;  // the next task's seven streamed columns into L2
+            u.next();
+            if (u.i <= d.ip) {
+                const int on = d.at(min(1 + V * (u.kt * BX + lane), d.kp), 1 + u.jr, u.i);
+                prefetch_l2(x + on);
+                prefetch_l2(p + on);
+                prefetch_l2(cs + on);
+                prefetch_l2(r + on);
+                prefetch_l2(v1 + on);
+                prefetch_l2(t + on);
+                prefetch_l2(cr + on);
+            }
+        }
         const int k0 = 1 + V * (tk.kt * BX + lane);
         if (k0 > d.kp) continue;
         const int nvalid = min(V, d.kp - k0 + 1);
