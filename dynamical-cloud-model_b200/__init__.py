@@ -117,7 +117,8 @@ def library():
             "dcm_profile_read": [P, _dp, C.POINTER(C.c_longlong), C.c_int],
             "dcm_solver_graphs": [P, C.c_int],
             "dcm_tune": [P, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
-                         C.POINTER(C.c_int)],
+                         C.POINTER(C.c_int), C.POINTER(C.c_int)],
+            "dcm_set_launch_shape": [P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int],
             "dcm_ensemble_create": [C.c_int, C.c_void_p, C.c_int, C.POINTER(C.c_void_p)],
             "dcm_ensemble_destroy": [P],
             "dcm_ensemble_member": [P, C.c_int, C.POINTER(C.c_void_p)],
@@ -141,7 +142,7 @@ EXPORTS = ("dcm_create", "dcm_destroy", "dcm_status_string", "dcm_last_error",
            "dcm_exchange_along_dim", "dcm_exchange_along_dim_wo", "dcm_state_upload",
            "dcm_driver_start", "dcm_step", "dcm_state_download", "dcm_profile_enable",
            "dcm_profile_read", "dcm_horizontal_means_noalloc", "dcm_solver_graphs", "dcm_tune",
-           "dcm_ensemble_create", "dcm_ensemble_destroy", "dcm_ensemble_member",
+           "dcm_set_launch_shape", "dcm_ensemble_create", "dcm_ensemble_destroy", "dcm_ensemble_member",
            "dcm_ensemble_step", "dcm_ensemble_last_error")
 
 PROF_CLASSES = ("setup", "jacobi", "matvec", "update", "post", "means", "sources", "rhs",
@@ -209,12 +210,19 @@ class DynamicalCore:
             self.h = None
 
     def tune(self, precision=1, use_cache=True):
-        """Autotune the solver launch shape for this grid (dcm_tune);
-        returns (warps per sweep block, warp tasks per warp, marching depth)."""
-        by, tasks, depth = C.c_int(), C.c_int(), C.c_int()
+        """Autotune the solver launch shape for this grid (dcm_tune); returns
+        (warps per sweep block, warp tasks per warp, marching depth, fused)."""
+        by, tasks, depth, fuse = C.c_int(), C.c_int(), C.c_int(), C.c_int()
         self._check(self.lib.dcm_tune(self.h, int(precision), int(bool(use_cache)), C.byref(by),
-                                      C.byref(tasks), C.byref(depth)))
-        return by.value, tasks.value, depth.value
+                                      C.byref(tasks), C.byref(depth), C.byref(fuse)))
+        return by.value, tasks.value, depth.value, fuse.value
+
+    def set_launch_shape(self, precision, by=8, tasks=0, depth=4, fuse=None):
+        """Set the solver launch shape of one precision (dcm_set_launch_shape)."""
+        if fuse is None:
+            fuse = 1 if precision == 1 else 0
+        self._check(self.lib.dcm_set_launch_shape(self.h, int(precision), int(by), int(tasks),
+                                                  int(depth), int(fuse)))
 
     def __del__(self):
         try:

@@ -89,7 +89,7 @@ struct dcm_handle {
     // launch shape of the solver kernels per precision (dcm_tune; [0] FP64,
     // [1] the FP32 iterations of the mixed form): warps per sweep block, warp
     // tasks per warp of the reducing kernels (0 = fill the GPU), marching depth
-    int tune_by[2] = {8, 8}, tune_tasks[2] = {0, 0}, tune_ni[2] = {4, 4};
+    int tune_by[2] = {8, 8}, tune_tasks[2] = {0, 0}, tune_ni[2] = {4, 4}, tune_fuse[2] = {0, 1};
     // bumped whenever captured pointers or launch shapes change (state
     // upload, tuning); an ensemble rebuilds its step graphs when it moves
     unsigned generation = 0;
@@ -217,6 +217,7 @@ SolverWork<double> solver_work(dcm_handle* h) {
     w.by = h->tune_by[0];
     w.tasks = h->tune_tasks[0];
     w.ni = h->tune_ni[0];
+    w.fuse = 0;
     w.max_blocks = (int)std::min<size_t>(h->npartials / 3, (size_t)1 << 30);
     return w;
 }
@@ -340,6 +341,7 @@ extern "C" int dcm_create(const dcm_grid* g, int device, dcm_handle** out) {
     h->nh = h->hd.n();
     CK(cudaSetDevice(device));
     CK(cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking));
+    solver_init();
     CK(cudaEventCreate(&h->ev0));
     CK(cudaEventCreate(&h->ev1));
     const size_t I2 = g->ip + 2, J2 = g->jp + 2, K2 = g->kp + 2;
@@ -897,6 +899,7 @@ SolverWork<float> solver_work_f(dcm_handle* h) {
     w.by = h->tune_by[1];
     w.tasks = h->tune_tasks[1];
     w.ni = h->tune_ni[1];
+    w.fuse = h->tune_fuse[1];
     w.max_blocks = (int)std::min<size_t>(h->npartials / 3, (size_t)1 << 30);
     return w;
 }
@@ -1324,30 +1327,33 @@ std::string tune_cache_path() {
     return std::string(home ? home : ".") + "/.cache/dcm_b200_solver_tune.txt";
 }
 
-// cache lines: "<sms> <ip> <jp> <kp> <precision> <by> <tasks> <depth> <ms per iteration>"
-bool tune_lookup(int sms, const Dims& d, int prec, int* by, int* tasks, int* depth) {
+// cache lines: "<sms> <ip> <jp> <kp> <precision> <by> <tasks> <depth> <fuse> <ms per iteration>"
+bool tune_lookup(int sms, const Dims& d, int prec, int* by, int* tasks, int* depth, int* fuse) {
     std::ifstream f(tune_cache_path());
     std::string line;
     bool found = false;
     while (std::getline(f, line)) {
         std::istringstream is(line);
-        int a[8];
+        int a[9];
         double ms;
-        if (!(is >> a[0] >> a[1] >> a[2] >> a[3] >> a[4] >> a[5] >> a[6] >> a[7] >> ms)) continue;
+        if (!(is >> a[0] >> a[1] >> a[2] >> a[3] >> a[4] >> a[5] >> a[6] >> a[7] >> a[8] >> ms))
+            continue;
         if (a[0] == sms && a[1] == d.ip && a[2] == d.jp && a[3] == d.kp && a[4] == prec) {
             *by = a[5];
             *tasks = a[6];
             *depth = a[7];
+            *fuse = a[8];
             found = true;  // the last entry wins
         }
     }
     return found;
 }
 
-void tune_store(int sms, const Dims& d, int prec, int by, int tasks, int depth, double ms) {
+void tune_store(int sms, const Dims& d, int prec, int by, int tasks, int depth, int fuse,
+                double ms) {
     std::ofstream f(tune_cache_path(), std::ios::app);
     if (f) f << sms << ' ' << d.ip << ' ' << d.jp << ' ' << d.kp << ' ' << prec << ' ' << by << ' '
-             << tasks << ' ' << depth << ' ' << ms << '\n';
+             << tasks << ' ' << depth << ' ' << fuse << ' ' << ms << '\n';
 }
 
 template <typename T>
@@ -1370,7 +1376,7 @@ __global__ void k_tune_rhs(Dims d, T* b, T* x) {
 // device time of `iters` iterations of the solver in precision T with the
 // given launch shape (graph-driven, tolerance unreachable, itmax = iters)
 template <typename T>
-double tune_time(dcm_handle* h, int by, int tasks, int depth, int iters) {
+double tune_time(dcm_handle* h, int by, int tasks, int depth, int fuse, int iters) {
     SolverWork<T> w;
     T *x, *b;
     if constexpr (std::is_same<T, double>::value) {
@@ -1388,6 +1394,7 @@ double tune_time(dcm_handle* h, int by, int tasks, int depth, int iters) {
     w.by = by;
     w.tasks = tasks;
     w.ni = depth;
+    w.fuse = fuse;
     const Metrics<T>& mt = metrics_of<T>(h);
     double best = 1e30;
     for (int rep = 0; rep < 3; rep++) {
@@ -1409,39 +1416,63 @@ double tune_time(dcm_handle* h, int by, int tasks, int depth, int iters) {
 }  // namespace
 
 extern "C" int dcm_tune(dcm_handle* h, int precision, int use_cache, int* by, int* tasks,
-                        int* depth) {
+                        int* depth, int* fuse) {
     CHECK_H();
     if (precision != 0 && precision != 1) return fail(h, DCM_E_ARG, "tune: precision");
     int sms = 0;
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
-    int b0 = 8, t0 = 0, n0 = 4;
-    if (!(use_cache && tune_lookup(sms, h->d, precision, &b0, &t0, &n0))) {
+    int b0 = 8, t0 = 0, n0 = 4, f0 = 0;
+    if (!(use_cache && tune_lookup(sms, h->d, precision, &b0, &t0, &n0, &f0))) {
         static const int BYS[3] = {2, 4, 8}, TASKS[3] = {0, 1, 2}, DEPTHS[4] = {1, 2, 4, 8};
         double best = 1e30;
+        auto consider = [&](int bv, int tv, int nv, int fv) -> bool {
+            const double ms = precision == 0 ? tune_time<double>(h, bv, tv, nv, 0, 12)
+                                             : tune_time<float>(h, bv, tv, nv, fv, 12);
+            if (ms < 0) return false;
+            if (ms < best) {
+                best = ms;
+                b0 = bv;
+                t0 = tv;
+                n0 = nv;
+                f0 = fv;
+            }
+            return true;
+        };
         for (int bi = 0; bi < 3; bi++)
             for (int ti = 0; ti < 3; ti++)
-                for (int ni = 0; ni < 4; ni++) {
-                    const double ms =
-                        precision == 0 ? tune_time<double>(h, BYS[bi], TASKS[ti], DEPTHS[ni], 12)
-                                       : tune_time<float>(h, BYS[bi], TASKS[ti], DEPTHS[ni], 12);
-                    if (ms < 0)
+                for (int ni = 0; ni < 4; ni++)
+                    if (!consider(BYS[bi], TASKS[ti], DEPTHS[ni], 0))
                         return fail(h, DCM_E_CUDA, "tune: a candidate launch shape failed");
-                    if (ms < best) {
-                        best = ms;
-                        b0 = BYS[bi];
-                        t0 = TASKS[ti];
-                        n0 = DEPTHS[ni];
-                    }
-                }
-        tune_store(sms, h->d, precision, b0, t0, n0, best);
+        // the fused preconditioner (FP32): the sweep shape does not apply
+        if (precision == 1)
+            for (int ti = 0; ti < 3; ti++)
+                if (!consider(8, TASKS[ti], 4, 1))
+                    return fail(h, DCM_E_CUDA, "tune: a candidate launch shape failed");
+        tune_store(sms, h->d, precision, b0, t0, n0, f0, best);
     }
     h->tune_by[precision] = b0;
     h->tune_tasks[precision] = t0;
     h->tune_ni[precision] = n0;
+    h->tune_fuse[precision] = precision == 1 ? f0 : 0;
     h->generation += 1;
     if (by) *by = b0;
     if (tasks) *tasks = t0;
     if (depth) *depth = n0;
+    if (fuse) *fuse = h->tune_fuse[precision];
+    return DCM_OK;
+}
+
+extern "C" int dcm_set_launch_shape(dcm_handle* h, int precision, int by, int tasks, int depth,
+                                    int fuse) {
+    CHECK_H();
+    if ((precision != 0 && precision != 1) || by < 1 || by > 8 || tasks < 0 || tasks > 15 ||
+        depth < 1 || depth > 63 || (fuse != 0 && fuse != 1))
+        return fail(h, DCM_E_ARG, "set_launch_shape: bad argument");
+    h->tune_by[precision] = by;
+    h->tune_tasks[precision] = tasks;
+    h->tune_ni[precision] = depth;
+    h->tune_fuse[precision] = precision == 1 ? fuse : 0;
+    h->generation += 1;
     return DCM_OK;
 }
 

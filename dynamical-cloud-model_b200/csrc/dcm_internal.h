@@ -85,7 +85,13 @@ struct SolverWork {
     int max_blocks = 0;
     // i-planes each stencil warp task marches over (tuning)
     int ni = 4;
+    // FP32: fuse the three Jacobi sweeps of a phase (columns of <= 128 levels)
+    int fuse = 1;
 };
+
+// one-time setup of the solver kernels (shared-memory limits); called at
+// handle creation, outside any stream capture
+void solver_init();
 
 // per-field scalars of one MPDATA call
 struct MpScalars {

@@ -64,6 +64,7 @@ struct SolverArgs {
     int tasks;        // warp tasks per warp of the reducing kernels (0: fill the GPU)
     int max_blocks;   // blocks a reducing kernel may use (partials capacity)
     int ni;           // i-planes a stencil warp task marches over
+    int fuse;         // FP32: the three sweeps of a phase as one kernel (k_precond3)
 };
 
 // a_p exactly as set_mat_a forms it (dynamics.f90:93-95)
@@ -494,6 +495,196 @@ __global__ void __launch_bounds__(256) k_sten(SolverArgs a, Coef<T> c, SolverBuf
     }
 }
 
+// --- fused preconditioner: the three Jacobi sweeps of one phase in one kernel
+// (FP32, columns of at most 128 levels: one warp holds a whole column).
+//
+// precondition() (dynamics.f90:241-270) with s0 = q/a_p:
+//     s1 = s0 + s0 - (A s0)/a_p,  s2 = s1 + s0 - (A s1)/a_p,  s3 = s2 + s0 - (A s2)/a_p
+// A block owns PJ output rows j0 .. j0+PJ-1 of an i-chunk and keeps PJ + 6
+// warps, one per row j0-3 .. j0+PJ+2.  The warps march over the planes with
+// the stages skewed by one plane: at step b, stage 0 forms s0 at plane b+3
+// (from r/a_p and v1/a_p in HBM), stage 1 sweeps plane b+2, stage 2 plane b+1
+// and stage 3 plane b, which it writes out.  A warp's own i-1, i, i+1 values
+// of each stage stay in registers (rings shifted every step); its j-1, j+1
+// values come from the neighbouring warps' previous-step results in shared
+// memory (double-buffered, one barrier per step); k neighbours are vector
+// elements and shuffles.  Edge warps compute only the stages their neighbours
+// need (a shrinking halo of 3, 2, 1 rows).  Each output point sees exactly the
+// arithmetic of the three unfused sweeps.
+constexpr int PJ = 16;        // output rows per block
+constexpr int PW = PJ + 6;    // warps per block
+constexpr int PD = 3;         // planes of r/a_p, v1/a_p (and old p) copied ahead
+
+// 16-byte asynchronous global -> shared copy (cp.async, L2 only) and its
+// group bookkeeping: a lane reads back only the slots it filled itself, so
+// waiting on its own groups is enough (no barrier)
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N)); }
+
+__device__ __forceinline__ int wrapn(int q, int n) { return ((q - 1) % n + n) % n + 1; }
+
+template <int MODE>
+__global__ void __launch_bounds__(PW * 32, 1)
+    k_precond3(SolverArgs a, Coef<float> c, SolverBufs B, const SolverScalars* S, int ni) {
+    // [stage 0..2][buffer 0..1][warp][lane], then the copy-ahead ring
+    // [PD][rh, vh, p][warp][lane]
+    extern __shared__ float4 sbuf[];
+    float4* ring = sbuf + 3 * 2 * PW * 32;
+    if (S->done || S->pause) return;
+    const Dims& d = a.d;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int kp = d.kp, jp = d.jp, ip = d.ip;
+    const int k0 = 1 + 4 * lane;
+    const bool live = k0 <= kp;
+    const int nvalid = live ? min(4, kp - k0 + 1) : 0;
+    const int j0 = 1 + blockIdx.x * PJ;
+    const int jrow = j0 - 3 + w;
+    const int jw = wrapn(jrow, jp);
+    const bool outrow = w >= 3 && w < 3 + PJ && jrow <= jp;
+    const bool st1 = w >= 1 && w <= PW - 2, st2 = w >= 2 && w <= PW - 3;
+    const int i0 = 1 + blockIdx.y * ni, i1 = min(i0 + ni - 1, ip);
+    const int K = d.K, KJ = d.K * d.J;
+    const int col = (live ? k0 : 1) + K * jw;
+    float au[4], ad[4];
+    vld(c.au + (live ? k0 : 1), au);
+    vld(c.ad + (live ? k0 : 1), ad);
+    const float an = ld(c.an + jw), as = ld(c.as + jw);
+    const float bet = (float)S->bet, omg = (float)S->omg, alf = (float)S->alf;
+    const bool first = S->it == 0 || S->fresh;
+    const float* __restrict__ rh = (const float*)B.rh;
+    const float* __restrict__ vh = (const float*)B.vh;
+    float* __restrict__ out = (float*)B.out;
+    auto slot = [&](int stage, int buf, int warp) -> float4& {
+        return sbuf[((stage * 2 + buf) * PW + warp) * 32 + lane];
+    };
+    auto f4 = [](const float (&v)[4]) { return make_float4(v[0], v[1], v[2], v[3]); };
+    auto rslot = [&](int step, int arr) -> float4& {
+        return ring[(((step % PD) * 3 + arr) * PW + w) * 32 + lane];
+    };
+    // copy-ahead of step t: r/a_p and v1/a_p at plane b+3, old p at plane b
+    const int bstart = i0 - 6, nsteps = i1 - bstart + 1;
+    int qf = wrapn(bstart + 3, ip);  // plane of the next fetch, wrapped into 1..ip
+    auto fetch = [&](int t) {
+        if (t < nsteps) {
+            const int b = bstart + t;
+            const int o = col + KJ * qf;
+            qf = qf == ip ? 1 : qf + 1;
+            cp_async16(&rslot(t, 0), rh + o);
+            if (!(MODE == 0 && first)) cp_async16(&rslot(t, 1), vh + o);
+            if (MODE == 0 && !first && outrow && b >= i0) cp_async16(&rslot(t, 2), out + col + KJ * b);
+        }
+        cp_async_commit();  // an empty group keeps the group count per step
+    };
+    // s0 = q / a_p from r/a_p and v1/a_p (s0val, :393 / :404)
+    auto s0_at = [&](int t, float (&s)[4]) {
+        const float4 x4 = rslot(t, 0);
+        const float x[4] = {x4.x, x4.y, x4.z, x4.w};
+        if (MODE == 0 && first) {
+#pragma unroll
+            for (int e = 0; e < 4; e++) s[e] = x[e] - bet * (omg * 0.0f);
+            return;
+        }
+        const float4 y4 = rslot(t, 1);
+        const float y[4] = {y4.x, y4.y, y4.z, y4.w};
+#pragma unroll
+        for (int e = 0; e < 4; e++) s[e] = MODE == 0 ? x[e] - bet * (omg * y[e]) : x[e] - alf * y[e];
+    };
+    // one Jacobi sweep at plane q: res = xc + s0c - (A x)/a_p, A in the FP32
+    // difference form of sten_task
+    auto sweep = [&](int iq, const float (&xm)[4], const float (&xc)[4], const float (&xp)[4],
+                     const float4 xs4, const float4 xn4, const float (&s0c)[4], float (&res)[4]) {
+        const float ae = ld(c.ae + iq), aw = ld(c.aw + iq);
+        const float sij = -ae - aw - an - as;
+        const float xs[4] = {xs4.x, xs4.y, xs4.z, xs4.w}, xn[4] = {xn4.x, xn4.y, xn4.z, xn4.w};
+        float prev = __shfl_up_sync(0xffffffffu, xc[3], 1);
+        float next = __shfl_down_sync(0xffffffffu, xc[0], 1);
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            const int kk = k0 + e;
+            float xd = e == 0 ? prev : xc[e - 1];
+            float xu = e == 3 ? next : xc[e + 1];
+            xd = kk == 1 ? xc[e] : xd;
+            xu = kk == kp ? xc[e] : xu;
+            const float ap = sij - au[e] - ad[e];
+            const float c0 = xc[e];
+            const float Ax = aw * (xm[e] - c0) + ae * (xp[e] - c0) + as * (xs[e] - c0) +
+                             an * (xn[e] - c0) + ad[e] * (xd - c0) + au[e] * (xu - c0);
+            res[e] = xc[e] + s0c[e] - Ax / ap;
+        }
+    };
+    float R0[4][4], R1[3][4], R2[3][4];  // s0 at b..b+3, s1 at b..b+2, s2 at b-1..b+1
+#pragma unroll
+    for (int r = 0; r < 4; r++)
+#pragma unroll
+        for (int e = 0; e < 4; e++) R0[r][e] = 0.0f;
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+#pragma unroll
+        for (int e = 0; e < 4; e++) R1[r][e] = R2[r][e] = 0.0f;
+#pragma unroll
+    for (int t = 0; t < PD; t++) fetch(t);
+    int q1 = wrapn(bstart + 1, ip), q2 = wrapn(bstart + 2, ip);  // planes b+1, b+2 wrapped
+    for (int b = bstart; b <= i1; b++) {
+        const int t = b - bstart;
+        const int cur = t & 1, prv = cur ^ 1;
+        cp_async_wait<PD - 1>();  // this lane's copies of step t have landed
+        // stage 0: s0 at plane b+3
+        s0_at(t, R0[3]);
+        // stage 1: s1 at plane b+2 (j neighbours: s0 at b+2 from the last step)
+        if (st1 && b >= i0 - 4) {
+            sweep(q2, R0[1], R0[2], R0[3], slot(0, prv, w - 1), slot(0, prv, w + 1), R0[2],
+                  R1[2]);
+        }
+        // stage 2: s2 at plane b+1
+        if (st2 && b >= i0 - 2) {
+            sweep(q1, R1[0], R1[1], R1[2], slot(1, prv, w - 1), slot(1, prv, w + 1), R0[1],
+                  R2[2]);
+        }
+        // stage 3: s3 at plane b, the output
+        if (outrow && b >= i0) {
+            float s3[4];
+            sweep(b, R2[0], R2[1], R2[2], slot(2, prv, w - 1), slot(2, prv, w + 1), R0[0], s3);
+            const int o = col + KJ * b;
+            if (MODE == 0) {
+                if (first) {
+#pragma unroll
+                    for (int e = 0; e < 4; e++) s3[e] = s3[e] + bet * 0.0f;  // :397
+                } else {
+                    const float4 p4 = rslot(t, 2);  // old p, copied ahead
+                    const float po[4] = {p4.x, p4.y, p4.z, p4.w};
+#pragma unroll
+                    for (int e = 0; e < 4; e++) s3[e] = s3[e] + bet * po[e];
+                }
+            }
+            if (live) vst(out + o, s3, nvalid);
+        }
+        // this step's values for the neighbours' next step
+        slot(0, cur, w) = f4(R0[3]);
+        slot(1, cur, w) = f4(R1[2]);
+        slot(2, cur, w) = f4(R2[2]);
+        fetch(t + PD);  // into the ring slot step t has finished with
+        q1 = q2;
+        q2 = q2 == ip ? 1 : q2 + 1;
+        __syncthreads();
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            R0[0][e] = R0[1][e];
+            R0[1][e] = R0[2][e];
+            R0[2][e] = R0[3][e];
+            R1[0][e] = R1[1][e];
+            R1[1][e] = R1[2][e];
+            R2[0][e] = R2[1][e];
+            R2[1][e] = R2[2][e];
+        }
+    }
+    cp_async_wait<0>();
+}
+
 // --- D: x, r updates, (r,r), (r,cr) -> err, next rho and bet -----------------
 template <typename T>
 __global__ void __launch_bounds__(256) k_bicg_update(SolverArgs a, Coef<T> c,
@@ -698,6 +889,37 @@ static void sten(const SolverArgs& a, const Coef<T>& c, const SolverBufs& B, Sol
     }
 }
 
+constexpr size_t PRECOND3_SMEM = sizeof(float4) * (3 * 2 + PD * 3) * PW * 32;
+
+// the fused preconditioner applies (FP32, one k-chunk per column)
+template <typename T>
+static bool fused_ok(const SolverArgs& a) {
+    return std::is_same<T, float>::value && a.fuse && a.nkt == 1;
+}
+
+// one fused preconditioner launch: PJ-row strips x i-chunks, at most one
+// block per SM so that the chunks (and their 6-plane warm-up) are as long as
+// the SM count allows
+static void precond3(const SolverArgs& a, const Coef<float>& c, const SolverBufs& B,
+                     SolverScalars* S, int mode, cudaStream_t st) {
+    ProfScope ps(P_JACOBI, st);
+    const int nstrips = (a.d.jp + PJ - 1) / PJ;
+    const int nch = std::max(1, std::min(a.d.ip, sm_count() / nstrips));
+    const int ni = (a.d.ip + nch - 1) / nch;
+    const dim3 grid(nstrips, (a.d.ip + ni - 1) / ni);
+    if (mode == 0)
+        k_precond3<0><<<grid, PW * 32, PRECOND3_SMEM, st>>>(a, c, B, S, ni);
+    else
+        k_precond3<1><<<grid, PW * 32, PRECOND3_SMEM, st>>>(a, c, B, S, ni);
+}
+
+void solver_init() {
+    cudaFuncSetAttribute(k_precond3<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)PRECOND3_SMEM);
+    cudaFuncSetAttribute(k_precond3<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)PRECOND3_SMEM);
+}
+
 template <typename T>
 static void launch_iteration(const SolverArgs& a, const Coef<T>& c, SolverWork<T>& w, T* x,
                              cudaStream_t st) {
@@ -706,15 +928,23 @@ static void launch_iteration(const SolverArgs& a, const Coef<T>& c, SolverWork<T
     B.v1 = w.v1;
     B.rh = w.rh;
     B.vh = w.vh;
+    const bool fused = fused_ok<T>(a);
     // phase B: precondition(s <- t), p = s + bet p, v1 = A p
-    B.out = w.sA;
-    sten<T, OP_SW1, 0>(a, c, B, w, st, P_JACOBI);
-    B.sin = w.sA;
-    B.out = w.sB;
-    sten<T, OP_SW, 0>(a, c, B, w, st, P_JACOBI);
-    B.sin = w.sB;
-    B.out = w.p;
-    sten<T, OP_SW3P, 0>(a, c, B, w, st, P_JACOBI);
+    if (fused) {
+        if constexpr (std::is_same<T, float>::value) {
+            B.out = w.p;
+            precond3(a, c, B, w.S, 0, st);
+        }
+    } else {
+        B.out = w.sA;
+        sten<T, OP_SW1, 0>(a, c, B, w, st, P_JACOBI);
+        B.sin = w.sA;
+        B.out = w.sB;
+        sten<T, OP_SW, 0>(a, c, B, w, st, P_JACOBI);
+        B.sin = w.sB;
+        B.out = w.p;
+        sten<T, OP_SW3P, 0>(a, c, B, w, st, P_JACOBI);
+    }
     B.sin = w.p;
     B.cr = w.cr;
     B.out = w.v1;
@@ -722,14 +952,21 @@ static void launch_iteration(const SolverArgs& a, const Coef<T>& c, SolverWork<T
     sten<T, OP_MATP, 0>(a, c, B, w, st, P_MATVEC);
     // phase C: precondition(cs <- s), t = A cs
     B.sin = nullptr;
-    B.out = w.sA;
-    sten<T, OP_SW1, 1>(a, c, B, w, st, P_JACOBI);
-    B.sin = w.sA;
-    B.out = w.sB;
-    sten<T, OP_SW, 1>(a, c, B, w, st, P_JACOBI);
-    B.sin = w.sB;
-    B.out = w.sA;
-    sten<T, OP_SW, 1>(a, c, B, w, st, P_JACOBI);
+    if (fused) {
+        if constexpr (std::is_same<T, float>::value) {
+            B.out = w.sA;
+            precond3(a, c, B, w.S, 1, st);
+        }
+    } else {
+        B.out = w.sA;
+        sten<T, OP_SW1, 1>(a, c, B, w, st, P_JACOBI);
+        B.sin = w.sA;
+        B.out = w.sB;
+        sten<T, OP_SW, 1>(a, c, B, w, st, P_JACOBI);
+        B.sin = w.sB;
+        B.out = w.sA;
+        sten<T, OP_SW, 1>(a, c, B, w, st, P_JACOBI);
+    }
     B.sin = w.sA;
     B.out = w.t;
     sten<T, OP_MATC, 1>(a, c, B, w, st, P_MATVEC);
@@ -847,6 +1084,7 @@ int solver_run(SolverWork<T>& w, const Dims& d, T* x, const T* b, const T* sw, c
     a.tasks = w.tasks;
     a.max_blocks = w.max_blocks;
     a.ni = w.ni >= 1 ? w.ni : 1;
+    a.fuse = w.fuse;
     const Coef<T> c = coef_of(w);
     SolverBufs B{};
     B.x = x;
@@ -886,8 +1124,10 @@ int solver_run(SolverWork<T>& w, const Dims& d, T* x, const T* b, const T* sw, c
         SolveGraph& G = *w.graph;
         const void* kp[6] = {x, b, sw, dzn, w.r, w.S};
         const double kd[3] = {tol, sc_floor, 0.0};
-        const int ki[6] = {itmax, wo, post ? 1 : 0, (int)sizeof(T), d.ip * 4096 + d.jp,
-                           d.kp + 65536 * (a.by + 64 * a.tasks + 1024 * a.ni)};
+        // launch shape: by < 16, tasks < 16, ni < 64, fuse < 2
+        const int shape = a.by + 16 * a.tasks + 256 * a.ni + 16384 * a.fuse;
+        const int ki[6] = {itmax, wo, post ? 1 : 0, (int)sizeof(T) + 16 * shape,
+                           d.ip * 4096 + d.jp, d.kp};
         if (!G.matches(kp, kd, ki)) {
             G.release();
             bool good = ok(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
@@ -1113,9 +1353,11 @@ int refine_run(SolverWork<float>& wf, SolverWork<double>& wd, const Dims& d, dou
     a.tasks = wf.tasks;
     a.max_blocks = wf.max_blocks;
     a.ni = 1;                      // the FP64 residual does not march
+    a.fuse = 0;
     SolverArgs af = a;             // vector warp tasks of the FP32 iterations
     af.nkt = kchunks<float>(d);
     af.ni = wf.ni >= 1 ? wf.ni : 1;
+    af.fuse = wf.fuse;
     Coef<double> cd;
     cd.ae = wd.ae; cd.aw = wd.aw; cd.an = wd.an; cd.as = wd.as; cd.au = wd.au; cd.ad = wd.ad;
     const Coef<float> cf = coef_of(wf);
@@ -1181,8 +1423,8 @@ int refine_run(SolverWork<float>& wf, SolverWork<double>& wd, const Dims& d, dou
         SolveGraph& G = *wf.graph;
         const void* kp[6] = {x, b, sw, dzn, dx, wf.S};
         const double kd[3] = {tol, delta, 0.0};
-        const int ki[6] = {itmax, max_updates, 1, 0, d.ip * 4096 + d.jp,
-                           d.kp + 65536 * (af.by + 64 * af.tasks + 1024 * af.ni)};
+        const int shape = af.by + 16 * af.tasks + 256 * af.ni + 16384 * af.fuse;
+        const int ki[6] = {itmax, max_updates, 1, 16 * shape, d.ip * 4096 + d.jp, d.kp};
         if (!G.matches(kp, kd, ki)) {
             G.release();
             bool good = ok(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));

@@ -260,20 +260,27 @@ int dcm_solver_graphs(dcm_handle *h, int on);
 /* ---- solver launch-shape autotuner (no counterpart in the reference) ---- */
 /* Chooses, for this handle's grid shape and the given precision (0 FP64,
  * 1 the FP32 iterations of the mixed form), the launch shape of the solver
- * kernels: warps per block of the Jacobi sweeps (2, 4, 8), warp tasks per
- * warp of the reducing kernels (0 = as many blocks as are resident, each
- * warp striding over many tasks; 1, 2 = that many tasks per warp) and the
- * depth, the number of i-planes each stencil warp task marches over (1, 2,
- * 4, 8), by timing 12 BiCGSTAB iterations of each of the 36 shapes on a
- * synthetic right-hand side, then applies the fastest to the handle for
- * that precision (each precision keeps its own launch shape).  With
- * use_cache the result is looked up first in, and otherwise appended to, a
- * text file: $DCM_TUNE_CACHE, or $HOME/.cache/dcm_b200_solver_tune.txt (one
- * line per SM count, grid shape and precision).  Uses the handle's scratch
- * fields; call it before dcm_state_upload or between steps, not
- * concurrently with other calls on the handle. */
+ * kernels: warps per block of the Jacobi sweeps (by: 2, 4, 8), warp tasks per
+ * warp of the reducing kernels (tasks: 0 = as many blocks as are resident,
+ * each warp striding over many tasks; 1, 2 = that many tasks per warp), the
+ * depth, the number of i-planes the first Jacobi sweep marches over (1, 2,
+ * 4, 8), and in FP32 whether the three sweeps of each preconditioner
+ * application run fused in one kernel (fuse: columns of at most 128 levels).
+ * It times 12 BiCGSTAB iterations of each candidate on a synthetic
+ * right-hand side and applies the fastest to the handle for that precision
+ * (each precision keeps its own launch shape).  With use_cache the result is
+ * looked up first in, and otherwise appended to, a text file:
+ * $DCM_TUNE_CACHE, or $HOME/.cache/dcm_b200_solver_tune.txt (one line per SM
+ * count, grid shape and precision).  Uses the handle's scratch fields; call
+ * it before dcm_state_upload or between steps, not concurrently with other
+ * calls on the handle. */
 int dcm_tune(dcm_handle *h, int precision, int use_cache, int *by, int *tasks,
-             int *depth);
+             int *depth, int *fuse);
+/* Sets the launch shape of one precision explicitly (same meaning and ranges
+ * as dcm_tune's results; by <= 8, depth <= 63, fuse only for precision 1).
+ * Default: by 8, tasks 0, depth 4, fuse 1 (FP32) / 0 (FP64). */
+int dcm_set_launch_shape(dcm_handle *h, int precision, int by, int tasks,
+                         int depth, int fuse);
 
 /* ---- batched ensemble (no counterpart in the reference) ------------------ */
 /* Independent domains of possibly different sizes on one device.  Each

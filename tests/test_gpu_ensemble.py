@@ -70,11 +70,11 @@ def test_tune_and_cache(dcm, tmp_path, monkeypatch):
     monkeypatch.setenv("DCM_TUNE_CACHE", str(tmp_path / "tune.txt"))
     c = small_bubble()
     core = dcm.DynamicalCore(c.grid)
-    by, tasks, depth = core.tune(precision=1, use_cache=True)
-    assert by in (2, 4, 8) and tasks in (0, 1, 2) and depth in (1, 2, 4, 8)
+    by, tasks, depth, fuse = core.tune(precision=1, use_cache=True)
+    assert by in (2, 4, 8) and tasks in (0, 1, 2) and depth in (1, 2, 4, 8) and fuse in (0, 1)
     lines = (tmp_path / "tune.txt").read_text().splitlines()
     assert len(lines) == 1
-    assert core.tune(precision=1, use_cache=True) == (by, tasks, depth)  # from the cache
+    assert core.tune(precision=1, use_cache=True) == (by, tasks, depth, fuse)  # from the cache
     assert len((tmp_path / "tune.txt").read_text().splitlines()) == 1
     # the tuned shape changes only the order of the dot-product sums
     _upload(core, c, 0)

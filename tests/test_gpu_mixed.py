@@ -85,3 +85,26 @@ def test_graph_and_host_loops_agree(dcm, precision):
     assert ia == ib
     for n in ("u", "v", "w", "th", "p", "psrc"):
         assert np.array_equal(fa[n], fb[n]), n
+
+
+@pytest.mark.parametrize("shape", [(24, 20, 16), (9, 30, 37), (1, 16, 14), (40, 1, 12)])
+def test_fused_preconditioner_matches_unfused(dcm, shape):
+    """The fused three-sweep preconditioner (FP32) performs each point's
+    arithmetic of the three separate sweeps: the two launch shapes give the
+    same iterations and fields to FP32 round-off, on strips and chunks that
+    wrap (jp < 20, ip = 1) and on ragged columns."""
+    ip, jp, kp = shape
+    c = cases.warm_bubble(ip=ip, jp=jp, kp=kp, dxyz=50.0, radius=200.0, zc=200.0, seed=41)
+    out = []
+    for fuse in (1, 0):
+        core = dcm.DynamicalCore(c.grid)
+        core.set_launch_shape(1, fuse=fuse)
+        core.upload_state(c.state, c.dt, ptol=c.ptol, kord=c.kord, precision=1)
+        core.driver_start()
+        its = [core.step(1).iters_last for _ in range(3)]
+        out.append((its, core.download_state()))
+        core.close()
+    (ia, fa), (ib, fb) = out
+    assert max(abs(a - b) for a, b in zip(ia, ib)) <= 2
+    for n in ("u", "v", "w", "th"):
+        assert relerr(fa[n], fb[n]) <= 1e-6, n
