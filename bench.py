@@ -128,6 +128,13 @@ PASSES = {"jacobi": 23.0 / 6.0, "matvec": 4.0, "update": 10.0, "setup": 4.0,
 # field passes of one BiCGSTAB iteration and of the rest of a step
 ITER_PASSES = 41.0
 STEP_PASSES = 60.0
+# With the fused preconditioner (FP32) one "jacobi" launch applies all three
+# sweeps of a phase: it reads r/a_p, v1/a_p (and old p) and writes p or cs,
+# 4 passes in phase B and 3 in phase C; the iteration then moves 7 + 8 + 10 =
+# 25 passes.  The three separate sweeps it replaces move 12 and 11.
+FUSED_JACOBI_PASSES = 3.5
+FUSED_REPLACED_PASSES = 11.5
+FUSED_ITER_PASSES = 25.0
 
 
 def make_case(pkg, name):
@@ -289,20 +296,26 @@ def run_b200(args, rank, world, local_rank, dist):
     classes = m32["classes"]
     dom = max(classes, key=lambda k: classes[k][0])
     dom_ms, dom_n = classes[dom]
-    dom_bytes = PASSES.get(dom, 0.0) * N * w32
-    achieved = dom_bytes / (dom_ms / dom_n / 1e3) / 1e9 if dom_n else None
+    fused = bool(m32["shape"]["fused_preconditioner"])
+    dom_passes = FUSED_JACOBI_PASSES if (fused and dom == "jacobi") else PASSES.get(dom, 0.0)
+    dom_bytes = dom_passes * N * w32
+    dom_s = dom_ms / dom_n / 1e3 if dom_n else None
+    achieved = dom_bytes / dom_s / 1e9 if dom_n else None
+    effective = (FUSED_REPLACED_PASSES * N * w32 / dom_s / 1e9
+                 if (fused and dom == "jacobi" and dom_n) else None)
     traffic = None
     tp = os.path.join(ROOT, "profiles", "dram_traffic.json")
     if os.path.exists(tp):
         with open(tp) as f:
             tr = json.load(f).get(case.name, {}).get("fp32", {})
-        traffic = tr.get(dom)
+        traffic = tr.get("jacobi_fused" if (fused and dom == "jacobi") else dom)
 
-    def step_model(m, w):
+    def step_model(m, w, iter_passes):
         it = m["iters"] / args.steps
-        b = (STEP_PASSES + ITER_PASSES * it) * N * w
+        b = (STEP_PASSES + iter_passes * it) * N * w
         gbs = b / (m["ms"] / args.steps / 1e3) / 1e9
-        return {"bytes_per_step": b, "GBs": gbs, "frac": gbs / peak, "iters_per_step": it}
+        return {"bytes_per_step": b, "GBs": gbs, "frac": gbs / peak, "iters_per_step": it,
+                "passes_per_iteration": iter_passes}
 
     # ---- accuracy: mixed against the FP64 path after the timed steps and
     #      after args.accuracy_steps
@@ -372,16 +385,24 @@ def run_b200(args, rank, world, local_rank, dist):
                  "tuned_launch_shape": m64["shape"],
                  "bicgstab_iters_per_step": m64["iters"] / args.steps,
                  "gpu_launches": m64["launches"], "clocks": m64["clocks"],
-                 "step_model": step_model(m64, 8.0),
+                 "step_model": step_model(m64, 8.0, ITER_PASSES),
                  "kernel_ms": {k: round(v[0], 3) for k, v in m64["classes"].items()}},
         "speedup_vs_fp64": m32["value"] / m64["value"],
         "accuracy_vs_fp64": acc,
-        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+        "roofline": {"bound": "hbm", "kernel": dom + (" (fused preconditioner)" if fused else ""),
+                     "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
                      "traffic": traffic, "peak_kind": peak_kind,
                      "bytes_per_launch": dom_bytes, "launches": dom_n,
                      "avg_launch_us": dom_ms / dom_n * 1e3 if dom_n else None,
-                     "step_model": step_model(m32, w32)},
+                     "effective_GBs": effective,
+                     "effective_frac": (effective / peak) if effective else None,
+                     "effective_note": ("bytes of the three separate sweeps one fused launch "
+                                        "replaces (11.5 passes) per launch time; the fused "
+                                        "kernel itself is issue-bound") if fused else None,
+                     "step_model": step_model(m32, w32,
+                                              FUSED_ITER_PASSES if fused else ITER_PASSES),
+                     "step_model_unfused_algorithm": step_model(m32, w32, ITER_PASSES)},
         "kernel_ms": {k: round(v[0], 3) for k, v in classes.items()},
         "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": m32["launches"],
         "clocks": m32["clocks"],
