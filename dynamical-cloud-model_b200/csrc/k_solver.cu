@@ -899,12 +899,13 @@ static bool fused_ok(const SolverArgs& a) {
 
 // one fused preconditioner launch: PJ-row strips x i-chunks, at most one
 // block per SM so that the chunks (and their 6-plane warm-up) are as long as
-// the SM count allows
+// the SM count allows, and no chunk shorter than 8 planes
 static void precond3(const SolverArgs& a, const Coef<float>& c, const SolverBufs& B,
                      SolverScalars* S, int mode, cudaStream_t st) {
     ProfScope ps(P_JACOBI, st);
     const int nstrips = (a.d.jp + PJ - 1) / PJ;
-    const int nch = std::max(1, std::min(a.d.ip, sm_count() / nstrips));
+    // chunks of at least 8 planes (each carries a 6-plane warm-up)
+    const int nch = std::max(1, std::min((a.d.ip + 7) / 8, sm_count() / nstrips));
     const int ni = (a.d.ip + nch - 1) / nch;
     const dim3 grid(nstrips, (a.d.ip + ni - 1) / ni);
     if (mode == 0)
