@@ -78,6 +78,16 @@ def exchange_full(a, lbc=0.0, ubc=0.0):
     return a
 
 
+def mixing_length_sq(grid, cvis=0.23, z0=1.0e-4):
+    """Smagorinsky mixing length squared on the w-levels, lamsq
+    (initialisation.f90:449-450), with the nominal horizontal spacings taken
+    from the grid's first interior cells.  cvis = 0.23 and z0 = 1e-4 m are
+    the reference's namelist.in values."""
+    dx_nm, dy_nm = float(grid.dx[1]), float(grid.dy[1])
+    return 1.0 / (1.0 / (cvis * (dx_nm + dy_nm + grid.dz) / 3.0) ** 2.0 +
+                  1.0 / (0.4 * (grid.z + z0)) ** 2.0)
+
+
 def _interp(zs, ths, z):
     """Linear interpolation of the sounding with the reference's clamps:
     find_pos / poly_int over the bracketing pair, min(z, z_top)."""

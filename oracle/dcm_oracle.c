@@ -84,17 +84,16 @@ void orc_exchange_along_dim(const orc_grid *g, double *a, double lbc,
         for (int j = 0; j <= jp + 1; j++) A3(a, 0, j, i) = lbc;
 }
 
-/* exchange_full, mpi_module.f90:926-1271.  After exchange_along_dim, the 12
- * edges and 8 corners are written from send buffers that were pre-filled
- * with this rank's own data (:1180, :1244-1246); with dims(3) = 1 every
- * up/down neighbour is MPI_PROC_NULL, the receive is a no-op, and the
- * buffers are written unconditionally (edges :1113-1126) or because
- * recv /= id (corners :1129-1136).  Net effect: every halo cell holds the
- * fully periodic image of an interior cell, except the interior of the top
- * and bottom planes, which hold ubc / lbc.                                 */
-void orc_exchange_full(const orc_grid *g, double *a, double lbc, double ubc) {
+/* The 12 edges and 8 corners written after the face exchange by both
+ * exchange_full (mpi_module.f90:965-1136) and exchange_full_wo (:1549-1720).
+ * Their send buffers are pre-filled with this rank's own data (:1180,
+ * :1244-1246, :1764, :1828-1830); with dims(3) = 1 every up/down neighbour is
+ * MPI_PROC_NULL, the receive is a no-op, and the buffers are written
+ * unconditionally (edges :1113-1126, :1697-1710) or because recv /= id
+ * (corners :1129-1136, :1713-1720).  Net effect: each edge and corner holds
+ * the fully periodic image of an interior cell.                             */
+static void edges_and_corners(const orc_grid *g, double *a) {
     const int ip = g->ip, jp = g->jp, kp = g->kp;
-    orc_exchange_along_dim(g, a, lbc, ubc);
     /* edges along k (ws_bt, wn_bt, es_bt, en_bt) */
     for (int k = 1; k <= kp; k++) {
         A3(a, k, jp + 1, ip + 1) = A3(a, k, 1, 1);
@@ -125,6 +124,25 @@ void orc_exchange_full(const orc_grid *g, double *a, double lbc, double ubc) {
     A3(a, kp + 1, 0, 0) = A3(a, 1, jp, ip);
     A3(a, 0, jp + 1, 0) = A3(a, kp, 1, ip);
     A3(a, 0, 0, 0) = A3(a, kp, jp, ip);
+}
+
+/* exchange_full, mpi_module.f90:926-1271: exchange_along_dim (faces, then
+ * the top / bottom planes set to ubc / lbc), then the edges and corners.
+ * Net effect: every halo cell holds the fully periodic image of an interior
+ * cell, except the interior of the top and bottom planes (ubc / lbc).      */
+void orc_exchange_full(const orc_grid *g, double *a, double lbc, double ubc) {
+    orc_exchange_along_dim(g, a, lbc, ubc);
+    edges_and_corners(g, a);
+}
+
+/* exchange_full_wo, mpi_module.f90:1511-1855: exchange_along_dim_wo (faces
+ * for k = 1..kp only), then the same edges and corners.  The interior of the
+ * top and bottom planes (k = 0 and kp+1, j = 1..jp, i = 1..ip) is left as it
+ * was; every other halo cell holds the periodic image of an interior cell
+ * (so k = 0 halo columns take level kp's values and k = kp+1 level 1's).   */
+void orc_exchange_full_wo(const orc_grid *g, double *a) {
+    orc_exchange_along_dim_wo(g, a);
+    edges_and_corners(g, a);
 }
 
 /* ------------------------------------------------------------------------ */
@@ -335,13 +353,15 @@ done:
 /* sources and momentum                                                     */
 /* ------------------------------------------------------------------------ */
 
-/* sources, dynamics.f90:639-1000, viscous = .false. branch */
-int orc_sources(const orc_grid *g, const orc_forcing *f, const double *ubar,
-                const double *vbar, const double *wbar, const double *thbar,
-                const double *zu, const double *zv, const double *zw,
-                const double *u, const double *v, const double *w,
-                const double *th, double *su, double *sv, double *sw,
-                double *sth, double *rhs) {
+/* sources, dynamics.f90:639-1000; vis == NULL or vis->viscous == 0 is the
+ * viscous = .false. branch */
+static int sources_impl(const orc_grid *g, const orc_forcing *f, const orc_viscous *vis,
+                        const double *ubar, const double *vbar, const double *wbar,
+                        const double *thbar, const double *zu, const double *zv,
+                        const double *zw, const double *u, const double *v, const double *w,
+                        const double *th, int nq, const double *q, int moisture,
+                        double *vism, double *vist, double *strain, double *su, double *sv,
+                        double *sw, double *sth, double *sq, double *rhs) {
     const int ip = g->ip, jp = g->jp, kp = g->kp;
     const double *dx = g->dx, *dy = g->dy, *dz = g->dz, *dxn = g->dxn,
                  *dyn = g->dyn, *dzn = g->dzn, *rhoa = g->rhoa,
@@ -435,11 +455,25 @@ int orc_sources(const orc_grid *g, const orc_forcing *f, const double *ubar,
                 for (int k = 1; k <= kp; k++)
                     A3(sw, k, j, i) = A3(sw, k, j, i) - rhoan[k] * (wbar[k] - f->w_subs[k]);
     }
-    /* non-viscous branch: full exchange, :909-916 */
-    orc_exchange_full(g, su, 0.0, 0.0);
-    orc_exchange_full(g, sv, 0.0, 0.0);
-    orc_exchange_full(g, sw, 0.0, 0.0);
-    orc_exchange_full(g, sth, 0.0, 0.0);
+    if (vis && vis->viscous) {
+        /* subgrid model, :878-893; its stresses are locals of sources (:736-737) */
+        const size_t n = NTOT;
+        double *tau = (double *)calloc(6 * n, sizeof(double));
+        double *viss = (moisture && nq > 0) ? (double *)calloc((size_t)nq * n, sizeof(double))
+                                            : NULL;
+        orc_calculate_subgrid_3d(g, vis->lamsq, vis->z0, vis->z0th, u, v, w, zu, zv, zw, th, nq,
+                                 q, vism, vist, viss, strain, tau, tau + n, tau + 2 * n,
+                                 tau + 3 * n, tau + 4 * n, tau + 5 * n, su, sv, sw, sth, sq,
+                                 moisture);
+        free(tau);
+        free(viss);
+    } else {
+        /* non-viscous branch: full exchange, :909-916 */
+        orc_exchange_full(g, su, 0.0, 0.0);
+        orc_exchange_full(g, sv, 0.0, 0.0);
+        orc_exchange_full(g, sw, 0.0, 0.0);
+        orc_exchange_full(g, sth, 0.0, 0.0);
+    }
     /* surface / lid conditions, :922-973 */
     for (int i = 0; i <= ip + 1; i++)
         for (int j = 0; j <= jp + 1; j++) {
@@ -469,6 +503,27 @@ int orc_sources(const orc_grid *g, const orc_forcing *f, const double *ubar,
                                 (A3(sv, 0, j, i) - A3(sv, 0, j - 1, i)) / dy[j - 1] +
                                 (A3(sw, 0, j, i) + A3(sw, 1, j, i)) / dz[1]);
     return ORC_OK;
+}
+
+int orc_sources(const orc_grid *g, const orc_forcing *f, const double *ubar,
+                const double *vbar, const double *wbar, const double *thbar,
+                const double *zu, const double *zv, const double *zw,
+                const double *u, const double *v, const double *w,
+                const double *th, double *su, double *sv, double *sw,
+                double *sth, double *rhs) {
+    return sources_impl(g, f, NULL, ubar, vbar, wbar, thbar, zu, zv, zw, u, v, w, th, 0, NULL,
+                        0, NULL, NULL, NULL, su, sv, sw, sth, NULL, rhs);
+}
+
+int orc_sources_viscous(const orc_grid *g, const orc_forcing *f, const orc_viscous *vis,
+                        const double *ubar, const double *vbar, const double *wbar,
+                        const double *thbar, const double *zu, const double *zv,
+                        const double *zw, const double *u, const double *v, const double *w,
+                        const double *th, int nq, const double *q, int moisture,
+                        double *vism, double *vist, double *strain, double *su, double *sv,
+                        double *sw, double *sth, double *sq, double *rhs) {
+    return sources_impl(g, f, vis, ubar, vbar, wbar, thbar, zu, zv, zw, u, v, w, th, nq, q,
+                        moisture, vism, vist, strain, su, sv, sw, sth, sq, rhs);
 }
 
 /* advance_momentum, dynamics.f90:1019-1099 */
@@ -1164,7 +1219,7 @@ void orc_driver_start(const orc_grid *g, orc_state *s) {
 }
 
 /* one pass of the time loop, driver_code.f90:304-676 (output, microphysics,
- * radiation and land surface off; subgrid off) */
+ * radiation and land surface off; the subgrid model when c->viscous is set) */
 int orc_model_step(const orc_grid *g, const orc_config *c, orc_state *s) {
     const int ip = g->ip, jp = g->jp, kp = g->kp;
     const size_t n = NTOT;
@@ -1178,8 +1233,24 @@ int orc_model_step(const orc_grid *g, const orc_config *c, orc_state *s) {
     orc_horizontal_means(g, c->moisture, c->nq, u, v, w, s->th, s->q, s->ubar,
                          s->vbar, s->wbar, s->thbar, s->qbar); /* :433 */
     orc_divergence_calc(g, u, v, w, s->div);                      /* :443 */
-    orc_sources(g, &c->forcing, s->ubar, s->vbar, s->wbar, s->thbar, zu, zv,
-                zw, u, v, w, s->th, s->su, s->sv, s->sw, s->sth, s->psrc);
+    if (c->viscous.viscous) { /* :455-479 with viscous = .true. */
+        const size_t nn = NTOT;
+        double *tmp[3] = {NULL, NULL, NULL};
+        double **own[3] = {&s->vism, &s->vist, &s->strain};
+        double *fld[3];
+        for (int a = 0; a < 3; a++) {
+            fld[a] = *own[a];
+            if (!fld[a]) fld[a] = tmp[a] = (double *)calloc(nn, sizeof(double));
+        }
+        orc_sources_viscous(g, &c->forcing, &c->viscous, s->ubar, s->vbar, s->wbar, s->thbar,
+                            zu, zv, zw, u, v, w, s->th, c->nq, s->q, c->moisture && s->q,
+                            fld[0], fld[1], fld[2], s->su, s->sv, s->sw, s->sth, s->sq,
+                            s->psrc);
+        for (int a = 0; a < 3; a++) free(tmp[a]);
+    } else {
+        orc_sources(g, &c->forcing, s->ubar, s->vbar, s->wbar, s->thbar, zu, zv,
+                    zw, u, v, w, s->th, s->su, s->sv, s->sw, s->sth, s->psrc);
+    }
     orc_exchange_along_dim_wo(g, s->psrc); /* :485 */
     int it = 0;
     double err = 0.0;

@@ -56,6 +56,7 @@ void orc_set_threads(int nthreads, int parallel_reductions);
 void orc_exchange_full(const orc_grid *g, double *a, double lbc, double ubc);
 void orc_exchange_along_dim(const orc_grid *g, double *a, double lbc, double ubc);
 void orc_exchange_along_dim_wo(const orc_grid *g, double *a);
+void orc_exchange_full_wo(const orc_grid *g, double *a);
 
 /* ---- pressure solver (dynamics.f90:34-482) ---- */
 double orc_inn_prod(const orc_grid *g, const double *x, const double *y);
@@ -76,6 +77,23 @@ int orc_sources(const orc_grid *g, const orc_forcing *f,
                 const double *u, const double *v, const double *w,
                 const double *th,
                 double *su, double *sv, double *sw, double *sth, double *rhs);
+/* sources with viscous = .true. (dynamics.f90:878-893): the subgrid model
+ * replaces the full exchange of su, sv, sw, sth.  lamsq: kp+2; vism, vist,
+ * strain: inout 3-D; q / sq (nq fields) used when moisture is set.          */
+typedef struct {
+    int viscous;
+    const double *lamsq;
+    double z0, z0th;
+} orc_viscous;
+int orc_sources_viscous(const orc_grid *g, const orc_forcing *f, const orc_viscous *vis,
+                        const double *ubar, const double *vbar, const double *wbar,
+                        const double *thbar,
+                        const double *zu, const double *zv, const double *zw,
+                        const double *u, const double *v, const double *w,
+                        const double *th, int nq, const double *q, int moisture,
+                        double *vism, double *vist, double *strain,
+                        double *su, double *sv, double *sw, double *sth, double *sq,
+                        double *rhs);
 void orc_advance_momentum(const orc_grid *g, double dt,
                           double *u, double *v, double *w,
                           const double *zu, const double *zv, const double *zw,
@@ -103,6 +121,18 @@ void orc_mpdata_3d_add(const orc_grid *g, double dt, const double *u,
                        int kord, int monotone, int neumann,
                        int limiter_variant);
 
+/* ---- Smagorinsky subgrid model (sgm/subgrid_3d.f90:38-493) ----
+ * z = g->zg (z(1) only).  viss / q / sq (nq fields each) are used only when
+ * moisture is set.                                                          */
+void orc_calculate_subgrid_3d(const orc_grid *g, const double *lamsq, double z0,
+                              double z0th, const double *u, const double *v,
+                              const double *w, const double *zu, const double *zv,
+                              const double *zw, const double *th, int nq, const double *q,
+                              double *vism, double *vist, double *viss, double *strain,
+                              double *tau11, double *tau22, double *tau33, double *tau12,
+                              double *tau13, double *tau23, double *su, double *sv,
+                              double *sw, double *sth, double *sq, int moisture);
+
 /* ---- diagnostics (diagnostics.f90) and scalar update (sgm/subgrid_3d.f90) */
 void orc_horizontal_means(const orc_grid *g, int moisture, int nq,
                           const double *u, const double *v, const double *w,
@@ -126,6 +156,7 @@ typedef struct {
     const int *c_s, *c_e;   /* 1-based category bounds, length ncat */
     double thbase, thtop;   /* lbc/ubc for scheme 2 */
     orc_forcing forcing;
+    orc_viscous viscous;    /* subgrid model in sources (viscous = 0: off) */
 } orc_config;
 
 typedef struct {
@@ -140,6 +171,7 @@ typedef struct {
     int bicgstab_first;
     int last_iters;
     double last_err;
+    double *vism, *vist, *strain;         /* subgrid fields (viscous only) */
 } orc_state;
 
 /* pre-loop velocity boundary fix-up (driver_code.f90:287-295) */

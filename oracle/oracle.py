@@ -19,7 +19,8 @@ _dp = C.POINTER(C.c_double)
 
 
 def build(force=False):
-    src = [os.path.join(HERE, f) for f in ("dcm_oracle.c", "dcm_oracle.h", "Makefile")]
+    src = [os.path.join(HERE, f)
+           for f in ("dcm_oracle.c", "dcm_oracle_sgm.c", "dcm_oracle.h", "Makefile")]
     if force or not os.path.exists(LIBPATH) or \
             any(os.path.getmtime(s) > os.path.getmtime(LIBPATH) for s in src):
         subprocess.run(["make", "-s", "-C", HERE], check=True)
@@ -38,12 +39,17 @@ class _OForcing(C.Structure):
                 ("w_subs", _dp), ("forcing_tau", C.c_double)]
 
 
+class _OViscous(C.Structure):
+    _fields_ = [("viscous", C.c_int), ("lamsq", _dp), ("z0", C.c_double), ("z0th", C.c_double)]
+
+
 class _OConfig(C.Structure):
     _fields_ = [("dt", C.c_double), ("ptol", C.c_double), ("advection_scheme", C.c_int),
                 ("kord", C.c_int), ("monotone", C.c_int), ("limiter_variant", C.c_int),
                 ("moisture", C.c_int), ("nq", C.c_int), ("ncat", C.c_int),
                 ("c_s", C.POINTER(C.c_int)), ("c_e", C.POINTER(C.c_int)),
-                ("thbase", C.c_double), ("thtop", C.c_double), ("forcing", _OForcing)]
+                ("thbase", C.c_double), ("thtop", C.c_double), ("forcing", _OForcing),
+                ("viscous", _OViscous)]
 
 
 class _OState(C.Structure):
@@ -51,7 +57,8 @@ class _OState(C.Structure):
                                    "th", "p", "su", "sv", "sw", "psrc", "div", "sth", "q", "sq",
                                    "ubar", "vbar", "wbar", "thbar", "qbar")] + [
         ("t1", C.c_double), ("t2", C.c_double), ("q1", _dp), ("q2", _dp), ("n", C.c_int),
-        ("bicgstab_first", C.c_int), ("last_iters", C.c_int), ("last_err", C.c_double)]
+        ("bicgstab_first", C.c_int), ("last_iters", C.c_int), ("last_err", C.c_double),
+        ("vism", _dp), ("vist", _dp), ("strain", _dp)]
 
 
 _lib = None
@@ -133,6 +140,42 @@ class OracleCore:
                              _F(u), _F(v), _F(w), _F(th), _F(su), _F(sv), _F(sw), _F(sth),
                              _F(rhs))
 
+    def sources_viscous(self, ubar, vbar, wbar, thbar, zu, zv, zw, u, v, w, th, su, sv, sw,
+                        sth, rhs, lamsq, z0, z0th, vism, vist, strain, q=None, sq=None,
+                        forcing=None):
+        """sources with viscous = .true.: the subgrid model in place of the
+        full exchange of su, sv, sw, sth (dynamics.f90:878-893)."""
+        fs, keep = self._forcing(forcing)
+        vis = _OViscous(1, None, float(z0), float(z0th))
+        lam = np.ascontiguousarray(lamsq, dtype=np.float64)
+        vis.lamsq = lam.ctypes.data_as(_dp)
+        nq = 0 if q is None else q.shape[0]
+        self.lib.orc_sources_viscous(
+            C.byref(self.g), C.byref(fs) if fs is not None else None, C.byref(vis),
+            _p(ubar), _p(vbar), _p(wbar), _p(thbar), _F(zu), _F(zv), _F(zw), _F(u), _F(v),
+            _F(w), _F(th), nq, None if q is None else q.ctypes.data_as(_dp), int(nq > 0),
+            _F(vism), _F(vist), _F(strain), _F(su), _F(sv), _F(sw), _F(sth),
+            None if sq is None else sq.ctypes.data_as(_dp), _F(rhs))
+
+    # sgm/subgrid_3d.f90
+    def calculate_subgrid_3d(self, lamsq, z0, z0th, u, v, w, zu, zv, zw, th, vism, vist,
+                             strain, tau11, tau22, tau33, tau12, tau13, tau23, su, sv, sw, sth,
+                             q=None, viss=None, sq=None):
+        """calculate_subgrid_3d (sgm/subgrid_3d.f90:38-357); z is the grid's z.
+        q, viss, sq: stacks of nq Fortran fields (moisture on when q is given)."""
+        lam = np.ascontiguousarray(lamsq, dtype=np.float64)
+        nq = 0 if q is None else q.shape[0]
+        self.lib.orc_calculate_subgrid_3d(
+            C.byref(self.g), _p(lam), C.c_double(z0), C.c_double(z0th),
+            *[_F(a) for a in (u, v, w, zu, zv, zw, th)], nq,
+            None if q is None else q.ctypes.data_as(_dp), _F(vism), _F(vist),
+            None if viss is None else viss.ctypes.data_as(_dp), _F(strain),
+            *[_F(a) for a in (tau11, tau22, tau33, tau12, tau13, tau23, su, sv, sw, sth)],
+            None if sq is None else sq.ctypes.data_as(_dp), int(nq > 0))
+
+    def exchange_full_wo(self, a):
+        self.lib.orc_exchange_full_wo(C.byref(self.g), _F(a))
+
     def advance_momentum(self, dt, u, v, w, zu, zv, zw, su, sv, sw, p):
         self.lib.orc_advance_momentum(C.byref(self.g), C.c_double(dt),
                                       *[_F(a) for a in (u, v, w, zu, zv, zw, su, sv, sw, p)])
@@ -202,7 +245,8 @@ class OracleModel:
     """model_driver's time loop on the CPU restatement."""
 
     def __init__(self, grid, state, dt, ptol=1e-10, kord=3, monotone=True, advection_scheme=1,
-                 limiter=0, nq=0, c_s=(), c_e=(), thbase=0.0, thtop=0.0, forcing=None):
+                 limiter=0, nq=0, c_s=(), c_e=(), thbase=0.0, thtop=0.0, forcing=None,
+                 viscous=None):
         self.lib = library()
         self.core = OracleCore(grid)
         sh = self.core.shape
@@ -248,6 +292,14 @@ class OracleModel:
         fs, self._fkeep = self.core._forcing(forcing)
         if fs is not None:
             cfg.forcing = fs
+        if viscous:
+            # viscous = dict(lamsq=(kp+2,), z0=..., z0th=...): the subgrid model
+            self._lamsq = np.ascontiguousarray(viscous["lamsq"], dtype=np.float64)
+            cfg.viscous = _OViscous(1, self._lamsq.ctypes.data_as(_dp),
+                                    float(viscous["z0"]), float(viscous["z0th"]))
+            for n in ("vism", "vist", "strain"):
+                self.f[n] = np.zeros(sh, order="F")
+                setattr(s, n, _F(self.f[n]))
         self.cfg = cfg
 
     def driver_start(self):

@@ -63,3 +63,18 @@ def live_mask_p(g):
 def small_bubble(ip=24, jp=20, kp=16, seed=7, dxyz=100.0):
     return cases.warm_bubble(ip=ip, jp=jp, kp=kp, dxyz=dxyz, radius=500.0, zc=800.0,
                              seed=seed)
+
+
+def subgrid_inputs(g, seed):
+    """Seeded inputs of the subgrid model: winds of a few m/s and potential
+    temperature perturbations of a few kelvin (so that both Richardson
+    branches and both surface-layer branches occur), every halo cell set;
+    the inout fields random too (the routine must keep what it does not
+    write)."""
+    rng = np.random.default_rng(seed)
+    f = {n: rand_field(g, rng, -4.0, 4.0) for n in ("u", "v", "w", "zu", "zv", "zw")}
+    f["th"] = rand_field(g, rng, -3.0, 3.0)
+    for n in ("vism", "vist", "strain", "tau11", "tau22", "tau33", "tau12", "tau13", "tau23",
+              "su", "sv", "sw", "sth"):
+        f[n] = rand_field(g, rng, -1.0, 1.0)
+    return f

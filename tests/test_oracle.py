@@ -7,7 +7,7 @@ restatements and to analytic invariants instead.
 import numpy as np
 import pytest
 
-from helpers import cases, fz, rand_field, relerr, small_bubble, velocities
+from helpers import cases, fz, rand_field, relerr, small_bubble, subgrid_inputs, velocities
 
 
 @pytest.fixture(scope="module")
@@ -150,3 +150,47 @@ def test_step_kh_2d_runs(orc):
     assert it > 0 and err < 1e-10
     f = m.fields()
     assert np.all(np.isfinite(f["u"])) and np.all(np.isfinite(f["th"]))
+
+
+def test_exchange_full_wo_matches_independent_restatement(orc, g):
+    import subgrid_np
+    rng = np.random.default_rng(5)
+    a = rand_field(g, rng)
+    b = a.copy(order="F")
+    orc.OracleCore(g).exchange_full_wo(a)
+    subgrid_np.exchange_full_wo(b)
+    assert np.array_equal(a, b)
+
+
+def test_subgrid_matches_independent_restatement(orc, g):
+    """calculate_subgrid_3d: the C restatement against the array-at-a-time
+    numpy one, every output field, moisture on (two q fields)."""
+    import subgrid_np
+    lamsq = cases.mixing_length_sq(g, 0.23, 0.1)
+    a = subgrid_inputs(g, 21)
+    rng = np.random.default_rng(22)
+    qs = [rand_field(g, rng, 0.0, 1e-2) for _ in range(2)]
+    sqs = [rand_field(g, rng, -1e-5, 1e-5) for _ in range(2)]
+    b = {n: x.copy(order="F") for n, x in a.items()}
+    _fortran_stack = orc._fortran_stack
+    q = _fortran_stack(qs)
+    sq = _fortran_stack(sqs)
+    viss = _fortran_stack([fz(g), fz(g)])
+    orc.OracleCore(g).calculate_subgrid_3d(
+        lamsq, 0.1, 0.1, a["u"], a["v"], a["w"], a["zu"], a["zv"], a["zw"], a["th"], a["vism"],
+        a["vist"], a["strain"], a["tau11"], a["tau22"], a["tau33"], a["tau12"], a["tau13"],
+        a["tau23"], a["su"], a["sv"], a["sw"], a["sth"], q=q, viss=viss, sq=sq)
+    sq_np = [x.copy(order="F") for x in sqs]
+    subgrid_np.subgrid(g, lamsq, 0.1, 0.1, b["u"], b["v"], b["w"], b["zu"], b["zv"], b["zw"],
+                       b["th"], b["vism"], b["vist"], b["strain"],
+                       [b[n] for n in ("tau11", "tau22", "tau33", "tau12", "tau13", "tau23")],
+                       b["su"], b["sv"], b["sw"], b["sth"], q=qs, sq=sq_np)
+    for n in a:
+        assert relerr(a[n], b[n]) <= 1e-14, n
+    for m in range(2):
+        assert relerr(sq[m], sq_np[m]) <= 1e-14, m
+        assert np.array_equal(viss[m], a["vist"]), m
+    # both branches of the Richardson functions and a live surface layer
+    kp = g.kp
+    assert np.any(a["vism"][1:kp - 1] == 0.0) and np.any(a["vism"][1:kp - 1] > 0.0)
+    assert np.all(np.isfinite(a["vism"][0, 1:-1, 1:-1]))
