@@ -52,7 +52,8 @@ class _Config(C.Structure):
                 ("itmax", C.c_int), ("moisture", C.c_int), ("nq", C.c_int), ("ncat", C.c_int),
                 ("c_s", C.POINTER(C.c_int)), ("c_e", C.POINTER(C.c_int)),
                 ("thbase", C.c_double), ("thtop", C.c_double), ("precision", C.c_int),
-                ("inner_tol", C.c_double), ("forcing", _Forcing)]
+                ("inner_tol", C.c_double), ("forcing", _Forcing), ("viscous", C.c_int),
+                ("lamsq", _dp), ("z0", C.c_double), ("z0th", C.c_double)]
 
 
 class _Fields(C.Structure):
@@ -108,6 +109,9 @@ def library():
             "dcm_exchange_full": [P, _dp, C.c_double, C.c_double],
             "dcm_exchange_along_dim": [P, _dp, C.c_double, C.c_double],
             "dcm_exchange_along_dim_wo": [P, _dp],
+            "dcm_exchange_full_wo": [P, _dp],
+            "dcm_calculate_subgrid_3d": [P, _dp, C.c_double, C.c_double] + [_dp] * 7 +
+                                        [C.c_int] + [_dp] * 16 + [C.c_int],
             "dcm_state_upload": [P, C.POINTER(_Config), C.POINTER(_Fields)],
             "dcm_driver_start": [P],
             "dcm_step": [P, C.c_int, C.POINTER(StepStats)],
@@ -143,7 +147,8 @@ EXPORTS = ("dcm_create", "dcm_destroy", "dcm_status_string", "dcm_last_error",
            "dcm_driver_start", "dcm_step", "dcm_state_download", "dcm_profile_enable",
            "dcm_profile_read", "dcm_horizontal_means_noalloc", "dcm_solver_graphs", "dcm_tune",
            "dcm_set_launch_shape", "dcm_ensemble_create", "dcm_ensemble_destroy", "dcm_ensemble_member",
-           "dcm_ensemble_step", "dcm_ensemble_last_error")
+           "dcm_ensemble_step", "dcm_ensemble_last_error", "dcm_exchange_full_wo",
+           "dcm_calculate_subgrid_3d")
 
 PROF_CLASSES = ("setup", "jacobi", "matvec", "update", "post", "means", "sources", "rhs",
                 "adv_ref", "mp_shift", "upwind", "antidiff", "beta", "limit", "restore",
@@ -365,10 +370,33 @@ class DynamicalCore:
     def exchange_along_dim_wo(self, a):
         self._check(self.lib.dcm_exchange_along_dim_wo(self.h, self.F(a)))
 
+    def exchange_full_wo(self, a):
+        self._check(self.lib.dcm_exchange_full_wo(self.h, self.F(a)))
+
+    # ---- sgm/subgrid_3d.f90 -------------------------------------------------------
+    def calculate_subgrid_3d(self, lamsq, z0, z0th, u, v, w, zu, zv, zw, th, vism, vist,
+                             strain, tau11, tau22, tau33, tau12, tau13, tau23, su, sv, sw, sth,
+                             q=None, viss=None, sq=None):
+        """calculate_subgrid_3d (sgm/subgrid_3d.f90:38-357): the inout arrays
+        are updated in place as the reference does.  q, viss, sq are stacks
+        of nq Fortran fields (q[n] is field n); moisture is on when q is
+        given.  z(1) is the grid's z[1]."""
+        lam = np.ascontiguousarray(lamsq, dtype=np.float64)
+        nq = 0 if q is None else q.shape[0]
+        self._check(self.lib.dcm_calculate_subgrid_3d(
+            self.h, _ptr(lam), float(z0), float(z0th),
+            *[self.F(a) for a in (u, v, w, zu, zv, zw, th)], nq,
+            None if q is None else q.ctypes.data_as(_dp), self.F(vism), self.F(vist),
+            None if viss is None else viss.ctypes.data_as(_dp), self.F(strain),
+            *[self.F(a) for a in (tau11, tau22, tau33, tau12, tau13, tau23, su, sv, sw, sth)],
+            None if sq is None else sq.ctypes.data_as(_dp), int(nq > 0)))
+
     # ---- the device-resident time loop (model_driver) ---------------------------
     def upload_state(self, state, dt, ptol=1e-10, kord=3, monotone=True, advection_scheme=1,
                      limiter=0, itmax=9999, nq=0, c_s=(), c_e=(), thbase=0.0, thtop=0.0,
-                     forcing=None, precision=0, inner_tol=0.1):
+                     forcing=None, precision=0, inner_tol=0.1, viscous=None):
+        """viscous = dict(lamsq=(kp+2,), z0=..., z0th=...) switches the
+        subgrid model on in sources (dynamics.f90:878-893)."""
         K2 = self.grid.kp + 2
         cfg = _Config()
         cfg.dt, cfg.ptol = float(dt), float(ptol)
@@ -384,6 +412,11 @@ class DynamicalCore:
         fs, fkeep = self._forcing(forcing)
         if fs is not None:
             cfg.forcing = fs
+        if viscous:
+            lam = np.ascontiguousarray(viscous["lamsq"], dtype=np.float64)
+            cfg.viscous, cfg.lamsq = 1, _ptr(lam)
+            cfg.z0, cfg.z0th = float(viscous["z0"]), float(viscous["z0th"])
+            fkeep = dict(fkeep or {}, lamsq=lam)
         self._fkeep = fkeep
         sh = self.shape
         f = _Fields()

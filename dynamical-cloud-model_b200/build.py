@@ -22,7 +22,7 @@ FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
 # instead of the IEEE sequence.  The flag does not touch FP64 division, so
 # the FP64 parity path keeps the reference's correctly rounded divides.
 FILE_FLAGS = {"k_mpdata.cu": ["-prec-div=false"], "k_solver.cu": ["-prec-div=false"],
-              "k_dynamics.cu": ["-prec-div=false"]}
+              "k_dynamics.cu": ["-prec-div=false"], "k_subgrid.cu": ["-prec-div=false"]}
 
 
 def sources():

@@ -37,6 +37,8 @@ struct State {
     T *th = nullptr, *th2 = nullptr, *su = nullptr, *sv = nullptr, *sw = nullptr,
       *sth = nullptr, *means = nullptr;
     std::vector<T*> q, sq, qtmp;
+    // subgrid model (viscous): viscosities, strain rate, lamsq (kp+2)
+    T *vism = nullptr, *vist = nullptr, *strain = nullptr, *lamsq = nullptr;
 };
 
 }  // namespace
@@ -72,6 +74,7 @@ struct dcm_handle {
 
     // named full-size scratch buffers
     std::vector<double*> slots;
+    double* sg_lamsq = nullptr;  // lamsq of dcm_calculate_subgrid_3d (kp+2)
     int first_call = 1;  // bicgstab_first, dynamics.f90:17
 
     // FP32 copies for the mixed-precision form
@@ -171,6 +174,8 @@ enum {
     // mpdata work
     S_VA0, S_VA1, S_VA2, S_VL0, S_VL1, S_VL2, S_B0, S_B1, S_B2, S_B3, S_B4, S_B5,
     S_PSI_OUT, S_STAGE,
+    // subgrid drop-in: vism, vist, strain, tau11, tau22, tau33, tau12, tau13, tau23, q, sq
+    S_SG = 40,
     S_DYN = 64  // psi fields / scratch for vec: S_DYN + 4*q + {in, out, pa, pb}
 };
 
@@ -457,6 +462,7 @@ extern "C" int dcm_destroy(dcm_handle* h) {
     for (double* p : h->slots) free_field(p);
     for (float* p : h->fslots) free_field(p);
     cudaFree(h->metric_block_f);
+    cudaFree(h->sg_lamsq);
     cudaFree(h->S2);
     cudaFreeHost(h->hS2);
     cudaFree(h->forcing_f);
@@ -786,6 +792,74 @@ extern "C" int dcm_exchange_along_dim(dcm_handle* h, double* a, double lbc, doub
 extern "C" int dcm_exchange_along_dim_wo(dcm_handle* h, double* a) {
     return exchange_dropin(h, a, HALO_WO, 0.0, 0.0);
 }
+extern "C" int dcm_exchange_full_wo(dcm_handle* h, double* a) {
+    return exchange_dropin(h, a, HALO_FULL_WO, 0.0, 0.0);
+}
+
+// calculate_subgrid_3d (sgm/subgrid_3d.f90:38-357) on the caller's host arrays
+extern "C" int dcm_calculate_subgrid_3d(dcm_handle* h, const double* lamsq, double z0,
+                                        double z0th, const double* u, const double* v,
+                                        const double* w, const double* zu, const double* zv,
+                                        const double* zw, const double* th, int nq,
+                                        const double* q, double* vism, double* vist,
+                                        double* viss, double* strain, double* tau11,
+                                        double* tau22, double* tau33, double* tau12,
+                                        double* tau13, double* tau23, double* su, double* sv,
+                                        double* sw, double* sth, double* sq, int moisture) {
+    CHECK_H();
+    double* out[13] = {vism, vist, strain, tau11, tau22, tau33, tau12, tau13, tau23,
+                       su, sv, sw, sth};
+    const double* in[7] = {u, v, w, zu, zv, zw, th};
+    for (const double* a : in)
+        if (!a) return fail(h, DCM_E_ARG, "calculate_subgrid_3d: missing input field");
+    for (double* a : out)
+        if (!a) return fail(h, DCM_E_ARG, "calculate_subgrid_3d: missing inout field");
+    if (!lamsq || !(z0 > 0.0) || !(z0th > 0.0))
+        return fail(h, DCM_E_ARG, "calculate_subgrid_3d: lamsq, z0 > 0 and z0th > 0 needed");
+    if (moisture && (nq < 1 || !q || !viss || !sq))
+        return fail(h, DCM_E_ARG, "calculate_subgrid_3d: moisture needs nq, q, viss, sq");
+    if (h->h_zg.size() < 2)
+        return fail(h, DCM_E_ARG, "calculate_subgrid_3d: the grid's zg is needed (z(1))");
+    const size_t K2 = h->d.kp + 2;
+    if (!h->sg_lamsq) CK(cudaMalloc(&h->sg_lamsq, K2 * sizeof(double)));
+    CK(cudaMemcpyAsync(h->sg_lamsq, lamsq, K2 * sizeof(double), cudaMemcpyHostToDevice, h->st));
+    const int in_slot[7] = {S_U, S_V, S_W, S_ZU, S_ZV, S_ZW, S_TH};
+    double* I[7];
+    for (int c = 0; c < 7; c++) {
+        I[c] = slot(h, in_slot[c]);
+        NEED(I[c]);
+        RC(upload(h, I[c], in[c]));
+    }
+    double* O[13];
+    for (int c = 0; c < 13; c++) {
+        O[c] = c < 9 ? slot(h, S_SG + c) : slot(h, c == 9 ? S_SU : c == 10 ? S_SV
+                                                      : c == 11 ? S_SW : S_STH);
+        NEED(O[c]);
+        RC(upload(h, O[c], out[c]));
+    }
+    const SgsParams<double> P{h->sg_lamsq, h->h_zg[1], z0, z0th};
+    ScalarSet<double> set;
+    make_scalar_sets<double>(I[6], O[12], 0, nullptr, nullptr, 0, 0, &set, 1);
+    launch_subgrid<double>(h->d, h->mt, P, I[0], I[1], I[2], I[3], I[4], I[5], I[6], O[0], O[1],
+                           O[2], O + 3, O[9], O[10], O[11], &set, 1, false, h->st);
+    CK(cudaGetLastError());
+    for (int c = 0; c < 13; c++) RC(download(h, out[c], O[c]));
+    if (moisture) {
+        // viss(:,:,:,n) = vist (:182-187); then each q's diffusion (:319-346)
+        double *Q = slot(h, S_SG + 9), *SQ = slot(h, S_SG + 10);
+        NEED(Q); NEED(SQ);
+        for (int c = 0; c < nq; c++) {
+            RC(download(h, viss + (size_t)c * h->nh, O[1]));
+            RC(upload(h, Q, q + (size_t)c * h->nh));
+            RC(upload(h, SQ, sq + (size_t)c * h->nh));
+            make_scalar_sets<double>(Q, SQ, 0, nullptr, nullptr, 0, 0, &set, 1);
+            launch_subgrid_scalars<double>(h->d, h->mt, O[1], &set, 1, h->st);
+            CK(cudaGetLastError());
+            RC(download(h, sq + (size_t)c * h->nh, SQ));
+        }
+    }
+    return sync(h);
+}
 
 // =============================================================================
 // device-resident time loop
@@ -961,9 +1035,20 @@ int step_body(dcm_handle* h, cudaStream_t st, int phase, bool emit) {
     // sources (sth = 0 first, :340) + exchange_along_dim_wo(psrc), :455-487
     const Forcing<T> F = forcing_t<T>(h);
     const T* ubar = S.means;
+    // viscous: the subgrid model inside sources (dynamics.f90:878-893)
+    SgsStep<T> sg{};
+    if (c.viscous) {
+        sg.P = SgsParams<T>{S.lamsq, h->h_zg[1], c.z0, c.z0th};
+        sg.vism = S.vism;
+        sg.vist = S.vist;
+        sg.strain = S.strain;
+        sg.q = S.q.data();
+        sg.sq = S.sq.data();
+        sg.nq = nqq;
+    }
     launch_sources<T, double>(d, mt, h->mt, F, ubar, ubar + K2, ubar + 2 * K2, ubar + 3 * K2, zu,
                               zv, zw, u, v, w, S.th, S.su, S.sv, S.sw, S.sth, h->psrc, 1, 1,
-                              st);
+                              st, c.viscous ? &sg : nullptr);
     CK(cudaGetLastError());
     // pressure: bicgstab + exchange_along_dim_wo(p), :496-507
     if (!emit) h->first_call = 0;
@@ -1108,7 +1193,7 @@ int get_field(dcm_handle* h, double* dst, const T* src, size_t n = 0) {
 }
 
 template <typename T>
-int upload_state_t(dcm_handle* h, const dcm_fields* f) {
+int upload_state_t(dcm_handle* h, const dcm_fields* f, const double* lamsq_host) {
     State<T>& S = state_of<T>(h);
     const dcm_config& cfg = h->cfg;
     const int nqq = cfg.moisture ? cfg.nq : 0;
@@ -1149,6 +1234,24 @@ int upload_state_t(dcm_handle* h, const dcm_fields* f) {
     }
     if constexpr (std::is_same<T, float>::value) {
         launch_convert<float, double>(5 * K2, h->forcing_f, h->forcing_dev, h->st);
+    }
+    if (cfg.viscous) {
+        // vism, vist and strain are recomputed every step (their previous
+        // values are never read); lamsq in the field precision
+        T** sg[3] = {&S.vism, &S.vist, &S.strain};
+        for (auto pp : sg) {
+            *pp = alloc_owned<T>(h);
+            NEED(*pp);
+        }
+        S.lamsq = alloc_owned<T>(h, K2);
+        double* l64 = alloc_owned<double>(h, K2);
+        NEED(S.lamsq); NEED(l64);
+        RC(upload(h, l64, lamsq_host, K2));
+        if constexpr (std::is_same<T, float>::value)
+            launch_convert<float, double>(K2, S.lamsq, l64, h->st);
+        else
+            CK(cudaMemcpyAsync(S.lamsq, l64, K2 * sizeof(double), cudaMemcpyDeviceToDevice,
+                               h->st));
     }
     return DCM_OK;
 }
@@ -1203,8 +1306,13 @@ extern "C" int dcm_state_upload(dcm_handle* h, const dcm_config* cfg, const dcm_
     if (cfg->moisture && (cfg->nq < 1 || cfg->nq > NQMAX || cfg->ncat < 1 || !cfg->c_s ||
                           !cfg->c_e || !f->q))
         return fail(h, DCM_E_ARG, "state_upload: bad moisture config");
+    if (cfg->viscous && (!cfg->lamsq || !(cfg->z0 > 0.0) || !(cfg->z0th > 0.0)))
+        return fail(h, DCM_E_ARG, "state_upload: viscous needs lamsq, z0 > 0 and z0th > 0");
+    if (cfg->viscous && h->h_zg.size() < 2)
+        return fail(h, DCM_E_ARG, "state_upload: viscous needs the grid's zg (z(1))");
     free_state(h);
     h->cfg = *cfg;
+    h->cfg.lamsq = nullptr;  // copied to the device below; no host pointer is kept
     h->prec = cfg->precision;
     const int nqq = cfg->moisture ? cfg->nq : 0;
     if (nqq) {
@@ -1227,7 +1335,8 @@ extern "C" int dcm_state_upload(dcm_handle* h, const dcm_config* cfg, const dcm_
     RC(upload(h, h->p, f->p));
     RC(upload(h, h->div, f->div));
     RC(upload(h, h->psrc, f->psrc));
-    RC(h->prec == 0 ? upload_state_t<double>(h, f) : upload_state_t<float>(h, f));
+    RC(h->prec == 0 ? upload_state_t<double>(h, f, cfg->lamsq)
+                    : upload_state_t<float>(h, f, cfg->lamsq));
     h->q1.assign(nqq, 0.0);  // driver_code.f90:275-276
     h->q2.assign(nqq, 0.0);
     h->t1 = h->t2 = 0.0;  // saved locals, :260

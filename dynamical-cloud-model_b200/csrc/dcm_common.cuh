@@ -18,6 +18,8 @@
 //       periodic images; the whole top / bottom planes are ubc / lbc;
 //       vertical edges are left alone.
 //   exchange_along_dim_wo     (:1285-1494): x and y faces for k = 1..kp.
+//   exchange_full_wo          (:1511-1855): as exchange_full, but the
+//       interior of the top / bottom planes is left as it was.
 #pragma once
 #include <cstddef>
 #include <cstdint>
@@ -86,7 +88,10 @@ __device__ __forceinline__ int images(int c, int n, int* out) {
 }
 
 // ---- exchange_full images of v (interior cell k,j,i) -------------------
-template <typename T>
+// WO = true gives exchange_full_wo (mpi_module.f90:1511-1855): the same
+// images, except that the interior of the top / bottom planes is left as it
+// was (lbc / ubc unused).
+template <typename T, bool WO = false>
 __device__ __forceinline__ void put_full(T* __restrict__ a, const Dims& d,
                                          int k, int j, int i, T v, T lbc,
                                          T ubc) {
@@ -103,8 +108,10 @@ __device__ __forceinline__ void put_full(T* __restrict__ a, const Dims& d,
                 if ((a3 | b3 | c3) == 0) continue;
                 const int kk = ks[a3], jj = js[b3], ii = is[c3];
                 T val = v;
-                if ((kk == 0 || kk == d.kp + 1) && b3 == 0 && c3 == 0)
+                if ((kk == 0 || kk == d.kp + 1) && b3 == 0 && c3 == 0) {
+                    if (WO) continue;
                     val = (kk == 0) ? lbc : ubc;
+                }
                 a[d.at(kk, jj, ii)] = val;
             }
 }

@@ -150,7 +150,7 @@ int upwind_run(MpdataWork<T>& w, const Dims& d, const Metrics<T>& mt, T dt,
                T* psi_out, int neumann, cudaStream_t st);
 
 // --- k_dynamics.cu ---------------------------------------------------------
-enum HaloMode { HALO_FULL = 0, HALO_DIM = 1, HALO_WO = 2 };
+enum HaloMode { HALO_FULL = 0, HALO_DIM = 1, HALO_WO = 2, HALO_FULL_WO = 3 };
 
 template <typename T>
 void launch_exchange(const Dims& d, T* a, int mode, T lbc, T ubc,
@@ -174,15 +174,63 @@ void launch_means_div(const Dims& d, const Metrics<D>& mt, const T* u,
                       T* means /* (4+nq)*(kp+2) */, D* div, double* partials,
                       unsigned int* ticket, cudaStream_t st);
 
+// --- k_subgrid.cu ----------------------------------------------------------
+// Smagorinsky subgrid model, sgm/subgrid_3d.f90:38-493.
+template <typename T>
+struct SgsParams {
+    const T* lamsq;             // mixing length squared on the w-levels, kp+2
+    double z1, z0, z0th;        // z(1) and the roughness lengths of monin_obukhov
+};
+// scalars diffused in one pass: ds[m] += div(vist grad s[m]) / rhoan, or
+// ds[m] = that term alone where bit m of reset is set
+constexpr int SGS_MAXS = 9;
+constexpr int SGS_MAX_SETS = 8;  // th and up to 71 q fields in one step
+template <typename T>
+struct ScalarSet {
+    const T* s[SGS_MAXS];
+    T* ds[SGS_MAXS];
+    int n;
+    unsigned reset;
+};
+// tau (six fields: tau11, tau22, tau33, tau12, tau13, tau23) may be null;
+// rows = true applies the surface / lid rows of sources to su, sv, sw
+// instead of their exchange_full images alone
+template <typename T>
+void launch_subgrid(const Dims& d, const Metrics<T>& mt, const SgsParams<T>& P, const T* u,
+                    const T* v, const T* w, const T* zu, const T* zv, const T* zw, const T* th,
+                    T* vism, T* vist, T* strain, T* const* tau, T* su, T* sv, T* sw,
+                    const ScalarSet<T>* sets, int nsets, bool rows, cudaStream_t st);
+// the scalar diffusion pass alone (vist already computed)
+template <typename T>
+void launch_subgrid_scalars(const Dims& d, const Metrics<T>& mt, const T* vist,
+                            const ScalarSet<T>* sets, int nsets, cudaStream_t st);
+// groups th (if non-null) and the nq q fields into sets; returns the number
+// of sets, or -1 when more than max_sets are needed
+template <typename T>
+int make_scalar_sets(const T* th, T* sth, int sth_reset, T* const* q, T* const* sq, int nq,
+                     int sq_reset, ScalarSet<T>* sets, int max_sets);
+// the subgrid model inside the resident time step (sources with
+// viscous = .true.)
+template <typename T>
+struct SgsStep {
+    SgsParams<T> P;
+    T *vism, *vist, *strain;
+    T* const* q;   // nq current q fields
+    T* const* sq;  // their sources
+    int nq;
+};
+
 // sources (dynamics.f90:639-998); sth_reset applies the driver's sth = 0
-// first; rhs_wo applies the driver's exchange_along_dim_wo(psrc)
+// first; rhs_wo applies the driver's exchange_along_dim_wo(psrc); sg
+// non-null is the viscous = .true. branch (the subgrid model)
 template <typename T, typename R>
 void launch_sources(const Dims& d, const Metrics<T>& mt, const Metrics<R>& mtr,
                     const Forcing<T>& f, const T* ubar, const T* vbar,
                     const T* wbar, const T* thbar, const T* zu, const T* zv,
                     const T* zw, const T* u, const T* v, const T* w,
                     const T* th, T* su, T* sv, T* sw, T* sth, R* rhs,
-                    int sth_reset, int rhs_wo, cudaStream_t st);
+                    int sth_reset, int rhs_wo, cudaStream_t st,
+                    const SgsStep<T>* sg = nullptr);
 
 template <typename T>
 void launch_advance_momentum(const Dims& d, const Metrics<T>& mt, T dt, T* u,

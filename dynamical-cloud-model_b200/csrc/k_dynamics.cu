@@ -21,6 +21,8 @@ __global__ void __launch_bounds__(256) k_exchange(Dims d, T* __restrict__ a, int
     const T v = a[d.at(k, j, i)];
     if (mode == HALO_FULL)
         put_full(a, d, k, j, i, v, lbc, ubc);
+    else if (mode == HALO_FULL_WO)
+        put_full<T, true>(a, d, k, j, i, v, lbc, ubc);
     else if (mode == HALO_DIM)
         put_dim(a, d, k, j, i, v, lbc, ubc);
     else
@@ -162,7 +164,8 @@ __global__ void __launch_bounds__(256) k_sources(Dims d, Metrics<T> mt, Forcing<
                                                  const T* __restrict__ w,
                                                  const T* __restrict__ th, T* __restrict__ su,
                                                  T* __restrict__ sv, T* __restrict__ sw,
-                                                 T* __restrict__ sth, int sth_reset) {
+                                                 T* __restrict__ sth, int sth_reset,
+                                                 int interior_only) {
     const int k = 1 + blockIdx.x * BX + threadIdx.x;
     const int j = 1 + blockIdx.y * BY + threadIdx.y;
     const int i = 1 + blockIdx.z;
@@ -223,6 +226,15 @@ __global__ void __launch_bounds__(256) k_sources(Dims d, Metrics<T> mt, Forcing<
         vsv = vsv - rn * (zv[o] - ld(F.v_force + k)) / F.forcing_tau;
     }
     if (F.divergence) vsw = vsw - rn * (ld(wbar + k) - ld(F.w_subs + k));
+    if (interior_only) {
+        // viscous = .true.: the subgrid model adds to these values and writes
+        // the images and rows (dynamics.f90:878-893)
+        su[o] = vsu;
+        sv[o] = vsv;
+        sw[o] = vsw;
+        sth[o] = vsth;
+        return;
+    }
     const T z = T(0);
     put_full(sth, d, k, j, i, vsth, z, z);
     if (k == d.kp) {
@@ -280,12 +292,22 @@ void launch_sources(const Dims& d, const Metrics<T>& mt, const Metrics<R>& mtr,
                     const Forcing<T>& f, const T* ubar, const T* vbar, const T* wbar,
                     const T* thbar, const T* zu, const T* zv, const T* zw, const T* u, const T* v,
                     const T* w, const T* th, T* su, T* sv, T* sw, T* sth, R* rhs, int sth_reset,
-                    int rhs_wo, cudaStream_t st) {
+                    int rhs_wo, cudaStream_t st, const SgsStep<T>* sg) {
     const dim3 b(BX, BY);
     { ProfScope ps_(P_SOURCES, st);
     k_sources<T><<<interior_grid(d, d.kp), b, 0, st>>>(d, mt, f, ubar, vbar, wbar, thbar, zu, zv,
                                                        zw, u, v, w, th, su, sv, sw, sth,
-                                                       sth_reset);
+                                                       sth_reset, sg ? 1 : 0);
+    }
+    if (sg) {
+        // the subgrid model, then the rows of sources on su, sv, sw; sq is
+        // zeroed each step by the driver (driver_code.f90:342), so each q's
+        // diffusion term replaces it
+        ScalarSet<T> sets[SGS_MAX_SETS];
+        const int ns = make_scalar_sets<T>(th, sth, 0, sg->q, sg->sq, sg->nq, 1, sets,
+                                           SGS_MAX_SETS);
+        launch_subgrid<T>(d, mt, sg->P, u, v, w, zu, zv, zw, th, sg->vism, sg->vist, sg->strain,
+                          nullptr, su, sv, sw, sets, ns < 0 ? 0 : ns, true, st);
     }
     { ProfScope ps_(P_RHS, st);
     k_rhs<T, R><<<interior_grid(d, d.kp + 2), b, 0, st>>>(d, mtr, su, sv, sw, rhs, rhs_wo);
@@ -475,7 +497,7 @@ void launch_add_profile(const Dims& d, T* a, const T* prof, T sign, cudaStream_t
                                        const Forcing<T>&, const T*, const T*, const T*,         \
                                        const T*, const T*, const T*, const T*, const T*,        \
                                        const T*, const T*, const T*, T*, T*, T*, T*, D*, int,   \
-                                       int, cudaStream_t);                                      \
+                                       int, cudaStream_t, const SgsStep<T>*);                   \
     template void launch_advance_momentum<T>(const Dims&, const Metrics<T>&, T, T*, T*, T*,     \
                                              const T*, const T*, const T*, const T*,            \
                                              const T*, const T*, const T*, cudaStream_t);       \

@@ -3,13 +3,16 @@ solver iterations and device time of each step.  A small driver for
 profiling single kernels (ncu -k ... on a few steps) and for quick checks.
 
     python dynamical-cloud-model_b200/run_case.py --case warm_bubble \
-        --precision 1 --steps 1 [--host-loop]
+        --precision 1 --steps 1 [--host-loop] [--viscous] [--profile]
 
 Cases: warm_bubble (256x256x128), sheared_convection (512x512x256, 8 tracers),
 kelvin_helmholtz (128x1x64), or warm_bubble_IPxJPxKP /
 sheared_convection_IPxJPxKP for other sizes.  --host-loop drives the
 pressure solve from the host (the same kernels; a profiler sees every
 launch, which it cannot inside the graph-driven solve's conditional loop).
+--viscous switches the Smagorinsky subgrid model on in sources (cvis 0.23,
+z0 = z0th = 0.1 m); --profile prints the device time per kernel class over
+the steps after the first.
 """
 import argparse
 import importlib.util
@@ -52,6 +55,8 @@ def main():
     ap.add_argument("--steps", type=int, default=1)
     ap.add_argument("--host-loop", action="store_true")
     ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--viscous", action="store_true")
+    ap.add_argument("--profile", action="store_true")
     args = ap.parse_args()
     dcm = load()
     from dcm_b200 import cases
@@ -60,15 +65,23 @@ def main():
     if args.host_loop:
         core.solver_graphs(False)
     kw = dict(nq=c.nq, c_s=c.c_s, c_e=c.c_e) if c.nq else {}
+    if args.viscous:
+        kw["viscous"] = dict(lamsq=cases.mixing_length_sq(c.grid, 0.23, 0.1), z0=0.1, z0th=0.1)
     core.upload_state(c.state, c.dt, ptol=c.ptol, kord=c.kord, monotone=c.monotone,
                       precision=args.precision, **kw)
     core.driver_start()
     for s in range(args.steps):
+        if args.profile and s == min(1, args.steps - 1):
+            core.profile(True)  # after the first step (module loading, first-call set-up)
         st = core.step(1)
         print("%s precision %d step %d: %d iterations (%d updates, %d restarts), "
               "err %.3e, %.2f ms" % (c.name, args.precision, s + 1, st.iters_last,
                                      st.updates_last, st.restarts_last, st.err_last,
                                      st.ms_total), flush=True)
+    if args.profile:
+        for name, (ms, n) in core.profile_read().items():
+            if n:
+                print("  %-9s %9.3f ms  %6d launches" % (name, ms, n))
     core.close()
 
 

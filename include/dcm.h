@@ -155,14 +155,40 @@ int dcm_advance_scalar_fields_3d(dcm_handle *h, double dt, double *q,
                                  const double *sth, int nq, int moisture);
 
 /* Halo exchanges of mpi_module.f90 for one rank: exchange_full (:926-1271),
- * exchange_along_dim (:700-910), exchange_along_dim_wo (:1285-1494). */
+ * exchange_along_dim (:700-910), exchange_along_dim_wo (:1285-1494),
+ * exchange_full_wo (:1511-1855). */
 int dcm_exchange_full(dcm_handle *h, double *a, double lbc, double ubc);
 int dcm_exchange_along_dim(dcm_handle *h, double *a, double lbc, double ubc);
 int dcm_exchange_along_dim_wo(dcm_handle *h, double *a);
+int dcm_exchange_full_wo(dcm_handle *h, double *a);
+
+/* calculate_subgrid_3d, sgm/subgrid_3d.f90:38-357 (the Smagorinsky model,
+ * with richardson :448-493 and monin_obukhov :373-433), one rank.  z(1) is
+ * the grid's zg[1] (dcm_create needs zg); lamsq has kp+2 values.  In:
+ * u, v, w, zu, zv, zw, th (and q: nq consecutive fields, read only when
+ * moisture != 0).  Inout as in the reference: vism, vist (interior, the
+ * surface row and their exchange_full_wo images), strain (interior), the six
+ * stresses (interior and their exchange_along_dim(0, 0) images), su, sv, sw,
+ * sth (+= the stress / diffusion terms, then exchange_full(0, 0)); with
+ * moisture, viss (nq fields, each set to vist) and sq (nq fields, += the
+ * diffusion of each q, then exchange_full(0, 0)).  The arguments dt, z, zn
+ * and the metric arrays of the Fortran interface come from the handle. */
+int dcm_calculate_subgrid_3d(dcm_handle *h, const double *lamsq, double z0,
+                             double z0th, const double *u, const double *v,
+                             const double *w, const double *zu,
+                             const double *zv, const double *zw,
+                             const double *th, int nq, const double *q,
+                             double *vism, double *vist, double *viss,
+                             double *strain, double *tau11, double *tau22,
+                             double *tau33, double *tau12, double *tau13,
+                             double *tau23, double *su, double *sv,
+                             double *sw, double *sth, double *sq,
+                             int moisture);
 
 /* ---- device-resident time loop ------------------------------------------- */
 /* Configuration of model_driver's dry step (driver_code.f90:304-676) with
- * output, microphysics, radiation, land surface and subgrid off. */
+ * output, microphysics, radiation and land surface off; the subgrid model
+ * (sources with viscous = .true.) on when viscous != 0. */
 typedef struct {
     double dt, ptol;
     int advection_scheme;   /* 0 upwind, 1 mpdata, 2 mpdata_3d_add        */
@@ -180,6 +206,11 @@ typedef struct {
                                of the true residual when its residual has
                                fallen by this factor (0 -> 0.1)            */
     dcm_forcing forcing;
+    int viscous;            /* 1: sources calls calculate_subgrid_3d
+                               (dynamics.f90:878-893); needs the grid's zg */
+    const double *lamsq;    /* kp+2: mixing length squared on the w-levels
+                               (initialisation.f90:449-450)                */
+    double z0, z0th;        /* roughness lengths for momentum and scalars  */
 } dcm_config;
 
 /* Host fields of the driver (all Fortran layout, double).  The three

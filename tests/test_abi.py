@@ -55,3 +55,23 @@ def test_create_rejects_bad_grid_before_touching_the_device():
     g.ip, g.jp, g.kp = 8, 8, 1  # kp < 3
     h = ctypes.c_void_p()
     assert lib.dcm_create(ctypes.byref(g), 0, ctypes.byref(h)) == dcm.DCM_E_ARG
+
+
+def declared_arity():
+    """Number of parameters of every function include/dcm.h declares."""
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    out = {}
+    for m in re.finditer(r"\b(dcm_[a-z0-9_]+)\s*\(([^)]*)\)\s*;", text):
+        args = m.group(2).strip()
+        out[m.group(1)] = 0 if args in ("", "void") else args.count(",") + 1
+    return out
+
+
+def test_binding_signatures_match_the_header():
+    dcm = load_dcm()
+    lib = dcm.library()
+    arity = declared_arity()
+    bad = {n: (len(getattr(lib, n).argtypes), k) for n, k in arity.items()
+           if len(getattr(lib, n).argtypes or ()) != k}
+    assert not bad, bad
