@@ -37,8 +37,10 @@ struct State {
     T *th = nullptr, *th2 = nullptr, *su = nullptr, *sv = nullptr, *sw = nullptr,
       *sth = nullptr, *means = nullptr;
     std::vector<T*> q, sq, qtmp;
-    // subgrid model (viscous): viscosities, strain rate, lamsq (kp+2)
+    // subgrid model (viscous): viscosities, strain rate, lamsq (kp+2) and
+    // the six stresses (scratch of each step)
     T *vism = nullptr, *vist = nullptr, *strain = nullptr, *lamsq = nullptr;
+    T* tau[6]{};
 };
 
 }  // namespace
@@ -1042,6 +1044,7 @@ int step_body(dcm_handle* h, cudaStream_t st, int phase, bool emit) {
         sg.vism = S.vism;
         sg.vist = S.vist;
         sg.strain = S.strain;
+        sg.tau = S.tau;
         sg.q = S.q.data();
         sg.sq = S.sq.data();
         sg.nq = nqq;
@@ -1236,9 +1239,10 @@ int upload_state_t(dcm_handle* h, const dcm_fields* f, const double* lamsq_host)
         launch_convert<float, double>(5 * K2, h->forcing_f, h->forcing_dev, h->st);
     }
     if (cfg.viscous) {
-        // vism, vist and strain are recomputed every step (their previous
-        // values are never read); lamsq in the field precision
-        T** sg[3] = {&S.vism, &S.vist, &S.strain};
+        // vism, vist, strain and the stresses are recomputed every step
+        // (their previous values are never read); lamsq in the field precision
+        T** sg[9] = {&S.vism, &S.vist, &S.strain, &S.tau[0], &S.tau[1],
+                     &S.tau[2], &S.tau[3], &S.tau[4], &S.tau[5]};
         for (auto pp : sg) {
             *pp = alloc_owned<T>(h);
             NEED(*pp);

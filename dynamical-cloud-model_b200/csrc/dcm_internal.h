@@ -192,8 +192,7 @@ struct ScalarSet {
     int n;
     unsigned reset;
 };
-// tau (six fields: tau11, tau22, tau33, tau12, tau13, tau23) may be null;
-// rows = true applies the surface / lid rows of sources to su, sv, sw
+// tau: six fields (tau11, tau22, tau33, tau12, tau13, tau23); rows = true applies the surface / lid rows of sources to su, sv, sw
 // instead of their exchange_full images alone
 template <typename T>
 void launch_subgrid(const Dims& d, const Metrics<T>& mt, const SgsParams<T>& P, const T* u,
@@ -215,6 +214,7 @@ template <typename T>
 struct SgsStep {
     SgsParams<T> P;
     T *vism, *vist, *strain;
+    T* const* tau; // six stress fields (scratch)
     T* const* q;   // nq current q fields
     T* const* sq;  // their sources
     int nq;

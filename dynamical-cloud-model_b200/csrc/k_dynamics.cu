@@ -307,7 +307,7 @@ void launch_sources(const Dims& d, const Metrics<T>& mt, const Metrics<R>& mtr,
         const int ns = make_scalar_sets<T>(th, sth, 0, sg->q, sg->sq, sg->nq, 1, sets,
                                            SGS_MAX_SETS);
         launch_subgrid<T>(d, mt, sg->P, u, v, w, zu, zv, zw, th, sg->vism, sg->vist, sg->strain,
-                          nullptr, su, sv, sw, sets, ns < 0 ? 0 : ns, true, st);
+                          sg->tau, su, sv, sw, sets, ns < 0 ? 0 : ns, true, st);
     }
     { ProfScope ps_(P_RHS, st);
     k_rhs<T, R><<<interior_grid(d, d.kp + 2), b, 0, st>>>(d, mtr, su, sv, sw, rhs, rhs_wo);

@@ -10,16 +10,16 @@
 //   k_sgs_visc    strain, vism, vist (+ the surface row k = 0) and the
 //                 exchange_full_wo images of vism / vist      (:91-180)
 //   k_sgs_tau     the six stresses with their exchange_along_dim images
-//                 (:191-237); only the stand-alone entry point needs them as
-//                 arrays
-//   k_sgs_mom     su, sv, sw += stress divergence (:240-284), the stresses
-//                 re-evaluated in registers from vism and zu, zv, zw instead
-//                 of re-read from six arrays (the stress that a halo index
-//                 names is the exchanged periodic image, so the index is
-//                 wrapped onto the interior first: the same arithmetic on
-//                 the same operands as the array form)
+//                 (:191-237)
+//   k_sgs_mom     su, sv, sw += stress divergence (:240-284)
 //   k_sgs_scalar  sth and every sq += diffusion (:289-345), th and the q
 //                 fields in one pass so that vist's stencil is loaded once
+// In FP64 these kernels are bound by the latency of the IEEE divisions that
+// parity with the reference keeps (about 30 per cell in k_sgs_visc), not by
+// HBM.  The stresses therefore go through six arrays, as in the reference:
+// evaluating each once and re-reading it costs 12 field passes of HBM,
+// re-evaluating the 15 that a cell's momentum sources name costs about twice
+// the divisions.
 // The image writers are those of dcm_common.cuh; in the time step the
 // momentum kernel also applies the surface / lid rows of sources
 // (dynamics.f90:922-973), as k_sources does in the inviscid step.
@@ -44,11 +44,7 @@ __device__ __forceinline__ float sg_pow(float x, float y) { return powf(x, y); }
 template <typename T>
 __device__ __forceinline__ T sq2(T x) { return x * x; }
 
-// periodic wrap of an index one step outside 1..n (the exchanged image)
-__device__ __forceinline__ int wrap1(int c, int n) { return c < 1 ? n : (c > n ? 1 : c); }
-
-// The stresses at interior cell (k, j, i), sgm/subgrid_3d.f90:194-220, each
-// written once and used both by k_sgs_tau and by k_sgs_mom.
+// The stresses at interior cell (k, j, i), sgm/subgrid_3d.f90:194-220.
 template <typename T>
 struct Stress {
     Dims d;
@@ -94,7 +90,7 @@ struct Stress {
 
 // ---- strain, Richardson functions, viscosities, surface layer -------------
 template <typename T>
-__global__ void __launch_bounds__(256) k_sgs_visc(Dims d, Metrics<T> mt, SgsParams<T> P,
+__global__ void __launch_bounds__(256, 4) k_sgs_visc(Dims d, Metrics<T> mt, SgsParams<T> P,
                                                   const T* __restrict__ u,
                                                   const T* __restrict__ v,
                                                   const T* __restrict__ w,
@@ -224,24 +220,24 @@ __global__ void __launch_bounds__(256) k_sgs_tau(Dims d, Metrics<T> mt, const T*
 }
 
 // ---- su, sv, sw += divergence of the stresses -----------------------------
-// ROWS = false: the exchange_full(0, 0) images of su, sv, sw (:279-284).
-// ROWS = true: those images followed by the surface / lid rows of sources
-// (dynamics.f90:922-973): levels 0 = -(level 1) for su, sv and 0 for sw,
-// levels kp, kp+1 = 0.
+// The stresses come from k_sgs_tau's arrays, halo faces included (the images
+// of exchange_along_dim).  ROWS = false: the exchange_full(0, 0) images of
+// su, sv, sw (:279-284).  ROWS = true: those images followed by the surface /
+// lid rows of sources (dynamics.f90:922-973): levels 0 = -(level 1) for su,
+// sv and 0 for sw, levels kp, kp+1 = 0.
 template <typename T, bool ROWS>
-__global__ void __launch_bounds__(256) k_sgs_mom(Dims d, Metrics<T> mt, const T* __restrict__ vism,
-                                                 const T* __restrict__ zu,
-                                                 const T* __restrict__ zv,
-                                                 const T* __restrict__ zw, T* __restrict__ su,
+__global__ void __launch_bounds__(256) k_sgs_mom(Dims d, Metrics<T> mt, const T* __restrict__ t11,
+                                                 const T* __restrict__ t22,
+                                                 const T* __restrict__ t33,
+                                                 const T* __restrict__ t12,
+                                                 const T* __restrict__ t13,
+                                                 const T* __restrict__ t23, T* __restrict__ su,
                                                  T* __restrict__ sv, T* __restrict__ sw) {
     const int k = 1 + blockIdx.x * BX + threadIdx.x;
     const int j = 1 + blockIdx.y * BY + threadIdx.y;
     const int i = 1 + blockIdx.z;
     if (k > d.kp || j > d.jp) return;
-    const Stress<T> S{d, mt, vism, zu, zv, zw};
     const int o = d.at(k, j, i);
-    const int ip1 = wrap1(i + 1, d.ip), im1 = wrap1(i - 1, d.ip);
-    const int jp1 = wrap1(j + 1, d.jp), jm1 = wrap1(j - 1, d.jp);
     const T z = T(0);
     if (ROWS && k == d.kp) {
         put_plane_images(su, d, d.kp, j, i, z);
@@ -255,16 +251,16 @@ __global__ void __launch_bounds__(256) k_sgs_mom(Dims d, Metrics<T> mt, const T*
     T vsu = su[o], vsv = sv[o], vsw = sw[o];
     const T dxm = ld(mt.dx + i - 1), dym = ld(mt.dy + j - 1);
     if (k <= d.kp - 1) {  // :256-261
-        const T t13 = S.t13(k, j, i), t23 = S.t23(k, j, i);
-        vsw = vsw + ((S.t33(k + 1, j, i) - S.t33(k, j, i)) / ld(mt.dzn + k) +
-                     (t13 - S.t13(k, j, im1)) / dxm + (t23 - S.t23(k, jm1, i)) / dym);
+        const T c13 = t13[o], c23 = t23[o];
+        vsw = vsw + ((t33[d.at(k + 1, j, i)] - t33[o]) / ld(mt.dzn + k) +
+                     (c13 - t13[d.at(k, j, i - 1)]) / dxm + (c23 - t23[d.at(k, j - 1, i)]) / dym);
         if (k >= 2) {  // :262-274
-            const T t12 = S.t12(k, j, i);
+            const T c12 = t12[o];
             const T dzm = ld(mt.dz + k - 1);
-            vsu = vsu + ((S.t11(k, j, ip1) - S.t11(k, j, i)) / ld(mt.dxn + i) +
-                         (t12 - S.t12(k, jm1, i)) / dym + (t13 - S.t13(k - 1, j, i)) / dzm);
-            vsv = vsv + ((S.t22(k, jp1, i) - S.t22(k, j, i)) / ld(mt.dyn + j) +
-                         (t12 - S.t12(k, j, im1)) / dxm + (t23 - S.t23(k - 1, j, i)) / dzm);
+            vsu = vsu + ((t11[d.at(k, j, i + 1)] - t11[o]) / ld(mt.dxn + i) +
+                         (c12 - t12[d.at(k, j - 1, i)]) / dym + (c13 - t13[d.at(k - 1, j, i)]) / dzm);
+            vsv = vsv + ((t22[d.at(k, j + 1, i)] - t22[o]) / ld(mt.dyn + j) +
+                         (c12 - t12[d.at(k, j, i - 1)]) / dxm + (c23 - t23[d.at(k - 1, j, i)]) / dzm);
         }
     }
     if (ROWS) {
@@ -285,7 +281,7 @@ __global__ void __launch_bounds__(256) k_sgs_mom(Dims d, Metrics<T> mt, const T*
 
 // ---- sth, sq += diffusion (vist carries rhoa), exchange_full(0, 0) --------
 template <typename T>
-__global__ void __launch_bounds__(256) k_sgs_scalar(Dims d, Metrics<T> mt,
+__global__ void __launch_bounds__(256, 4) k_sgs_scalar(Dims d, Metrics<T> mt,
                                                     const T* __restrict__ vist, ScalarSet<T> set) {
     const int k = 1 + blockIdx.x * BX + threadIdx.x;
     const int j = 1 + blockIdx.y * BY + threadIdx.y;
@@ -327,13 +323,14 @@ void launch_subgrid(const Dims& d, const Metrics<T>& mt, const SgsParams<T>& P, 
     const dim3 b(BX, BY), g = interior_grid(d, d.kp);
     ProfScope ps_(P_SOURCES, st);
     k_sgs_visc<T><<<g, b, 0, st>>>(d, mt, P, u, v, w, th, vism, vist, strain);
-    if (tau)
-        k_sgs_tau<T><<<g, b, 0, st>>>(d, mt, vism, zu, zv, zw, tau[0], tau[1], tau[2], tau[3],
-                                      tau[4], tau[5]);
+    k_sgs_tau<T><<<g, b, 0, st>>>(d, mt, vism, zu, zv, zw, tau[0], tau[1], tau[2], tau[3],
+                                  tau[4], tau[5]);
     if (rows)
-        k_sgs_mom<T, true><<<g, b, 0, st>>>(d, mt, vism, zu, zv, zw, su, sv, sw);
+        k_sgs_mom<T, true><<<g, b, 0, st>>>(d, mt, tau[0], tau[1], tau[2], tau[3], tau[4],
+                                            tau[5], su, sv, sw);
     else
-        k_sgs_mom<T, false><<<g, b, 0, st>>>(d, mt, vism, zu, zv, zw, su, sv, sw);
+        k_sgs_mom<T, false><<<g, b, 0, st>>>(d, mt, tau[0], tau[1], tau[2], tau[3], tau[4],
+                                             tau[5], su, sv, sw);
     for (int c = 0; c < nsets; c++) k_sgs_scalar<T><<<g, b, 0, st>>>(d, mt, vist, sets[c]);
 }
 
