@@ -53,7 +53,8 @@ class _Config(C.Structure):
                 ("c_s", C.POINTER(C.c_int)), ("c_e", C.POINTER(C.c_int)),
                 ("thbase", C.c_double), ("thtop", C.c_double), ("precision", C.c_int),
                 ("inner_tol", C.c_double), ("forcing", _Forcing), ("viscous", C.c_int),
-                ("lamsq", _dp), ("z0", C.c_double), ("z0th", C.c_double)]
+                ("lamsq", _dp), ("z0", C.c_double), ("z0th", C.c_double),
+                ("precond", C.c_int), ("precond_lo", C.c_double)]
 
 
 class _Fields(C.Structure):
@@ -394,9 +395,12 @@ class DynamicalCore:
     # ---- the device-resident time loop (model_driver) ---------------------------
     def upload_state(self, state, dt, ptol=1e-10, kord=3, monotone=True, advection_scheme=1,
                      limiter=0, itmax=9999, nq=0, c_s=(), c_e=(), thbase=0.0, thtop=0.0,
-                     forcing=None, precision=0, inner_tol=0.1, viscous=None):
+                     forcing=None, precision=0, inner_tol=0.1, viscous=None, precond=0,
+                     precond_lo=0.05):
         """viscous = dict(lamsq=(kp+2,), z0=..., z0th=...) switches the
-        subgrid model on in sources (dynamics.f90:878-893)."""
+        subgrid model on in sources (dynamics.f90:878-893).  precond = 1
+        gives the mixed form's FP32 iterations Chebyshev-weighted Jacobi
+        sweeps on [precond_lo, 2] (0: the reference's sweeps)."""
         K2 = self.grid.kp + 2
         cfg = _Config()
         cfg.dt, cfg.ptol = float(dt), float(ptol)
@@ -409,6 +413,7 @@ class DynamicalCore:
         cfg.c_s, cfg.c_e = self._cs, self._ce
         cfg.thbase, cfg.thtop, cfg.precision = float(thbase), float(thtop), int(precision)
         cfg.inner_tol = float(inner_tol)
+        cfg.precond, cfg.precond_lo = int(precond), float(precond_lo)
         fs, fkeep = self._forcing(forcing)
         if fs is not None:
             cfg.forcing = fs

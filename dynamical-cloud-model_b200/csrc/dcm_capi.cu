@@ -977,6 +977,8 @@ SolverWork<float> solver_work_f(dcm_handle* h) {
     w.ni = h->tune_ni[1];
     w.fuse = h->tune_fuse[1];
     w.max_blocks = (int)std::min<size_t>(h->npartials / 3, (size_t)1 << 30);
+    w.cheb = h->cfg.precond == 1 ? 1 : 0;
+    w.cheb_lo = h->cfg.precond_lo > 0.0 ? h->cfg.precond_lo : 0.05;
     return w;
 }
 
@@ -1310,6 +1312,10 @@ extern "C" int dcm_state_upload(dcm_handle* h, const dcm_config* cfg, const dcm_
     if (cfg->moisture && (cfg->nq < 1 || cfg->nq > NQMAX || cfg->ncat < 1 || !cfg->c_s ||
                           !cfg->c_e || !f->q))
         return fail(h, DCM_E_ARG, "state_upload: bad moisture config");
+    if (cfg->precond != 0 && cfg->precond != 1)
+        return fail(h, DCM_E_ARG, "state_upload: precond must be 0 or 1");
+    if (cfg->precond == 1 && !(cfg->precond_lo >= 0.0 && cfg->precond_lo < 2.0))
+        return fail(h, DCM_E_ARG, "state_upload: precond_lo must lie in [0, 2)");
     if (cfg->viscous && (!cfg->lamsq || !(cfg->z0 > 0.0) || !(cfg->z0th > 0.0)))
         return fail(h, DCM_E_ARG, "state_upload: viscous needs lamsq, z0 > 0 and z0th > 0");
     if (cfg->viscous && h->h_zg.size() < 2)

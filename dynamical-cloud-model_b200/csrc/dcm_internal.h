@@ -87,6 +87,11 @@ struct SolverWork {
     int ni = 4;
     // FP32: fuse the three Jacobi sweeps of a phase (columns of <= 128 levels)
     int fuse = 1;
+    // FP32 iterations of the mixed form: Chebyshev-weighted Jacobi sweeps on
+    // the interval [cheb_lo, 2] of the spectrum of D^-1 A (0: the reference's
+    // unweighted sweeps)
+    int cheb = 0;
+    double cheb_lo = 0.05;
 };
 
 // one-time setup of the solver kernels (shared-memory limits); called at

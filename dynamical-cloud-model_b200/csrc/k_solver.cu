@@ -36,6 +36,7 @@
 // few ulp per sweep, far below the 1e-10 parity bar.  The iteration then
 // moves 41 field passes instead of 39.
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <type_traits>
@@ -65,6 +66,11 @@ struct SolverArgs {
     int max_blocks;   // blocks a reducing kernel may use (partials capacity)
     int ni;           // i-planes a stencil warp task marches over
     int fuse;         // FP32: the three sweeps of a phase as one kernel (k_precond3)
+    // Chebyshev-weighted sweeps (mixed form only): x1 = cw[0] s0, then
+    // x_m+1 = x_m + cw[m] (s0 - (A x_m)/a_p), m = 1..3, in place of the
+    // reference's x1 = s0, x_m+1 = x_m + s0 - (A x_m)/a_p
+    int cheb;
+    double cw[4];
 };
 
 // a_p exactly as set_mat_a forms it (dynamics.f90:93-95)
@@ -87,6 +93,7 @@ enum SOp {
 struct SolverBufs {
     const void *x, *b, *r, *v1, *rh, *vh, *sin, *cr;
     void *out, *out2, *out3;
+    int sweep;  // 1..3: which Jacobi sweep of the preconditioner a launch is
 };
 
 // q / a_p of the preconditioner input, formed from rh = r/a_p and vh = v1/a_p:
@@ -103,6 +110,19 @@ __device__ __forceinline__ T s0val(const T* __restrict__ rh, const T* __restrict
 // blockIdx.z -> i.  k neighbours come from the adjacent lanes by shuffle
 // (Neumann mirror at k = 1 and kp, dynamics.f90:206-211), j and i
 // neighbours (periodic) through L1/L2.
+// One Chebyshev-weighted sweep at a point, with every rounding explicit so
+// that the fused and the separate sweeps agree bit for bit:
+//     res = sc x + w (s0 - sc (A x)/a_p),   q = (A x)/a_p
+// sc = w1 on the first sweep (its operand is w1 s0, applied here by
+// linearity instead of to the seven operand values), 1 on the others.
+__device__ __forceinline__ float cheb_update(float xc, float s0, float q, float sc, float w) {
+    return __fmaf_rn(w, __fsub_rn(s0, __fmul_rn(q, sc)), __fmul_rn(xc, sc));
+}
+__device__ __forceinline__ double cheb_update(double xc, double s0, double q, double sc,
+                                              double w) {
+    return __fma_rn(w, __dsub_rn(s0, __dmul_rn(q, sc)), __dmul_rn(xc, sc));
+}
+
 template <typename T, int OP, int MODE>
 struct StenCtx {
     Dims d;
@@ -113,6 +133,9 @@ struct StenCtx {
     SolverBufs B;
     T bet, omg, alf;
     bool first;
+    bool cheb;  // weighted sweeps (cheb_update)
+    T wx;       // first sweep: the scale w1 of its operand s0 (1 otherwise)
+    T ws;       // this sweep's weight
 };
 
 // Ask L2 for the line holding p ahead of its use (no register is written).
@@ -355,8 +378,14 @@ __device__ __forceinline__ void sten_task(const StenCtx<T, OP, MODE>& C, int kc,
             C1.first = C.first;
             xload(C1, o, s0);
         }
+        if (C.cheb) {
 #pragma unroll
-        for (int q = 0; q < V; q++) res[q] = xc[q] + s0[q] - Ax[q] / ap[q];
+            for (int q = 0; q < V; q++)
+                res[q] = cheb_update(xc[q], s0[q], Ax[q] / ap[q], C.wx, C.ws);
+        } else {
+#pragma unroll
+            for (int q = 0; q < V; q++) res[q] = xc[q] + s0[q] - Ax[q] / ap[q];
+        }
         if (OP == OP_SW3P) {
             T pold[V];
             if (C.first) {
@@ -455,6 +484,10 @@ __global__ void __launch_bounds__(256) k_sten(SolverArgs a, Coef<T> c, SolverBuf
     C.omg = (T)S->omg;
     C.alf = (T)S->alf;
     C.first = S->it == 0 || S->fresh;
+    C.cheb = a.cheb != 0;
+    C.wx = (OP == OP_SW1 && a.cheb) ? (T)a.cw[0] : T(1);
+    // (selected, not indexed: a run-time index would copy a.cw to the stack)
+    C.ws = !a.cheb ? T(1) : (T)(B.sweep == 3 ? a.cw[3] : B.sweep == 2 ? a.cw[2] : a.cw[1]);
     const Dims& d = a.d;
     double acc[NV];
 #pragma unroll
@@ -528,7 +561,7 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 
 __device__ __forceinline__ int wrapn(int q, int n) { return ((q - 1) % n + n) % n + 1; }
 
-template <int MODE>
+template <int MODE, bool CHEB>
 __global__ void __launch_bounds__(PW * 32, 1)
     k_precond3(SolverArgs a, Coef<float> c, SolverBufs B, const SolverScalars* S, int ni) {
     // [stage 0..2][buffer 0..1][warp][lane], then the copy-ahead ring
@@ -556,6 +589,10 @@ __global__ void __launch_bounds__(PW * 32, 1)
     const float an = ld(c.an + jw), as = ld(c.as + jw);
     const float bet = (float)S->bet, omg = (float)S->omg, alf = (float)S->alf;
     const bool first = S->it == 0 || S->fresh;
+    // CHEB: weighted sweeps (cheb_update); stage 1's operand is w1 s0, and
+    // stages 1..3 weigh their corrections by w2..w4
+    const float w1 = CHEB ? (float)a.cw[0] : 1.0f, w2 = CHEB ? (float)a.cw[1] : 1.0f,
+                w3 = CHEB ? (float)a.cw[2] : 1.0f, w4 = CHEB ? (float)a.cw[3] : 1.0f;
     const float* __restrict__ rh = (const float*)B.rh;
     const float* __restrict__ vh = (const float*)B.vh;
     float* __restrict__ out = (float*)B.out;
@@ -594,10 +631,12 @@ __global__ void __launch_bounds__(PW * 32, 1)
 #pragma unroll
         for (int e = 0; e < 4; e++) s[e] = MODE == 0 ? x[e] - bet * (omg * y[e]) : x[e] - alf * y[e];
     };
-    // one Jacobi sweep at plane q: res = xc + s0c - (A x)/a_p, A in the FP32
-    // difference form of sten_task
+    // one Jacobi sweep at plane q: res = xc + s0c - (A x)/a_p (the
+    // reference's sweep), or with CHEB cheb_update(xc, s0c, (A x)/a_p, sc, wv);
+    // A in the FP32 difference form of sten_task
     auto sweep = [&](int iq, const float (&xm)[4], const float (&xc)[4], const float (&xp)[4],
-                     const float4 xs4, const float4 xn4, const float (&s0c)[4], float (&res)[4]) {
+                     const float4 xs4, const float4 xn4, const float (&s0c)[4], float (&res)[4],
+                     float sc, float wv) {
         const float ae = ld(c.ae + iq), aw = ld(c.aw + iq);
         const float sij = -ae - aw - an - as;
         const float xs[4] = {xs4.x, xs4.y, xs4.z, xs4.w}, xn[4] = {xn4.x, xn4.y, xn4.z, xn4.w};
@@ -614,7 +653,7 @@ __global__ void __launch_bounds__(PW * 32, 1)
             const float c0 = xc[e];
             const float Ax = aw * (xm[e] - c0) + ae * (xp[e] - c0) + as * (xs[e] - c0) +
                              an * (xn[e] - c0) + ad[e] * (xd - c0) + au[e] * (xu - c0);
-            res[e] = xc[e] + s0c[e] - Ax / ap;
+            res[e] = CHEB ? cheb_update(xc[e], s0c[e], Ax / ap, sc, wv) : xc[e] + s0c[e] - Ax / ap;
         }
     };
     float R0[4][4], R1[3][4], R2[3][4];  // s0 at b..b+3, s1 at b..b+2, s2 at b-1..b+1
@@ -638,17 +677,18 @@ __global__ void __launch_bounds__(PW * 32, 1)
         // stage 1: s1 at plane b+2 (j neighbours: s0 at b+2 from the last step)
         if (st1 && b >= i0 - 4) {
             sweep(q2, R0[1], R0[2], R0[3], slot(0, prv, w - 1), slot(0, prv, w + 1), R0[2],
-                  R1[2]);
+                  R1[2], w1, w2);
         }
         // stage 2: s2 at plane b+1
         if (st2 && b >= i0 - 2) {
             sweep(q1, R1[0], R1[1], R1[2], slot(1, prv, w - 1), slot(1, prv, w + 1), R0[1],
-                  R2[2]);
+                  R2[2], 1.0f, w3);
         }
         // stage 3: s3 at plane b, the output
         if (outrow && b >= i0) {
             float s3[4];
-            sweep(b, R2[0], R2[1], R2[2], slot(2, prv, w - 1), slot(2, prv, w + 1), R0[0], s3);
+            sweep(b, R2[0], R2[1], R2[2], slot(2, prv, w - 1), slot(2, prv, w + 1), R0[0], s3,
+                  1.0f, w4);
             const int o = col + KJ * b;
             if (MODE == 0) {
                 if (first) {
@@ -908,17 +948,19 @@ static void precond3(const SolverArgs& a, const Coef<float>& c, const SolverBufs
     const int nch = std::max(1, std::min((a.d.ip + 7) / 8, sm_count() / nstrips));
     const int ni = (a.d.ip + nch - 1) / nch;
     const dim3 grid(nstrips, (a.d.ip + ni - 1) / ni);
+    auto go = [&](auto kern) { kern<<<grid, PW * 32, PRECOND3_SMEM, st>>>(a, c, B, S, ni); };
     if (mode == 0)
-        k_precond3<0><<<grid, PW * 32, PRECOND3_SMEM, st>>>(a, c, B, S, ni);
+        a.cheb ? go(k_precond3<0, true>) : go(k_precond3<0, false>);
     else
-        k_precond3<1><<<grid, PW * 32, PRECOND3_SMEM, st>>>(a, c, B, S, ni);
+        a.cheb ? go(k_precond3<1, true>) : go(k_precond3<1, false>);
 }
 
 void solver_init() {
-    cudaFuncSetAttribute(k_precond3<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)PRECOND3_SMEM);
-    cudaFuncSetAttribute(k_precond3<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)PRECOND3_SMEM);
+    const int sm = (int)PRECOND3_SMEM;
+    cudaFuncSetAttribute(k_precond3<0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    cudaFuncSetAttribute(k_precond3<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    cudaFuncSetAttribute(k_precond3<0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    cudaFuncSetAttribute(k_precond3<1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
 }
 
 template <typename T>
@@ -938,12 +980,15 @@ static void launch_iteration(const SolverArgs& a, const Coef<T>& c, SolverWork<T
         }
     } else {
         B.out = w.sA;
+        B.sweep = 1;
         sten<T, OP_SW1, 0>(a, c, B, w, st, P_JACOBI);
         B.sin = w.sA;
         B.out = w.sB;
+        B.sweep = 2;
         sten<T, OP_SW, 0>(a, c, B, w, st, P_JACOBI);
         B.sin = w.sB;
         B.out = w.p;
+        B.sweep = 3;
         sten<T, OP_SW3P, 0>(a, c, B, w, st, P_JACOBI);
     }
     B.sin = w.p;
@@ -960,12 +1005,15 @@ static void launch_iteration(const SolverArgs& a, const Coef<T>& c, SolverWork<T
         }
     } else {
         B.out = w.sA;
+        B.sweep = 1;
         sten<T, OP_SW1, 1>(a, c, B, w, st, P_JACOBI);
         B.sin = w.sA;
         B.out = w.sB;
+        B.sweep = 2;
         sten<T, OP_SW, 1>(a, c, B, w, st, P_JACOBI);
         B.sin = w.sB;
         B.out = w.sA;
+        B.sweep = 3;
         sten<T, OP_SW, 1>(a, c, B, w, st, P_JACOBI);
     }
     B.sin = w.sA;
@@ -1069,6 +1117,23 @@ bool side_streams(SolveGraph& G) {
 
 }  // namespace
 
+// Weights of the Chebyshev-weighted sweeps: the preconditioned operator is
+// 1 - R(D^-1 A) with R(mu) = prod_m (1 - mu / theta_m), theta_m the four
+// roots of the degree-4 Chebyshev polynomial on [lo, 2]
+// (theta_m = (2 + lo)/2 + (2 - lo)/2 cos((2m - 1) pi / 8)); the reference's
+// sweeps are theta_m = 1, R(mu) = (1 - mu)^4, which vanishes at mu = 0 and at
+// the checkerboard modes' mu = 2 alike.  Same three operator applications.
+static void cheb_weights(double lo, double (&w)[4]) {
+    const double pi = 3.14159265358979323846;
+    for (int m = 1; m <= 4; m++)
+        w[m - 1] = 1.0 / ((2.0 + lo) / 2.0 + (2.0 - lo) / 2.0 * std::cos((2 * m - 1) * pi / 8.0));
+}
+
+static void no_cheb(SolverArgs& a) {
+    a.cheb = 0;
+    for (double& x : a.cw) x = 1.0;
+}
+
 template <typename T>
 int solver_run(SolverWork<T>& w, const Dims& d, T* x, const T* b, const T* sw, const T* dzn,
                double tol, int itmax, int wo, int chunk, cudaStream_t st, SolverScalars* host_S,
@@ -1086,6 +1151,7 @@ int solver_run(SolverWork<T>& w, const Dims& d, T* x, const T* b, const T* sw, c
     a.max_blocks = w.max_blocks;
     a.ni = w.ni >= 1 ? w.ni : 1;
     a.fuse = w.fuse;
+    no_cheb(a);  // the FP64 path keeps the reference's sweeps
     const Coef<T> c = coef_of(w);
     SolverBufs B{};
     B.x = x;
@@ -1355,10 +1421,15 @@ int refine_run(SolverWork<float>& wf, SolverWork<double>& wd, const Dims& d, dou
     a.max_blocks = wf.max_blocks;
     a.ni = 1;                      // the FP64 residual does not march
     a.fuse = 0;
+    no_cheb(a);
     SolverArgs af = a;             // vector warp tasks of the FP32 iterations
     af.nkt = kchunks<float>(d);
     af.ni = wf.ni >= 1 ? wf.ni : 1;
     af.fuse = wf.fuse;
+    if (wf.cheb) {
+        af.cheb = 1;
+        cheb_weights(wf.cheb_lo, af.cw);
+    }
     Coef<double> cd;
     cd.ae = wd.ae; cd.aw = wd.aw; cd.an = wd.an; cd.as = wd.as; cd.au = wd.au; cd.ad = wd.ad;
     const Coef<float> cf = coef_of(wf);
@@ -1423,8 +1494,9 @@ int refine_run(SolverWork<float>& wf, SolverWork<double>& wd, const Dims& d, dou
     if (use_graph) {
         SolveGraph& G = *wf.graph;
         const void* kp[6] = {x, b, sw, dzn, dx, wf.S};
-        const double kd[3] = {tol, delta, 0.0};
-        const int shape = af.by + 16 * af.tasks + 256 * af.ni + 16384 * af.fuse;
+        const double kd[3] = {tol, delta, af.cheb ? wf.cheb_lo : 0.0};
+        const int shape =
+            af.by + 16 * af.tasks + 256 * af.ni + 16384 * af.fuse + 32768 * af.cheb;
         const int ki[6] = {itmax, max_updates, 1, 16 * shape, d.ip * 4096 + d.jp, d.kp};
         if (!G.matches(kp, kd, ki)) {
             G.release();

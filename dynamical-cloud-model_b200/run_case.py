@@ -10,7 +10,9 @@ kelvin_helmholtz (128x1x64), or warm_bubble_IPxJPxKP /
 sheared_convection_IPxJPxKP for other sizes.  --host-loop drives the
 pressure solve from the host (the same kernels; a profiler sees every
 launch, which it cannot inside the graph-driven solve's conditional loop).
---viscous switches the Smagorinsky subgrid model on in sources (cvis 0.23,
+--precond 1 gives the mixed form Chebyshev-weighted sweeps on
+[--precond-lo, 2].  --viscous switches the Smagorinsky subgrid model on in
+sources (cvis 0.23,
 z0 = z0th = 0.1 m); --profile prints the device time per kernel class over
 the steps after the first.
 """
@@ -56,6 +58,8 @@ def main():
     ap.add_argument("--host-loop", action="store_true")
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--viscous", action="store_true")
+    ap.add_argument("--precond", type=int, default=0, choices=[0, 1])
+    ap.add_argument("--precond-lo", type=float, default=0.05)
     ap.add_argument("--profile", action="store_true")
     args = ap.parse_args()
     dcm = load()
@@ -68,7 +72,8 @@ def main():
     if args.viscous:
         kw["viscous"] = dict(lamsq=cases.mixing_length_sq(c.grid, 0.23, 0.1), z0=0.1, z0th=0.1)
     core.upload_state(c.state, c.dt, ptol=c.ptol, kord=c.kord, monotone=c.monotone,
-                      precision=args.precision, **kw)
+                      precision=args.precision, precond=args.precond,
+                      precond_lo=args.precond_lo, **kw)
     core.driver_start()
     for s in range(args.steps):
         if args.profile and s == min(1, args.steps - 1):

@@ -211,6 +211,14 @@ typedef struct {
     const double *lamsq;    /* kp+2: mixing length squared on the w-levels
                                (initialisation.f90:449-450)                */
     double z0, z0th;        /* roughness lengths for momentum and scalars  */
+    int precond;            /* precision 1: preconditioner of the FP32
+                               iterations.  0: the reference's three Jacobi
+                               sweeps (dynamics.f90:241-270); 1: the same
+                               three sweeps with Chebyshev weights on
+                               [precond_lo, 2] of the spectrum of D^-1 A
+                               (fewer iterations, same cost per iteration).
+                               FP64 always uses the reference's sweeps.     */
+    double precond_lo;      /* lower end of that interval (0 -> 0.05)      */
 } dcm_config;
 
 /* Host fields of the driver (all Fortran layout, double).  The three

@@ -19,10 +19,10 @@ MIXED_TOL = 1e-5
 FIELDS = ("u", "v", "w", "zu", "zv", "zw", "th", "su", "sv", "sw")
 
 
-def _run(dcm, orc, c, nsteps, **kw):
+def _run(dcm, orc, c, nsteps, precond=0, **kw):
     core = dcm.DynamicalCore(c.grid)
     core.upload_state(c.state, c.dt, ptol=c.ptol, kord=c.kord, monotone=c.monotone,
-                      nq=c.nq, c_s=c.c_s, c_e=c.c_e, precision=1, **kw)
+                      nq=c.nq, c_s=c.c_s, c_e=c.c_e, precision=1, precond=precond, **kw)
     core.driver_start()
     errs = []
     for _ in range(nsteps):
@@ -43,10 +43,14 @@ def _errors(c, got, ref):
     return e
 
 
-@pytest.mark.parametrize("case,nsteps", [("bubble", 1), ("kh", 1), ("bubble", 10)])
-def test_mixed_against_oracle(dcm, orc, case, nsteps):
+# The 2-D shear layer is held to one step: its u of 10 m/s makes the centred
+# momentum sources near-cancelling sums, which FP32 fields resolve to about
+# 1e-3 of their own size after a few steps (whatever the preconditioner).
+@pytest.mark.parametrize("case,nsteps,precond", [("bubble", 1, 0), ("kh", 1, 0), ("bubble", 10, 0),
+                                                 ("bubble", 10, 1), ("kh", 1, 1)])
+def test_mixed_against_oracle(dcm, orc, case, nsteps, precond):
     c = small_bubble() if case == "bubble" else cases.kelvin_helmholtz(ip=40, jp=1, kp=12)
-    got, ref, errs = _run(dcm, orc, c, nsteps)
+    got, ref, errs = _run(dcm, orc, c, nsteps, precond=precond)
     assert all(e < c.ptol for e in errs), errs
     e = _errors(c, got, ref)
     print(case, nsteps, {k: f"{v:.2e}" for k, v in e.items()})
@@ -87,24 +91,50 @@ def test_graph_and_host_loops_agree(dcm, precision):
         assert np.array_equal(fa[n], fb[n]), n
 
 
+@pytest.mark.parametrize("precond", [0, 1])
 @pytest.mark.parametrize("shape", [(24, 20, 16), (9, 30, 37), (1, 16, 14), (40, 1, 12)])
-def test_fused_preconditioner_matches_unfused(dcm, shape):
+def test_fused_preconditioner_matches_unfused(dcm, shape, precond):
     """The fused three-sweep preconditioner (FP32) performs each point's
-    arithmetic of the three separate sweeps: the two launch shapes give the
-    same iterations and fields to FP32 round-off, on strips and chunks that
-    wrap (jp < 20, ip = 1) and on ragged columns."""
+    arithmetic of the three separate sweeps, unweighted and Chebyshev
+    weighted: the two launch shapes give the same iterations and fields to
+    FP32 round-off, on strips and chunks that wrap (jp < 20, ip = 1) and on
+    ragged columns."""
     ip, jp, kp = shape
     c = cases.warm_bubble(ip=ip, jp=jp, kp=kp, dxyz=50.0, radius=200.0, zc=200.0, seed=41)
     out = []
     for fuse in (1, 0):
         core = dcm.DynamicalCore(c.grid)
         core.set_launch_shape(1, fuse=fuse)
-        core.upload_state(c.state, c.dt, ptol=c.ptol, kord=c.kord, precision=1)
+        core.upload_state(c.state, c.dt, ptol=c.ptol, kord=c.kord, precision=1,
+                          precond=precond)
         core.driver_start()
         its = [core.step(1).iters_last for _ in range(3)]
         out.append((its, core.download_state()))
         core.close()
     (ia, fa), (ib, fb) = out
-    assert max(abs(a - b) for a, b in zip(ia, ib)) <= 2
+    # the two launch shapes contract a few products into FMAs differently,
+    # so the FP32 recursions part by round-off and stop a few iterations apart
+    assert max(abs(a - b) for a, b in zip(ia, ib)) <= 4, (ia, ib)
+    assert abs(sum(ia) - sum(ib)) <= 0.05 * sum(ib), (ia, ib)
     for n in ("u", "v", "w", "th"):
         assert relerr(fa[n], fb[n]) <= 1e-6, n
+
+
+def test_chebyshev_sweeps_take_fewer_iterations(dcm):
+    """The Chebyshev-weighted sweeps cost the same three operator
+    applications as the reference's and converge in fewer FP32 iterations
+    (the reference's preconditioned operator 1 - (1 - mu)^4 vanishes at the
+    checkerboard modes' mu = 2 as well as at mu = 0)."""
+    c = cases.warm_bubble(ip=48, jp=48, kp=32, dxyz=50.0, radius=500.0, zc=600.0, seed=43)
+    its = {}
+    for precond in (0, 1):
+        core = dcm.DynamicalCore(c.grid)
+        core.upload_state(c.state, c.dt, ptol=c.ptol, kord=c.kord, precision=1,
+                          precond=precond)
+        core.driver_start()
+        st = [core.step(1) for _ in range(3)]
+        assert all(s.err_last < c.ptol for s in st)
+        its[precond] = sum(s.iters_last for s in st)
+        core.close()
+    print("FP32 iterations over 3 steps", its)
+    assert its[1] < 0.85 * its[0], its
