@@ -23,7 +23,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIBPATH = os.path.join(HERE, "libdcm_b200.so")
 
 DCM_OK, DCM_E_NOCONV, DCM_E_BREAKDOWN, DCM_E_NONFINITE, DCM_E_CUDA = 0, 1, 2, 3, 4
-DCM_E_TIMEOUT, DCM_E_DECOMP, DCM_E_ARG, DCM_E_UNSUPPORTED = 5, 6, 7, 8
+DCM_E_TIMEOUT, DCM_E_DECOMP, DCM_E_ARG, DCM_E_UNSUPPORTED, DCM_E_IO = 5, 6, 7, 8, 9
 
 _dp = C.POINTER(C.c_double)
 
@@ -129,12 +129,19 @@ def library():
             "dcm_ensemble_member": [P, C.c_int, C.POINTER(C.c_void_p)],
             "dcm_ensemble_step": [P, C.c_int, C.POINTER(EnsembleStats)],
             "dcm_ensemble_last_error": [P],
+            "dcm_output_open": [P, C.c_char_p, _dp, _dp, _dp, _dp, C.c_int, C.c_char_p, C.c_int,
+                                C.POINTER(C.c_void_p)],
+            "dcm_output_write": [P, C.c_double],
+            "dcm_output_flush": [P],
+            "dcm_output_close": [P],
+            "dcm_output_last_error": [P],
         }
         for name, args in sig.items():
             f = getattr(lib, name)
             f.argtypes = args
             f.restype = C.c_char_p if name in ("dcm_status_string", "dcm_last_error",
-                                               "dcm_ensemble_last_error") else C.c_int
+                                               "dcm_ensemble_last_error",
+                                               "dcm_output_last_error") else C.c_int
         _lib = lib
     return _lib
 
@@ -149,7 +156,8 @@ EXPORTS = ("dcm_create", "dcm_destroy", "dcm_status_string", "dcm_last_error",
            "dcm_profile_read", "dcm_horizontal_means_noalloc", "dcm_solver_graphs", "dcm_tune",
            "dcm_set_launch_shape", "dcm_ensemble_create", "dcm_ensemble_destroy", "dcm_ensemble_member",
            "dcm_ensemble_step", "dcm_ensemble_last_error", "dcm_exchange_full_wo",
-           "dcm_calculate_subgrid_3d")
+           "dcm_calculate_subgrid_3d", "dcm_output_open", "dcm_output_write",
+           "dcm_output_flush", "dcm_output_close", "dcm_output_last_error")
 
 PROF_CLASSES = ("setup", "jacobi", "matvec", "update", "post", "means", "sources", "rhs",
                 "adv_ref", "mp_shift", "upwind", "antidiff", "beta", "limit", "restore",
@@ -510,6 +518,61 @@ def fortran_stack(fields):
     for q, a in enumerate(fields):
         out[q][...] = a
     return out
+
+
+class Output:
+    """The reference's output routine (driver_code.f90:725-1145) for a
+    DynamicalCore's resident state: a netCDF classic file written by
+    dcm_output_*.  write(time) appends one record of the current state and
+    returns at once; the record reaches the file while later steps run.
+    x, y, z are the grid coordinates with their halo (default: the grid's),
+    trefn the reference temperature profile (kp+2, default zeros), q_names
+    the nq tracer names (default q1, q2, ...)."""
+
+    def __init__(self, core, path, x=None, y=None, z=None, trefn=None, q_names=None, nprec=1):
+        self.lib = core.lib
+        g = core.grid
+        nq = getattr(core, "_nq", 0) or 0
+        keep = [np.ascontiguousarray(a if a is not None else b, dtype=np.float64)
+                for a, b in ((x, g.x), (y, g.y), (z, g.z))]
+        tref = None if trefn is None else np.ascontiguousarray(trefn, dtype=np.float64)
+        names = b""
+        if nq:
+            q_names = q_names or ["q%d" % (m + 1) for m in range(nq)]
+            names = b"".join(n.encode()[:20].ljust(20) for n in q_names)
+        self._keep = (keep, tref, names)
+        o = C.c_void_p()
+        st = self.lib.dcm_output_open(core.h, os.fsencode(path), *[_ptr(a) for a in keep],
+                                      _ptr(tref) if tref is not None else None, int(nq),
+                                      names if nq else None, int(nprec), C.byref(o))
+        if st:
+            raise DCMError(st, self.lib.dcm_status_string(st).decode())
+        self.o = o
+
+    def _check(self, st):
+        if st:
+            msg = self.lib.dcm_output_last_error(self.o)
+            raise DCMError(st, (msg or b"").decode() or
+                           self.lib.dcm_status_string(st).decode())
+
+    def write(self, time):
+        self._check(self.lib.dcm_output_write(self.o, float(time)))
+
+    def flush(self):
+        self._check(self.lib.dcm_output_flush(self.o))
+
+    def close(self):
+        if getattr(self, "o", None):
+            st = self.lib.dcm_output_close(self.o)
+            self.o = None
+            if st:
+                raise DCMError(st, self.lib.dcm_status_string(st).decode())
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Ensemble:

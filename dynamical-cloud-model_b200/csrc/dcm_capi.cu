@@ -319,6 +319,7 @@ extern "C" const char* dcm_status_string(int s) {
         case DCM_E_DECOMP: return "only a 1x1x1 process grid is supported";
         case DCM_E_ARG: return "invalid argument";
         case DCM_E_UNSUPPORTED: return "unsupported configuration";
+        case DCM_E_IO: return "output file error";
         default: return "unknown status";
     }
 }
@@ -1788,3 +1789,50 @@ extern "C" int dcm_ensemble_step(dcm_ensemble* e, int nsteps, dcm_ensemble_stats
     }
     return rc;
 }
+
+// =============================================================================
+// read-only view of the resident state for the output writer (dcm_output.cu)
+// =============================================================================
+namespace dcm {
+
+int resident_view(dcm_handle* h, ResidentView* out) {
+    if (!h || !out || !h->resident) return DCM_E_ARG;
+    int cu, cz, ct;
+    roles_of(h->nstep % 3, cu, cz, ct);
+    ResidentView& v = *out;
+    v.d = h->d;
+    v.prec = h->prec;
+    v.p = h->p;
+    v.div = h->div;
+    v.st = h->st;
+    v.device = h->device;
+    v.q.clear();
+    auto fill = [&](auto& S) {
+        v.u = S.U[cu];
+        v.v = S.V[cu];
+        v.w = S.W[cu];
+        v.th = S.th;
+        for (auto* q : S.q) v.q.push_back(q);
+    };
+    if (h->prec == 0)
+        fill(h->s64);
+    else
+        fill(h->s32);
+    return DCM_OK;
+}
+
+int host_profiles(dcm_handle* h, std::vector<double>* rhoa, std::vector<double>* thetan) {
+    if (!h || !rhoa || !thetan) return DCM_E_ARG;
+    const size_t K2 = h->d.kp + 2;
+    rhoa->assign(K2, 0.0);
+    thetan->assign(K2, 0.0);
+    if (cudaSetDevice(h->device) != cudaSuccess) return DCM_E_CUDA;
+    if (cudaMemcpy(rhoa->data(), h->mt.rhoa, K2 * sizeof(double), cudaMemcpyDeviceToHost) !=
+            cudaSuccess ||
+        cudaMemcpy(thetan->data(), h->mt.thetan, K2 * sizeof(double), cudaMemcpyDeviceToHost) !=
+            cudaSuccess)
+        return DCM_E_CUDA;
+    return DCM_OK;
+}
+
+}  // namespace dcm

@@ -1,6 +1,7 @@
 // dcm_internal.h -- device work areas and host-side entry points shared by
 // the kernel files and the C-ABI layer.
 #pragma once
+#include <vector>
 #include <cuda_runtime.h>
 
 #include <utility>
@@ -153,6 +154,21 @@ template <typename T>
 int upwind_run(MpdataWork<T>& w, const Dims& d, const Metrics<T>& mt, T dt,
                const T* u, const T* v, const T* wv, const T* psi_in,
                T* psi_out, int neumann, cudaStream_t st);
+
+// --- dcm_capi.cu: a read-only view of the resident state (output writer) ----
+struct ResidentView {
+    Dims d;              // pitched device layout
+    int prec = 0;        // 0: FP64 fields; 1: FP32 fields (p and div are FP64 in both)
+    const void *u = nullptr, *v = nullptr, *w = nullptr, *th = nullptr;  // current roles
+    const double *p = nullptr, *div = nullptr;
+    std::vector<const void*> q;  // nq fields when moisture is on
+    cudaStream_t st = nullptr;   // the handle's stream (orders the view after the step)
+    int device = 0;
+};
+// DCM_E_ARG when no state is resident
+int resident_view(dcm_handle* h, ResidentView* out);
+// host copies of the handle's rhoa and thetan (kp+2 each)
+int host_profiles(dcm_handle* h, std::vector<double>* rhoa, std::vector<double>* thetan);
 
 // --- k_dynamics.cu ---------------------------------------------------------
 enum HaloMode { HALO_FULL = 0, HALO_DIM = 1, HALO_WO = 2, HALO_FULL_WO = 3 };

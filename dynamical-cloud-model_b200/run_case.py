@@ -10,6 +10,8 @@ kelvin_helmholtz (128x1x64), or warm_bubble_IPxJPxKP /
 sheared_convection_IPxJPxKP for other sizes.  --host-loop drives the
 pressure solve from the host (the same kernels; a profiler sees every
 launch, which it cannot inside the graph-driven solve's conditional loop).
+--output FILE writes the reference's netCDF output before every
+--output-every steps and reports the host time of each write call.
 --precond 1 gives the mixed form Chebyshev-weighted sweeps on
 [--precond-lo, 2].  --viscous switches the Smagorinsky subgrid model on in
 sources (cvis 0.23,
@@ -20,6 +22,7 @@ import argparse
 import importlib.util
 import os
 import sys
+import time
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 
@@ -61,6 +64,9 @@ def main():
     ap.add_argument("--precond", type=int, default=0, choices=[0, 1])
     ap.add_argument("--precond-lo", type=float, default=0.05)
     ap.add_argument("--profile", action="store_true")
+    ap.add_argument("--output", default=None,
+                    help="netCDF file written before every --output-every steps")
+    ap.add_argument("--output-every", type=int, default=1)
     args = ap.parse_args()
     dcm = load()
     from dcm_b200 import cases
@@ -75,14 +81,26 @@ def main():
                       precision=args.precision, precond=args.precond,
                       precond_lo=args.precond_lo, **kw)
     core.driver_start()
+    out = dcm.Output(core, args.output) if args.output else None
+    t_write = []
     for s in range(args.steps):
         if args.profile and s == min(1, args.steps - 1):
             core.profile(True)  # after the first step (module loading, first-call set-up)
+        if out and s % args.output_every == 0:
+            t0 = time.perf_counter()
+            out.write(s * c.dt)
+            t_write.append((time.perf_counter() - t0) * 1e3)
         st = core.step(1)
         print("%s precision %d step %d: %d iterations (%d updates, %d restarts), "
               "err %.3e, %.2f ms" % (c.name, args.precision, s + 1, st.iters_last,
                                      st.updates_last, st.restarts_last, st.err_last,
                                      st.ms_total), flush=True)
+    if out:
+        t0 = time.perf_counter()
+        out.close()
+        print("output: %d records, host ms per write call %s, close (drain) %.1f ms" % (
+            len(t_write), " ".join("%.2f" % t for t in t_write),
+            (time.perf_counter() - t0) * 1e3), flush=True)
     if args.profile:
         for name, (ms, n) in core.profile_read().items():
             if n:

@@ -35,7 +35,8 @@ typedef enum {
     DCM_E_TIMEOUT = 5,     /* a bounded device wait expired                 */
     DCM_E_DECOMP = 6,      /* process grid is not 1 x 1 x 1                 */
     DCM_E_ARG = 7,         /* invalid argument                              */
-    DCM_E_UNSUPPORTED = 8  /* configuration outside the implemented path    */
+    DCM_E_UNSUPPORTED = 8, /* configuration outside the implemented path    */
+    DCM_E_IO = 9           /* writing an output file failed                 */
 } dcm_status;
 
 /* Grid description.  All arrays are host pointers, length n+2 (index 0..n+1),
@@ -253,6 +254,34 @@ int dcm_driver_start(dcm_handle *h);
 int dcm_step(dcm_handle *h, int nsteps, dcm_step_stats *stats);
 /* Download the state; velocities come back in their current roles. */
 int dcm_state_download(dcm_handle *h, dcm_fields *f);
+
+/* ---- output (driver_code.f90:725-1145) ---------------------------------- */
+/* The reference's output routine for the resident state: a netCDF classic
+ * file (CDF-1, CDF-2 when an offset needs 64 bits) with the reference's
+ * dimensions (times, ip, jp, kp [, nq, nprec, l_q_names]), variables
+ * (time, x, y, z, rhoa, thetan, trefn, th, u, v, w, p, div [, q_names, q,
+ * precip]), "units" attributes and FP32 values; q and precip have the q
+ * index fastest as the reference's reshape writes them.  precip (the
+ * microphysics' output) is written as zeros.
+ * dcm_output_open writes the header and the fixed variables: x (ip+2), y
+ * (jp+2), z (kp+2), trefn (kp+2, NULL: zeros) as the driver holds them,
+ * rhoa and thetan from the handle; nq must be the resident number of q
+ * fields (0 without moisture), q_names nq blank-padded names of 20 chars.
+ * dcm_output_write appends one record of the current state with the given
+ * time, as output() does at each output time: it queues a packing kernel on
+ * the handle's stream and returns; a copy stream and a writer thread put the
+ * record in the file while later dcm_step calls run (two records in flight;
+ * a third write waits for the first).  dcm_output_flush waits until every
+ * queued record is in the file; dcm_output_close flushes and closes.  Close
+ * the output before dcm_destroy or a new dcm_state_upload. */
+typedef struct dcm_output dcm_output;
+int dcm_output_open(dcm_handle *h, const char *path, const double *x,
+                    const double *y, const double *z, const double *trefn,
+                    int nq, const char *q_names, int nprec, dcm_output **out);
+int dcm_output_write(dcm_output *o, double time);
+int dcm_output_flush(dcm_output *o);
+int dcm_output_close(dcm_output *o);
+const char *dcm_output_last_error(const dcm_output *o);
 
 /* ---- horizontal means without device allocation ------------------------- */
 /* No counterpart in the reference.  Same per-level means as
