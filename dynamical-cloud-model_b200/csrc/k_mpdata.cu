@@ -12,6 +12,8 @@
 //   k_antidiff  antidiffusive pseudo-velocities (eqs 13/14/38, G = rho)
 //   k_beta      beta_up / beta_down (eqs 19/20)
 //   k_limit     limited velocities (eq 18)
+#include <algorithm>
+
 #include "dcm_internal.h"
 #include "dcm_prof.h"
 
@@ -93,10 +95,14 @@ __global__ void __launch_bounds__(256) k_upwind(Dims d, Metrics<T> mt, T dt,
     if (!FIRST && Mgate && Mgate->early) return;
     const int k = 1 + blockIdx.x * BX + threadIdx.x;
     const int j = 1 + blockIdx.y * BY + threadIdx.y;
-    const int i = 1 + blockIdx.z;
     const T m = FIRST || LAST ? (T)M->m : T(0);
     double acc[1] = {0.0};
     const bool in = k <= d.kp && j <= d.jp;
+    // the first pass also sums the shifted field (the early-return test):
+    // its blocks stride over the i-planes, so that a few thousand blocks,
+    // not one per plane, publish reduction partials
+    const int istep = FIRST ? (int)gridDim.z : d.ip;
+    for (int i = 1 + blockIdx.z; i <= d.ip; i += istep)
     if (in) {
         auto P = [&](int kk, int jj, int ii) -> T {
             const T x = src[d.at(kk, jj, ii)];
@@ -125,7 +131,7 @@ __global__ void __launch_bounds__(256) k_upwind(Dims d, Metrics<T> mt, T dt,
             if (k == d.kp) fzr = -fzl;
         }
         const T nv = pc - (fxr - fxl) - (fyr - fyl) - (fzr - fzl);  // :115
-        if (FIRST) acc[0] = (double)pc;
+        if (FIRST) acc[0] += (double)pc;
         if (LAST) {
             const T lb = (T)M->lbc + m, ub = (T)M->ubc + m;
             if (exch == 0) {
@@ -444,20 +450,21 @@ int mpdata_run(MpdataWork<T>& w, const Dims& d, const Metrics<T>& mt, T dt,
         return cudaGetLastError() == cudaSuccess ? 0 : DCM_E_CUDA;
     }
     const Vel<T> V0{u, v, wv};
+    const dim3 gfirst(g.x, g.y, std::min(g.z, 16u));  // blocks stride over i
     // it = 1: donor cell of the shifted input (:684)
     for (int q = 0; q < nq; q++) {
         const T* sa = sadd ? sadd[q] : nullptr;
         if (kord == 1)
             { ProfScope ps_(P_UPWIND, st);
-            k_upwind<T, true, true><<<g, b, 0, st>>>(d, mt, dt, V0, psi_in[q], psi_out[q], neumann,
-                                                     1, sa, dt_add, w.partials, w.ticket, w.M + q,
-                                                     nullptr);
+            k_upwind<T, true, true><<<gfirst, b, 0, st>>>(d, mt, dt, V0, psi_in[q], psi_out[q],
+                                                          neumann, 1, sa, dt_add, w.partials,
+                                                          w.ticket, w.M + q, nullptr);
             }
         else
             { ProfScope ps_(P_UPWIND, st);
-            k_upwind<T, true, false><<<g, b, 0, st>>>(d, mt, dt, V0, psi_in[q], w.pa[q], neumann,
-                                                      1, nullptr, T(0), w.partials, w.ticket,
-                                                      w.M + q, nullptr);
+            k_upwind<T, true, false><<<gfirst, b, 0, st>>>(d, mt, dt, V0, psi_in[q], w.pa[q],
+                                                           neumann, 1, nullptr, T(0), w.partials,
+                                                           w.ticket, w.M + q, nullptr);
             }
     }
     // velocity sets: A receives antidiffusive velocities, L limited ones

@@ -21,18 +21,30 @@ def _members():
                               seed=10 + n) for n, (ip, jp, kp, amp) in enumerate(SIZES)]
 
 
-def _upload(core, c, precision):
+def _upload(core, c, precision, **kw):
     core.upload_state(c.state, c.dt, ptol=c.ptol, kord=c.kord, monotone=c.monotone,
-                      precision=precision)
+                      precision=precision, **kw)
     core.driver_start()
 
 
-@pytest.mark.parametrize("precision", [0, 1])
-def test_ensemble_matches_standalone(dcm, precision):
+def _options(c, opts):
+    kw = {}
+    if "cheb" in opts:
+        kw.update(precond=1, precond_lo=0.05)
+    if "viscous" in opts:
+        kw["viscous"] = dict(lamsq=cases.mixing_length_sq(c.grid, 0.23, 0.1), z0=0.1, z0th=0.1)
+    return kw
+
+
+@pytest.mark.parametrize("precision,opts", [(0, ()), (1, ()), (1, ("cheb",)),
+                                            (0, ("viscous",)), (1, ("cheb", "viscous"))])
+def test_ensemble_matches_standalone(dcm, precision, opts):
+    """Also with the Chebyshev-weighted sweeps and with the subgrid model in
+    the captured step."""
     cs = _members()
     ens = dcm.Ensemble([c.grid for c in cs])
     for core, c in zip(ens.members, cs):
-        _upload(core, c, precision)
+        _upload(core, c, precision, **_options(c, opts))
     its_e = []
     for _ in range(4):
         st = ens.step(1)
@@ -42,7 +54,7 @@ def test_ensemble_matches_standalone(dcm, precision):
     ens.close()
     for n, c in enumerate(cs):
         core = dcm.DynamicalCore(c.grid)
-        _upload(core, c, precision)
+        _upload(core, c, precision, **_options(c, opts))
         its = [core.step(1).iters_last for _ in range(4)]
         ref = core.download_state()
         core.close()
