@@ -327,7 +327,9 @@ def run_b200(args, rank, world, local_rank, dist):
     #      after args.accuracy_steps
     acc = {}
     if args.accuracy_steps:
-        cores = [core, pkg.DynamicalCore(g, device=local_rank)]
+        # the FP64 run on a second handle, the mixed one on this handle, which
+        # the end-to-end leg below uses next with the same layout
+        cores = [pkg.DynamicalCore(g, device=local_rank), core]
         for prec, c in zip((0, 1), cores):
             c.upload_state(case.state, case.dt, precision=prec, **kw,
                            **(PRECOND if prec == 1 else {}))
@@ -338,7 +340,7 @@ def run_b200(args, rank, world, local_rank, dist):
                 c.step(n - done)
             done = n
             acc[str(n)] = field_errors(g, cores[0].download_state(), cores[1].download_state())
-        cores[1].close()
+        cores[0].close()
 
     # ---- end to end through the C-ABI with host buffers (pinned), mixed form
     host = {n: pinned_like(getattr(case.state, n)) for n in
@@ -355,7 +357,9 @@ def run_b200(args, rank, world, local_rank, dist):
     t0 = time.perf_counter()
     core.upload_state(st_host, case.dt, precision=1, **kw, **PRECOND)
     core.driver_start()
+    tu = time.perf_counter()
     core.step(args.steps)
+    ts = time.perf_counter()
     out = core.download_state(out=outbufs)
     t1 = time.perf_counter()
     barrier()
@@ -365,8 +369,11 @@ def run_b200(args, rank, world, local_rank, dist):
     d2h = sum(a.nbytes for a in out.values() if isinstance(a, np.ndarray))
     e2e = {"value": world * N * args.steps / e2e_s, "unit": "grid-pt-steps/s",
            "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
+           "host_ms": {"upload": (tu - t0) * 1e3, "steps": (ts - tu) * 1e3,
+                       "download": (t1 - ts) * 1e3},
            "note": "mixed form: upload of the FP64 host state, K steps, download of the "
-                   "state, per K-step call"}
+                   "state, per K-step call, on a handle whose device buffers an earlier "
+                   "upload of the same layout allocated"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:

@@ -41,6 +41,7 @@ struct State {
     // the six stresses (scratch of each step)
     T *vism = nullptr, *vist = nullptr, *strain = nullptr, *lamsq = nullptr;
     T* tau[6]{};
+    double* lamsq64 = nullptr;
 };
 
 }  // namespace
@@ -77,6 +78,7 @@ struct dcm_handle {
     // named full-size scratch buffers
     std::vector<double*> slots;
     double* sg_lamsq = nullptr;  // lamsq of dcm_calculate_subgrid_3d (kp+2)
+    double* dense_stage = nullptr;  // one field in the host layout (uploads)
     int first_call = 1;  // bicgstab_first, dynamics.f90:17
 
     // FP32 copies for the mixed-precision form
@@ -183,16 +185,27 @@ enum {
 
 // n = 0: a whole field, dense host columns of kp+2 into pitched device
 // columns of K (one 2-D copy); n > 0: n contiguous elements (1-D profiles).
+// A whole field goes as one contiguous copy into a dense staging buffer and is
+// re-pitched (and converted to TO) on the device: a pitched 2-D host-to-device
+// copy of 1 KB rows ran at a sixth of the rate of the contiguous one.  The
+// stream orders the next field's copy into the stage after this kernel.
+template <typename TO>
+int upload_field(dcm_handle* h, TO* dst, const double* src) {
+    if (!src) return DCM_OK;
+    if (!h->dense_stage) CK(cudaMalloc(&h->dense_stage, h->nh * sizeof(double)));
+    CK(cudaMemcpyAsync(h->dense_stage, src, h->nh * sizeof(double), cudaMemcpyHostToDevice,
+                       h->st));
+    launch_repitch<TO>(h->hd, h->d, dst, h->dense_stage, h->st);
+    return DCM_OK;
+}
+
 int upload(dcm_handle* h, double* dst, const double* src, size_t n = 0) {
     if (!src) return DCM_OK;
     if (n) {
         CK(cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyHostToDevice, h->st));
         return DCM_OK;
     }
-    const size_t w = (size_t)h->hd.K * sizeof(double);
-    CK(cudaMemcpy2DAsync(dst, (size_t)h->d.K * sizeof(double), src, w, w,
-                         (size_t)h->d.J * h->d.I, cudaMemcpyHostToDevice, h->st));
-    return DCM_OK;
+    return upload_field<double>(h, dst, src);
 }
 int download(dcm_handle* h, double* dst, const double* src, size_t n = 0) {
     if (!dst) return DCM_OK;
@@ -466,6 +479,7 @@ extern "C" int dcm_destroy(dcm_handle* h) {
     for (float* p : h->fslots) free_field(p);
     cudaFree(h->metric_block_f);
     cudaFree(h->sg_lamsq);
+    cudaFree(h->dense_stage);
     cudaFree(h->S2);
     cudaFreeHost(h->hS2);
     cudaFree(h->forcing_f);
@@ -1172,18 +1186,11 @@ int one_step(dcm_handle* h) {
     return DCM_OK;
 }
 
-// host double field -> device field of precision T (via an FP64 staging slot;
-// the stream orders the next field's copy into the slot after this
-// conversion, and the caller synchronises once at the end)
+// host double field -> device field of precision T (through the dense
+// staging buffer; the caller synchronises once at the end)
 template <typename T>
 int put_field(dcm_handle* h, T* dst, const double* src) {
-    if (!src) return DCM_OK;
-    if constexpr (std::is_same<T, double>::value) return upload(h, dst, src);
-    double* stage = slot(h, S_STAGE);
-    NEED(stage);
-    RC(upload(h, stage, src));
-    launch_convert<T, double>(h->n, dst, stage, h->st);
-    return DCM_OK;
+    return upload_field<T>(h, dst, src);
 }
 template <typename T>
 int get_field(dcm_handle* h, double* dst, const T* src, size_t n = 0) {
@@ -1198,6 +1205,21 @@ int get_field(dcm_handle* h, double* dst, const T* src, size_t n = 0) {
     return DCM_OK;
 }
 
+// A resident buffer of an earlier upload with the same layout is zeroed and
+// kept (the state it then holds is the one a fresh allocation would give);
+// otherwise a new zeroed buffer.  Keeping the buffers keeps the pointers that
+// the captured pressure solves were built on.
+template <typename U>
+bool reuse_or_alloc(dcm_handle* h, U*& ptr, size_t n = 0) {
+    if (ptr) {
+        U* raw = n ? ptr : ptr - FIELD_SHIFT;
+        return cudaMemsetAsync(raw, 0, (n ? n : h->n + FIELD_PAD) * sizeof(U), h->st) ==
+               cudaSuccess;
+    }
+    ptr = alloc_owned<U>(h, n);
+    return ptr != nullptr;
+}
+
 template <typename T>
 int upload_state_t(dcm_handle* h, const dcm_fields* f, const double* lamsq_host) {
     State<T>& S = state_of<T>(h);
@@ -1208,15 +1230,12 @@ int upload_state_t(dcm_handle* h, const dcm_fields* f, const double* lamsq_host)
                    &S.V[2], &S.W[0], &S.W[1], &S.W[2]};
     for (int c = 0; c < 9; c++) {
         if (!in3[c]) return fail(h, DCM_E_ARG, "state_upload: missing velocity");
-        *dst3[c] = alloc_owned<T>(h);
-        NEED(*dst3[c]);
+        if (!reuse_or_alloc(h, *dst3[c])) return fail(h, DCM_E_CUDA, "device allocation failed");
         RC(put_field<T>(h, *dst3[c], in3[c]));
     }
     T** fl[6] = {&S.th, &S.th2, &S.su, &S.sv, &S.sw, &S.sth};
-    for (auto pp : fl) {
-        *pp = alloc_owned<T>(h);
-        NEED(*pp);
-    }
+    for (auto pp : fl)
+        if (!reuse_or_alloc(h, *pp)) return fail(h, DCM_E_CUDA, "device allocation failed");
     if (!f->th || !f->p) return fail(h, DCM_E_ARG, "state_upload: missing th or p");
     const double* src[5] = {f->th, f->su, f->sv, f->sw, f->sth};
     T* dst[5] = {S.th, S.su, S.sv, S.sw, S.sth};
@@ -1224,19 +1243,18 @@ int upload_state_t(dcm_handle* h, const dcm_fields* f, const double* lamsq_host)
         RC(put_field<T>(h, dst[c], src[c]));
     }
     const size_t K2 = h->d.kp + 2;
-    S.means = alloc_owned<T>(h, (4 + nqq) * K2);
-    NEED(S.means);
+    if (!reuse_or_alloc(h, S.means, (4 + nqq) * K2))
+        return fail(h, DCM_E_CUDA, "device allocation failed");
+    S.q.resize(nqq, nullptr);
+    S.sq.resize(nqq, nullptr);
+    S.qtmp.resize(nqq, nullptr);
     for (int c = 0; c < nqq; c++) {
-        T* a = alloc_owned<T>(h);
-        T* sq = alloc_owned<T>(h);
-        T* t = alloc_owned<T>(h);
-        NEED(a); NEED(sq); NEED(t);
-        RC(put_field<T>(h, a, f->q + (size_t)c * h->nh));
-        // sq is zeroed by the driver each step (:342) and nothing in the dry
-        // step writes it, so it stays zero
-        S.q.push_back(a);
-        S.sq.push_back(sq);
-        S.qtmp.push_back(t);
+        if (!reuse_or_alloc(h, S.q[c]) || !reuse_or_alloc(h, S.sq[c]) ||
+            !reuse_or_alloc(h, S.qtmp[c]))
+            return fail(h, DCM_E_CUDA, "device allocation failed");
+        // sq is zeroed by the driver each step (:342); without the subgrid
+        // model nothing in the dry step writes it, so it stays zero
+        RC(put_field<T>(h, S.q[c], f->q + (size_t)c * h->nh));
     }
     if constexpr (std::is_same<T, float>::value) {
         launch_convert<float, double>(5 * K2, h->forcing_f, h->forcing_dev, h->st);
@@ -1246,13 +1264,11 @@ int upload_state_t(dcm_handle* h, const dcm_fields* f, const double* lamsq_host)
         // (their previous values are never read); lamsq in the field precision
         T** sg[9] = {&S.vism, &S.vist, &S.strain, &S.tau[0], &S.tau[1],
                      &S.tau[2], &S.tau[3], &S.tau[4], &S.tau[5]};
-        for (auto pp : sg) {
-            *pp = alloc_owned<T>(h);
-            NEED(*pp);
-        }
-        S.lamsq = alloc_owned<T>(h, K2);
-        double* l64 = alloc_owned<double>(h, K2);
-        NEED(S.lamsq); NEED(l64);
+        for (auto pp : sg)
+            if (!reuse_or_alloc(h, *pp)) return fail(h, DCM_E_CUDA, "device allocation failed");
+        if (!reuse_or_alloc(h, S.lamsq, K2) || !reuse_or_alloc(h, S.lamsq64, K2))
+            return fail(h, DCM_E_CUDA, "device allocation failed");
+        double* l64 = S.lamsq64;
         RC(upload(h, l64, lamsq_host, K2));
         if constexpr (std::is_same<T, float>::value)
             launch_convert<float, double>(K2, S.lamsq, l64, h->st);
@@ -1321,7 +1337,14 @@ extern "C" int dcm_state_upload(dcm_handle* h, const dcm_config* cfg, const dcm_
         return fail(h, DCM_E_ARG, "state_upload: viscous needs lamsq, z0 > 0 and z0th > 0");
     if (cfg->viscous && h->h_zg.size() < 2)
         return fail(h, DCM_E_ARG, "state_upload: viscous needs the grid's zg (z(1))");
-    free_state(h);
+    // buffers of the resident state are kept when the layout is the same
+    // (no cudaFree, which synchronises the device; the captured solves stay
+    // valid); a changed layout frees them
+    const bool same_layout = h->resident && h->prec == cfg->precision &&
+                             (h->cfg.moisture ? h->cfg.nq : 0) ==
+                                 (cfg->moisture ? cfg->nq : 0) &&
+                             (h->cfg.viscous != 0) == (cfg->viscous != 0);
+    if (!same_layout) free_state(h);
     h->cfg = *cfg;
     h->cfg.lamsq = nullptr;  // copied to the device below; no host pointer is kept
     h->prec = cfg->precision;
@@ -1339,10 +1362,8 @@ extern "C" int dcm_state_upload(dcm_handle* h, const dcm_config* cfg, const dcm_
     forcing_of(h, &cfg->forcing, h->forcing_dev, &rc);
     if (rc != DCM_OK) return fail(h, rc, "state_upload: forcing arrays");
     h->nstep = 0;
-    h->p = alloc_owned<double>(h);
-    h->div = alloc_owned<double>(h);
-    h->psrc = alloc_owned<double>(h);
-    NEED(h->p); NEED(h->div); NEED(h->psrc);
+    if (!reuse_or_alloc(h, h->p) || !reuse_or_alloc(h, h->div) || !reuse_or_alloc(h, h->psrc))
+        return fail(h, DCM_E_CUDA, "device allocation failed");
     RC(upload(h, h->p, f->p));
     RC(upload(h, h->div, f->div));
     RC(upload(h, h->psrc, f->psrc));

@@ -282,6 +282,9 @@ void launch_advance_scalar(const Dims& d, T dt, T* a, const T* s,
 // element-wise precision conversion of n values
 template <typename TO, typename FROM>
 void launch_convert(size_t n, TO* to, const FROM* from, cudaStream_t st);
+// dense host-layout field (hd) -> pitched device field (d), converted to TO
+template <typename TO>
+void launch_repitch(const Dims& hd, const Dims& d, TO* dst, const double* src, cudaStream_t st);
 
 // psi (+/-) psi_1d(k) over the whole array (mpdata_3d_add :175-188)
 template <typename T>

@@ -5,6 +5,8 @@
 // (dynamics.f90:1019-1099, driver_code.f90:592-674), adv_ref_state
 // (pamm/sfvt/advection_3d.F90:1148-1218), advance_scalar_fields_3d
 // (sgm/subgrid_3d.f90:582-624) and the stand-alone halo exchanges.
+#include <algorithm>
+
 #include "dcm_internal.h"
 #include "dcm_prof.h"
 
@@ -527,5 +529,31 @@ void launch_convert(size_t n, TO* to, const FROM* from, cudaStream_t st) {
 }
 template void launch_convert<float, double>(size_t, float*, const double*, cudaStream_t);
 template void launch_convert<double, float>(size_t, double*, const float*, cudaStream_t);
+
+// dense host-layout columns (hd.K = kp+2 levels) -> pitched device columns
+// (d.K levels), converting to TO: one warp per column, lanes along k
+template <typename TO>
+__global__ void __launch_bounds__(256) k_repitch(Dims hd, Dims d, TO* __restrict__ dst,
+                                                 const double* __restrict__ src) {
+    const int lane = threadIdx.x & 31;
+    const size_t ncol = (size_t)hd.J * hd.I;
+    const size_t w0 = (blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5;
+    const size_t nw = (gridDim.x * (size_t)blockDim.x) >> 5;
+    for (size_t col = w0; col < ncol; col += nw) {
+        const double* __restrict__ s = src + col * hd.K;
+        TO* __restrict__ t = dst + col * d.K;
+        for (int k = lane; k < hd.K; k += 32) t[k] = (TO)s[k];
+    }
+}
+template <typename TO>
+void launch_repitch(const Dims& hd, const Dims& d, TO* dst, const double* src, cudaStream_t st) {
+    const size_t ncol = (size_t)hd.J * hd.I;
+    const unsigned nb = (unsigned)std::min<size_t>((ncol + 7) / 8, 148 * 32);
+    k_repitch<TO><<<nb, 256, 0, st>>>(hd, d, dst, src);
+}
+template void launch_repitch<double>(const Dims&, const Dims&, double*, const double*,
+                                     cudaStream_t);
+template void launch_repitch<float>(const Dims&, const Dims&, float*, const double*,
+                                    cudaStream_t);
 
 }  // namespace dcm

@@ -130,3 +130,38 @@ def test_ragged_shapes_mixed(dcm, orc, shape):
     for n in ("u", "v", "w", "th"):
         assert relerr(got[n], ref[n]) <= 1e-5, n
     assert relerr(got["p"], ref["p"], live_mask_p(c.grid)) <= 1e-5
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_reupload_with_the_same_layout(dcm, precision):
+    """A second dcm_state_upload of the same layout keeps the device buffers
+    (zeroed) and the captured solves: the steps that follow are bit-identical
+    to those of a fresh handle, after a first run that left every buffer
+    dirty; a layout change (moisture on) still works."""
+    c1 = cases.sheared_convection(ip=16, jp=12, kp=12, ntracers=2, seed=5)
+    c2 = cases.sheared_convection(ip=16, jp=12, kp=12, ntracers=2, seed=6)
+    kw = dict(nq=2, c_s=c1.c_s, c_e=c1.c_e, precision=precision)
+    core = dcm.DynamicalCore(c1.grid)
+    core.upload_state(c1.state, c1.dt, ptol=c1.ptol, kord=c1.kord, **kw)
+    core.driver_start()
+    core.step(3)
+    core.upload_state(c2.state, c2.dt, ptol=c2.ptol, kord=c2.kord, **kw)
+    core.driver_start()
+    its = [core.step(1).iters_last for _ in range(3)]
+    got = core.download_state()
+    fresh = dcm.DynamicalCore(c2.grid)
+    fresh.upload_state(c2.state, c2.dt, ptol=c2.ptol, kord=c2.kord, **kw)
+    fresh.driver_start()
+    its_f = [fresh.step(1).iters_last for _ in range(3)]
+    ref = fresh.download_state()
+    fresh.close()
+    assert its == its_f
+    for n in ("u", "v", "w", "th", "p", "su", "sth", "psrc", "div"):
+        assert np.array_equal(got[n], ref[n]), n
+    for q in range(2):
+        assert np.array_equal(got["q"][q], ref["q"][q]), q
+    # another layout on the same handle: no tracers
+    core.upload_state(c2.state, c2.dt, ptol=c2.ptol, kord=c2.kord, precision=precision)
+    core.driver_start()
+    assert core.step(2).err_last < c2.ptol
+    core.close()
