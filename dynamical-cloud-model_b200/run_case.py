@@ -63,6 +63,8 @@ def main():
     ap.add_argument("--viscous", action="store_true")
     ap.add_argument("--precond", type=int, default=0, choices=[0, 1])
     ap.add_argument("--precond-lo", type=float, default=0.05)
+    ap.add_argument("--fuse", type=int, default=None, choices=[0, 1],
+                    help="FP32 preconditioner: separate sweeps (0) or the fused kernel (1)")
     ap.add_argument("--profile", action="store_true")
     ap.add_argument("--output", default=None,
                     help="netCDF file written before every --output-every steps")
@@ -74,6 +76,8 @@ def main():
     core = dcm.DynamicalCore(c.grid, device=args.device)
     if args.host_loop:
         core.solver_graphs(False)
+    if args.fuse is not None:
+        core.set_launch_shape(1, fuse=args.fuse)
     kw = dict(nq=c.nq, c_s=c.c_s, c_e=c.c_e) if c.nq else {}
     if args.viscous:
         kw["viscous"] = dict(lamsq=cases.mixing_length_sq(c.grid, 0.23, 0.1), z0=0.1, z0th=0.1)
