@@ -110,6 +110,14 @@ __device__ __forceinline__ T s0val(const T* __restrict__ rh, const T* __restrict
 // blockIdx.z -> i.  k neighbours come from the adjacent lanes by shuffle
 // (Neumann mirror at k = 1 and kp, dynamics.f90:206-211), j and i
 // neighbours (periodic) through L1/L2.
+// (A x)/a_p of a Jacobi sweep.  FP32 (the mixed form's preconditioner):
+// the two-instruction approximate divide (within 2 ulp, as the full-range
+// sequence that -prec-div=false gives, for |a_p| in [2^-126, 2^126], which
+// any grid spacing between 1e-19 m and 1e19 m keeps); FP64: the correctly
+// rounded divide of the reference's arithmetic.
+__device__ __forceinline__ float sweep_div(float a, float b) { return __fdividef(a, b); }
+__device__ __forceinline__ double sweep_div(double a, double b) { return a / b; }
+
 // One Chebyshev-weighted sweep at a point, with every rounding explicit so
 // that the fused and the separate sweeps agree bit for bit:
 //     res = sc x + w (s0 - sc (A x)/a_p),   q = (A x)/a_p
@@ -381,10 +389,10 @@ __device__ __forceinline__ void sten_task(const StenCtx<T, OP, MODE>& C, int kc,
         if (C.cheb) {
 #pragma unroll
             for (int q = 0; q < V; q++)
-                res[q] = cheb_update(xc[q], s0[q], Ax[q] / ap[q], C.wx, C.ws);
+                res[q] = cheb_update(xc[q], s0[q], sweep_div(Ax[q], ap[q]), C.wx, C.ws);
         } else {
 #pragma unroll
-            for (int q = 0; q < V; q++) res[q] = xc[q] + s0[q] - Ax[q] / ap[q];
+            for (int q = 0; q < V; q++) res[q] = xc[q] + s0[q] - sweep_div(Ax[q], ap[q]);
         }
         if (OP == OP_SW3P) {
             T pold[V];
@@ -653,7 +661,8 @@ __global__ void __launch_bounds__(PW * 32, 1)
             const float c0 = xc[e];
             const float Ax = aw * (xm[e] - c0) + ae * (xp[e] - c0) + as * (xs[e] - c0) +
                              an * (xn[e] - c0) + ad[e] * (xd - c0) + au[e] * (xu - c0);
-            res[e] = CHEB ? cheb_update(xc[e], s0c[e], Ax / ap, sc, wv) : xc[e] + s0c[e] - Ax / ap;
+            const float q = sweep_div(Ax, ap);
+            res[e] = CHEB ? cheb_update(xc[e], s0c[e], q, sc, wv) : xc[e] + s0c[e] - q;
         }
     };
     float R0[4][4], R1[3][4], R2[3][4];  // s0 at b..b+3, s1 at b..b+2, s2 at b-1..b+1
