@@ -63,6 +63,8 @@ def main():
     ap.add_argument("--viscous", action="store_true")
     ap.add_argument("--precond", type=int, default=0, choices=[0, 1])
     ap.add_argument("--precond-lo", type=float, default=0.05)
+    ap.add_argument("--inner-tol", type=float, default=0.1,
+                    help="mixed form: the reliable-update factor")
     ap.add_argument("--fuse", type=int, default=None, choices=[0, 1],
                     help="FP32 preconditioner: separate sweeps (0) or the fused kernel (1)")
     ap.add_argument("--profile", action="store_true")
@@ -83,7 +85,7 @@ def main():
         kw["viscous"] = dict(lamsq=cases.mixing_length_sq(c.grid, 0.23, 0.1), z0=0.1, z0th=0.1)
     core.upload_state(c.state, c.dt, ptol=c.ptol, kord=c.kord, monotone=c.monotone,
                       precision=args.precision, precond=args.precond,
-                      precond_lo=args.precond_lo, **kw)
+                      precond_lo=args.precond_lo, inner_tol=args.inner_tol, **kw)
     core.driver_start()
     out = dcm.Output(core, args.output) if args.output else None
     t_write = []
