@@ -181,6 +181,14 @@ __global__ void __launch_bounds__(256) k_upwind(Dims d, Metrics<T> mt, T dt,
 }
 
 // ---- antidiffusive velocities (:320-505) ------------------------------------
+// Quotients of the antidiffusive velocities: FP64 (the parity path) the
+// correctly rounded divide; FP32 (the mixed form, whose fields carry 1e-7)
+// the two-instruction approximate divide, within 2 ulp for divisors of
+// magnitude 2^-126..2^126 (the denominators here are grid spacings, densities
+// and sums of shifted, non-negative psi plus 1e-30)
+__device__ __forceinline__ double adiv(double a, double b) { return a / b; }
+__device__ __forceinline__ float adiv(float a, float b) { return __fdividef(a, b); }
+
 template <typename T>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_antidiff(Dims d, Metrics<T> mt, T dt,
                                                   Vel<T> Vt,
@@ -209,68 +217,77 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_antidiff(Dims d
     const T g_bar1 = rn, g_bar2 = rn;
     const T g_bar3 = h * (rn + rnp);
 
-    const T u_div1 = (ra * (W(k, j, i) + W(k, j, i + 1)) - ram * (W(k - 1, j, i) + W(k - 1, j, i + 1))) /
-                         (dzm * g_bar1) +
-                     (rn * (V(k, j, i) + V(k, j, i + 1) - V(k, j - 1, i) - V(k, j - 1, i + 1))) /
-                         (dym * g_bar1);
-    const T u_div2 = (ra * (W(k, j, i) + W(k, j + 1, i)) - ram * (W(k - 1, j, i) + W(k - 1, j + 1, i))) /
-                         (dzm * g_bar2) +
-                     (rn * (U(k, j, i) + U(k, j + 1, i) - U(k, j, i - 1) - U(k, j + 1, i - 1))) /
-                         (dxm * g_bar2);
-    const T u_div3 = (rn * (U(k, j, i) - U(k, j, i - 1)) + rnp * (U(k + 1, j, i) - U(k + 1, j, i - 1))) /
-                         (dxm * g_bar3) +
-                     (rn * (V(k, j, i) - V(k, j - 1, i)) + rnp * (V(k + 1, j, i) - V(k + 1, j - 1, i))) /
-                         (dym * g_bar3);
+    // every quotient through adiv: FP64 divides exactly as written (the
+    // reference's arithmetic), FP32 with the approximate divide
+    const T u_div1 = adiv(ra * (W(k, j, i) + W(k, j, i + 1)) - ram * (W(k - 1, j, i) + W(k - 1, j, i + 1)),
+                          dzm * g_bar1) +
+                     adiv(rn * (V(k, j, i) + V(k, j, i + 1) - V(k, j - 1, i) - V(k, j - 1, i + 1)),
+                          dym * g_bar1);
+    const T u_div2 = adiv(ra * (W(k, j, i) + W(k, j + 1, i)) - ram * (W(k - 1, j, i) + W(k - 1, j + 1, i)),
+                          dzm * g_bar2) +
+                     adiv(rn * (U(k, j, i) + U(k, j + 1, i) - U(k, j, i - 1) - U(k, j + 1, i - 1)),
+                          dxm * g_bar2);
+    const T u_div3 = adiv(rn * (U(k, j, i) - U(k, j, i - 1)) + rnp * (U(k + 1, j, i) - U(k + 1, j, i - 1)),
+                          dxm * g_bar3) +
+                     adiv(rn * (V(k, j, i) - V(k, j - 1, i)) + rnp * (V(k + 1, j, i) - V(k + 1, j - 1, i)),
+                          dym * g_bar3);
 
     const T uc = U(k, j, i), vc = V(k, j, i), wc = W(k, j, i);
+    // q4 * A / g * B / C / E, evaluated left to right as the reference does
+    auto term = [&](T A, T g, T B, T Cd, T E) { return adiv(adiv(adiv(q4 * A, g) * B, Cd), E); };
     const T u_j_bar1 =
         h * dt * uc *
-        (q4 * (ra * W(k, j, i + 1) + ra * W(k, j, i) + ram * W(k - 1, j, i + 1) + ram * W(k - 1, j, i)) /
-             g_bar1 *
-             (P(k + 1, j, i + 1) + P(k + 1, j, i) - P(k - 1, j, i + 1) - P(k - 1, j, i)) /
-             (P(k + 1, j, i + 1) + P(k + 1, j, i) + P(k - 1, j, i + 1) + P(k - 1, j, i) + small) /
-             (h * (dznm + dzn)) +
-         q4 * (rn * V(k, j, i + 1) + rn * V(k, j, i) + rn * V(k, j - 1, i + 1) + rn * V(k, j - 1, i)) /
-             g_bar1 *
-             (P(k, j + 1, i + 1) + P(k, j + 1, i) - P(k, j - 1, i + 1) - P(k, j - 1, i)) /
-             (P(k, j + 1, i + 1) + P(k, j + 1, i) + P(k, j - 1, i + 1) + P(k, j - 1, i) + small) /
-             (h * (dynm + dyn)));
+        (term(ra * W(k, j, i + 1) + ra * W(k, j, i) + ram * W(k - 1, j, i + 1) + ram * W(k - 1, j, i),
+              g_bar1,
+              P(k + 1, j, i + 1) + P(k + 1, j, i) - P(k - 1, j, i + 1) - P(k - 1, j, i),
+              P(k + 1, j, i + 1) + P(k + 1, j, i) + P(k - 1, j, i + 1) + P(k - 1, j, i) + small,
+              h * (dznm + dzn)) +
+         term(rn * V(k, j, i + 1) + rn * V(k, j, i) + rn * V(k, j - 1, i + 1) + rn * V(k, j - 1, i),
+              g_bar1,
+              P(k, j + 1, i + 1) + P(k, j + 1, i) - P(k, j - 1, i + 1) - P(k, j - 1, i),
+              P(k, j + 1, i + 1) + P(k, j + 1, i) + P(k, j - 1, i + 1) + P(k, j - 1, i) + small,
+              h * (dynm + dyn)));
     const T u_j_bar2 =
         h * dt * vc *
-        (q4 * (ra * W(k, j + 1, i) + ra * W(k, j, i) + ram * W(k - 1, j + 1, i) + ram * W(k - 1, j, i)) /
-             g_bar2 *
-             (P(k + 1, j + 1, i) + P(k + 1, j, i) - P(k - 1, j + 1, i) - P(k - 1, j, i)) /
-             (P(k + 1, j + 1, i) + P(k + 1, j, i) + P(k - 1, j + 1, i) + P(k - 1, j, i) + small) /
-             (h * (dznm + dzn)) +
-         q4 * (rn * U(k, j + 1, i) + rn * U(k, j, i) + rn * U(k, j + 1, i - 1) + rn * U(k, j, i - 1)) /
-             g_bar2 *
-             (P(k, j + 1, i + 1) + P(k, j, i + 1) - P(k, j + 1, i - 1) - P(k, j, i - 1)) /
-             (P(k, j + 1, i + 1) + P(k, j, i + 1) + P(k, j + 1, i - 1) + P(k, j, i - 1) + small) /
-             (h * (dxnm + dxn)));
+        (term(ra * W(k, j + 1, i) + ra * W(k, j, i) + ram * W(k - 1, j + 1, i) + ram * W(k - 1, j, i),
+              g_bar2,
+              P(k + 1, j + 1, i) + P(k + 1, j, i) - P(k - 1, j + 1, i) - P(k - 1, j, i),
+              P(k + 1, j + 1, i) + P(k + 1, j, i) + P(k - 1, j + 1, i) + P(k - 1, j, i) + small,
+              h * (dznm + dzn)) +
+         term(rn * U(k, j + 1, i) + rn * U(k, j, i) + rn * U(k, j + 1, i - 1) + rn * U(k, j, i - 1),
+              g_bar2,
+              P(k, j + 1, i + 1) + P(k, j, i + 1) - P(k, j + 1, i - 1) - P(k, j, i - 1),
+              P(k, j + 1, i + 1) + P(k, j, i + 1) + P(k, j + 1, i - 1) + P(k, j, i - 1) + small,
+              h * (dxnm + dxn)));
     const T u_j_bar3 =
         h * dt * wc *
-        (q4 * (rnp * V(k + 1, j, i) + rn * V(k, j, i) + rnp * V(k + 1, j - 1, i) + rn * V(k, j - 1, i)) /
-             g_bar3 *
-             (P(k + 1, j + 1, i) + P(k, j + 1, i) - P(k + 1, j - 1, i) - P(k, j - 1, i)) /
-             (P(k + 1, j + 1, i) + P(k, j + 1, i) + P(k + 1, j - 1, i) + P(k, j - 1, i) + small) /
-             (h * (dynm + dyn)) +
-         q4 * (rnp * U(k + 1, j, i) + rn * U(k, j, i) + rnp * U(k + 1, j, i - 1) + rn * U(k, j, i - 1)) /
-             g_bar3 *
-             (P(k + 1, j, i + 1) + P(k, j, i + 1) - P(k + 1, j, i - 1) - P(k, j, i - 1)) /
-             (P(k + 1, j, i + 1) + P(k, j, i + 1) + P(k + 1, j, i - 1) + P(k, j, i - 1) + small) /
-             (h * (dxnm + dxn)));
+        (term(rnp * V(k + 1, j, i) + rn * V(k, j, i) + rnp * V(k + 1, j - 1, i) + rn * V(k, j - 1, i),
+              g_bar3,
+              P(k + 1, j + 1, i) + P(k, j + 1, i) - P(k + 1, j - 1, i) - P(k, j - 1, i),
+              P(k + 1, j + 1, i) + P(k, j + 1, i) + P(k + 1, j - 1, i) + P(k, j - 1, i) + small,
+              h * (dynm + dyn)) +
+         term(rnp * U(k + 1, j, i) + rn * U(k, j, i) + rnp * U(k + 1, j, i - 1) + rn * U(k, j, i - 1),
+              g_bar3,
+              P(k + 1, j, i + 1) + P(k, j, i + 1) - P(k + 1, j, i - 1) - P(k, j, i - 1),
+              P(k + 1, j, i + 1) + P(k, j, i + 1) + P(k + 1, j, i - 1) + P(k, j, i - 1) + small,
+              h * (dxnm + dxn)));
 
     const T pc = P(k, j, i);
-    T us = (fabs(uc) * dx - dt * uc * uc) * (P(k, j, i + 1) - pc) / (P(k, j, i + 1) + pc + small) / dxn -
+    T us = adiv(adiv((fabs(uc) * dx - dt * uc * uc) * (P(k, j, i + 1) - pc),
+                     P(k, j, i + 1) + pc + small),
+                dxn) -
            u_j_bar1;
-    T vs = (fabs(vc) * dy - dt * vc * vc) * (P(k, j + 1, i) - pc) / (P(k, j + 1, i) + pc + small) / dyn -
+    T vs = adiv(adiv((fabs(vc) * dy - dt * vc * vc) * (P(k, j + 1, i) - pc),
+                     P(k, j + 1, i) + pc + small),
+                dyn) -
            u_j_bar2;
-    T ws = (fabs(wc) * dz - dt * (ra / g_bar3) * wc * wc) * (P(k + 1, j, i) - pc) /
-               (P(k + 1, j, i) + pc + small) / dzn -
+    T ws = adiv(adiv((fabs(wc) * dz - dt * adiv(ra, g_bar3) * wc * wc) * (P(k + 1, j, i) - pc),
+                     P(k + 1, j, i) + pc + small),
+                dzn) -
            u_j_bar3;
-    us = us - q4 * dt * uc * ((U(k, j, i + 1) - U(k, j, i - 1)) / dxm + u_div1);  // :489-499
-    vs = vs - q4 * dt * vc * ((V(k, j + 1, i) - V(k, j - 1, i)) / dym + u_div2);
-    ws = ws - q4 * dt * wc * ((rap * W(k + 1, j, i) - ram * W(k - 1, j, i)) / (dzm * g_bar3) + u_div3);
+    us = us - q4 * dt * uc * (adiv(U(k, j, i + 1) - U(k, j, i - 1), dxm) + u_div1);  // :489-499
+    vs = vs - q4 * dt * vc * (adiv(V(k, j + 1, i) - V(k, j - 1, i), dym) + u_div2);
+    ws = ws - q4 * dt * wc * (adiv(rap * W(k + 1, j, i) - ram * W(k - 1, j, i), dzm * g_bar3) + u_div3);
     // exchange_full(..., 0, 0) of the new velocities, :528-533
     put_full(out.u, d, k, j, i, us, T(0), T(0));
     put_full(out.v, d, k, j, i, vs, T(0), T(0));
