@@ -24,7 +24,9 @@ struct SolverScalars {
     // FP64 residual keeping the FP32 correction, 2 = its vectors went
     // non-finite, drop the correction since the last update
     int restart;
-    int rounds;    // loop rounds of a graph-driven solve (bounded, see k_loop_cond)
+    int rounds;    // iterations of a graph-driven solve (bounded, see k_loop_cond)
+    int cycles;    // mixed form, graph-driven: FP64 update cycles (outer loop rounds)
+    int ru_runs;   // mixed form, graph-driven: reliable-update branches taken
     int fresh;     // the next iteration starts a recursion (p = v1 = 0)
     int restarts;  // restarts of this solve
     int cycle_it;  // FP32 iterations since the last FP64 update

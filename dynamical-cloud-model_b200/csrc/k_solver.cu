@@ -71,6 +71,11 @@ struct SolverArgs {
     // reference's x1 = s0, x_m+1 = x_m + s0 - (A x_m)/a_p
     int cheb;
     double cw[4];
+    // graph-driven loops: the update kernel sets the condition of the WHILE
+    // node around the iteration (cond) itself, bounded by cond_max
+    // iterations; cond_max = 0 outside a graph loop
+    cudaGraphConditionalHandle cond = 0;
+    int cond_max = 0;
 };
 
 // a_p exactly as set_mat_a forms it (dynamics.f90:93-95)
@@ -434,6 +439,8 @@ __device__ __forceinline__ void reduce_tail(const SolverArgs& a, double (&acc)[N
             S->early = 0;
             S->done = 0;
             S->rounds = 0;
+            S->cycles = 0;
+            S->ru_runs = 0;
             if (err < a.tol) {  // :382-383 early return
                 S->early = 1;
                 S->done = 1;
@@ -734,6 +741,26 @@ __global__ void __launch_bounds__(PW * 32, 1)
     cp_async_wait<0>();
 }
 
+// Condition of a graph-driven loop: one more iteration while the solve has
+// neither finished nor paused for a reliable update.  The round budget bounds
+// the loop whatever the scalars do: past it the solve stops with
+// DCM_E_TIMEOUT.
+__device__ __forceinline__ unsigned loop_cond(cudaGraphConditionalHandle h, SolverScalars* S,
+                                              int max_rounds) {
+    unsigned go = (S->done || S->pause) ? 0u : 1u;
+    if (go) {
+        if (S->rounds >= max_rounds) {
+            S->status = DCM_E_TIMEOUT;
+            S->done = 1;
+            go = 0u;
+        } else {
+            S->rounds = S->rounds + 1;
+        }
+    }
+    cudaGraphSetConditional(h, go);
+    return go;
+}
+
 // --- D: x, r updates, (r,r), (r,cr) -> err, next rho and bet -----------------
 template <typename T>
 __global__ void __launch_bounds__(256) k_bicg_update(SolverArgs a, Coef<T> c,
@@ -747,7 +774,12 @@ __global__ void __launch_bounds__(256) k_bicg_update(SolverArgs a, Coef<T> c,
                                                      T* __restrict__ rh, Red2 R,
                                                      SolverScalars* S) {
     __shared__ double smem[64];
-    if (S->done || S->pause) return;
+    if (S->done || S->pause) {
+        // stopped earlier in this iteration: end the graph loop
+        if (a.cond_max && blockIdx.x == 0 && threadIdx.x == 0 && threadIdx.y == 0)
+            cudaGraphSetConditional(a.cond, 0u);
+        return;
+    }
     const Dims& d = a.d;
     const T alf = (T)S->alf, omg = (T)S->omg;
     double acc[2] = {0.0, 0.0};
@@ -836,6 +868,7 @@ __global__ void __launch_bounds__(256) k_bicg_update(SolverArgs a, Coef<T> c,
             S->rho = s[1];  // (r,cr) of the next iteration, :391
             S->bet = (S->rho / S->nrm) * (S->alf / S->omg);  // :392
         }
+        if (a.cond_max) loop_cond(a.cond, S, a.cond_max);
     }
 }
 
@@ -1039,27 +1072,31 @@ static void launch_iteration(const SolverArgs& a, const Coef<T>& c, SolverWork<T
 }
 
 // ---- graph-driven loops ------------------------------------------------------
-// Condition of the WHILE node: one more round while the solve has not set
-// `done`.  The round budget bounds the loop whatever the scalars do: past it
-// the solve stops with DCM_E_TIMEOUT.
+// The first condition of an iteration loop, before its WHILE node; the update
+// kernel sets it after every iteration (loop_cond).
 __global__ void k_loop_cond(cudaGraphConditionalHandle h, SolverScalars* S, int max_rounds) {
-    unsigned go = S->done ? 0u : 1u;
-    if (go) {
-        if (S->rounds >= max_rounds) {
-            S->status = DCM_E_TIMEOUT;
-            S->done = 1;
-            go = 0u;
-        } else {
-            S->rounds = S->rounds + 1;
-        }
-    }
-    cudaGraphSetConditional(h, go);
+    loop_cond(h, S, max_rounds);
 }
 
-// Condition of the IF/ELSE node of the mixed solve: reliable update or
-// another FP32 iteration.
-__global__ void k_branch_pause(cudaGraphConditionalHandle h, const SolverScalars* S) {
-    cudaGraphSetConditional(h, S->pause ? 1u : 0u);
+// Mixed form: the start of an FP64 update cycle, the first condition of its
+// loop of FP32 iterations.
+__global__ void k_cycle_start(cudaGraphConditionalHandle h, SolverScalars* S, int max_rounds) {
+    S->cycles = S->cycles + 1;
+    loop_cond(h, S, max_rounds);
+}
+
+// Mixed form: condition of the outer WHILE node, another cycle while the
+// solve has not finished.
+__global__ void k_outer_cond(cudaGraphConditionalHandle h, const SolverScalars* S) {
+    cudaGraphSetConditional(h, S->done ? 0u : 1u);
+}
+
+// Condition of the IF node of the mixed solve: the FP32 iterations paused
+// for a reliable update (otherwise they finished).
+__global__ void k_branch_pause(cudaGraphConditionalHandle h, SolverScalars* S) {
+    const unsigned go = S->pause ? 1u : 0u;
+    if (go) S->ru_runs = S->ru_runs + 1;
+    cudaGraphSetConditional(h, go);
 }
 
 namespace {
@@ -1191,9 +1228,11 @@ int solver_run(SolverWork<T>& w, const Dims& d, T* x, const T* b, const T* sw, c
         bool good = capture_cond_handle(s, &hw, 0);
         if (good) k_loop_cond<<<1, 1, 0, s>>>(hw, w.S, max_rounds);
         good = good && capture_cond_node(s, hw, cudaGraphCondTypeWhile, 1, body);
+        SolverArgs ai = a;  // the update kernel sets the loop's condition
+        ai.cond = hw;
+        ai.cond_max = max_rounds;
         good = good && capture_into(G.side[0], body[0], [&](cudaStream_t s2) {
-                   launch_iteration<T>(a, c, w, x, s2);
-                   k_loop_cond<<<1, 1, 0, s2>>>(hw, w.S, max_rounds);
+                   launch_iteration<T>(ai, c, w, x, s2);
                });
         post_launch(s);
         return good && cudaPeekAtLastError() == cudaSuccess;
@@ -1229,13 +1268,13 @@ int solver_run(SolverWork<T>& w, const Dims& d, T* x, const T* b, const T* sw, c
         if (!ok(cudaGraphLaunch(G.exec, st))) return DCM_E_CUDA;
         cudaMemcpyAsync(host_S, w.S, sizeof(SolverScalars), cudaMemcpyDeviceToHost, st);
         if (cudaStreamSynchronize(st) != cudaSuccess) return DCM_E_CUDA;
-        const long long r = host_S->rounds;
+        const long long r = host_S->rounds;  // iterations run
         if (g_prof) {
             g_prof->add(P_SETUP, 1);
-            g_prof->add(P_JACOBI, 6 * r);
+            g_prof->add(P_JACOBI, (fused_ok<T>(a) ? 2 : 6) * r);
             g_prof->add(P_MATVEC, 2 * r);
             g_prof->add(P_UPDATE, r);
-            g_prof->add(P_OTHER, r + 1);
+            g_prof->add(P_OTHER, 1);
             if (post) g_prof->add(P_POST, 1);
         }
         if (launched_iters) *launched_iters = (int)r;
@@ -1345,6 +1384,8 @@ __global__ void __launch_bounds__(256) k_ru_residual(SolverArgs a, Coef<double> 
             S->status = 0;
             S->updates = 0;
             S->rounds = 0;
+            S->cycles = 0;
+            S->ru_runs = 0;
             S->restarts = 0;
             S->fresh = 0;
         }
@@ -1475,28 +1516,41 @@ int refine_run(SolverWork<float>& wf, SolverWork<double>& wd, const Dims& d, dou
         k_bicg_post<double, float><<<gi, bl, 0, s>>>(d, x, sw, dzn, wd.S, 1);
     };
     const int max_rounds = itmax + max_updates + 1;
-    // the whole mixed solve into the graph being captured on `s0`
+    // the whole mixed solve into the graph being captured on `s0`:
+    //   WHILE (not done) {                           one FP64 update cycle
+    //       WHILE (not done, not paused) { FP32 iteration }
+    //       IF (paused) { reliable update }
+    //   }
+    // The update kernel of each FP32 iteration sets the inner condition, so
+    // an iteration is its five (or nine) kernels and nothing else.  Both
+    // loops are bounded: a cycle starts with pause = 0, so every cycle that
+    // does not end the solve counts an iteration against max_rounds.
     auto emit = [&](cudaStream_t s0, SolveGraph& G) {
         if (!side_streams(G)) return false;
         CaptureGuard cgd;
-        cudaGraphConditionalHandle hw{};
+        cudaGraphConditionalHandle ho{};
         cudaGraph_t body[1] = {nullptr};
         begin(s0);
-        bool good = capture_cond_handle(s0, &hw, 0);
-        if (good) k_loop_cond<<<1, 1, 0, s0>>>(hw, wf.S, max_rounds);
-        good = good && capture_cond_node(s0, hw, cudaGraphCondTypeWhile, 1, body);
-        // loop body: branch on pause -> reliable update | FP32 iteration
+        bool good = capture_cond_handle(s0, &ho, 0);
+        if (good) k_outer_cond<<<1, 1, 0, s0>>>(ho, wf.S);
+        good = good && capture_cond_node(s0, ho, cudaGraphCondTypeWhile, 1, body);
         good = good && capture_into(G.side[0], body[0], [&](cudaStream_t s) {
-                   cudaGraphConditionalHandle hb{};
-                   cudaGraph_t br[2] = {nullptr, nullptr};
-                   bool g2 = capture_cond_handle(s, &hb, 0);
-                   if (g2) k_branch_pause<<<1, 1, 0, s>>>(hb, wf.S);
-                   g2 = g2 && capture_cond_node(s, hb, cudaGraphCondTypeIf, 2, br);
-                   g2 = g2 && capture_into(G.side[1], br[0], update);
-                   g2 = g2 && capture_into(G.side[1], br[1], [&](cudaStream_t s2) {
-                            launch_iteration<float>(af, cf, wf, dx, s2);
+                   cudaGraphConditionalHandle hi{}, hb{};
+                   cudaGraph_t in[1] = {nullptr}, br[1] = {nullptr};
+                   SolverArgs ai = af;
+                   bool g2 = capture_cond_handle(s, &hi, 0);
+                   if (g2) k_cycle_start<<<1, 1, 0, s>>>(hi, wf.S, max_rounds);
+                   g2 = g2 && capture_cond_node(s, hi, cudaGraphCondTypeWhile, 1, in);
+                   ai.cond = hi;
+                   ai.cond_max = max_rounds;
+                   g2 = g2 && capture_into(G.side[1], in[0], [&](cudaStream_t s2) {
+                            launch_iteration<float>(ai, cf, wf, dx, s2);
                         });
-                   k_loop_cond<<<1, 1, 0, s>>>(hw, wf.S, max_rounds);
+                   g2 = g2 && capture_cond_handle(s, &hb, 0);
+                   if (g2) k_branch_pause<<<1, 1, 0, s>>>(hb, wf.S);
+                   g2 = g2 && capture_cond_node(s, hb, cudaGraphCondTypeIf, 1, br);
+                   g2 = g2 && capture_into(G.side[1], br[0], update);
+                   k_outer_cond<<<1, 1, 0, s>>>(ho, wf.S);
                    if (!g2) good = false;
                });
         finish(s0);
@@ -1554,13 +1608,14 @@ int refine_run(SolverWork<float>& wf, SolverWork<double>& wd, const Dims& d, dou
     int status = hS_out->status;
     if (status == DCM_OK && !hS_in->done) status = DCM_E_NOCONV;  // host loop ran out
     if (use_graph && g_prof) {
-        const long long r = hS_in->rounds, u = hS_in->updates, itr = r - u;
+        // iterations, reliable updates and cycles the graph ran
+        const long long itr = hS_in->rounds, u = hS_in->ru_runs, cyc = hS_in->cycles;
         g_prof->add(P_SETUP, u + 1);
-        g_prof->add(P_JACOBI, 6 * itr);
+        g_prof->add(P_JACOBI, (fused_ok<float>(af) ? 2 : 6) * itr);
         g_prof->add(P_MATVEC, 2 * itr);
         g_prof->add(P_UPDATE, itr + u + 1);
         g_prof->add(P_POST, 1);
-        g_prof->add(P_OTHER, 2 * r + 3);
+        g_prof->add(P_OTHER, 3 * cyc + 3);
     }
     if (rs) {
         rs->outer = hS_in->updates;
