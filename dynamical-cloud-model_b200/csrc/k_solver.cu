@@ -46,6 +46,18 @@
 
 namespace dcm {
 
+// Programmatic dependent launch.  Inside a graph-driven iteration every
+// kernel but the first is launched with programmatic stream serialisation,
+// so it is launched while its predecessor finishes instead of after it.
+// pdl_wait holds the kernel until the predecessor has completed and its
+// writes are visible (for a kernel launched without the attribute nothing
+// is in flight and it returns at once); pdl_launch then lets the next kernel
+// be launched.  No kernel reads anything before pdl_wait.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_launch() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 template <typename T>
 struct Coef {
     const T *ae, *aw;  // per i
@@ -76,6 +88,8 @@ struct SolverArgs {
     // iterations; cond_max = 0 outside a graph loop
     cudaGraphConditionalHandle cond = 0;
     int cond_max = 0;
+    // launch with programmatic stream serialisation (pdl_wait)
+    int pdl = 0;
 };
 
 // a_p exactly as set_mat_a forms it (dynamics.f90:93-95)
@@ -487,6 +501,8 @@ __global__ void __launch_bounds__(256) k_sten(SolverArgs a, Coef<T> c, SolverBuf
     constexpr int NV = (OP == OP_SETUP || OP == OP_MATC) ? 2 : 1;
     constexpr bool RED = OP == OP_SETUP || OP == OP_MATC || OP == OP_MATP;
     __shared__ double smem[64];
+    pdl_wait();
+    pdl_launch();
     if (OP != OP_SETUP && (S->done || S->pause)) return;
     StenCtx<T, OP, MODE> C;
     C.d = a.d;
@@ -583,6 +599,8 @@ __global__ void __launch_bounds__(PW * 32, 1)
     // [PD][rh, vh, p][warp][lane]
     extern __shared__ float4 sbuf[];
     float4* ring = sbuf + 3 * 2 * PW * 32;
+    pdl_wait();
+    pdl_launch();
     if (S->done || S->pause) return;
     const Dims& d = a.d;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -774,6 +792,8 @@ __global__ void __launch_bounds__(256) k_bicg_update(SolverArgs a, Coef<T> c,
                                                      T* __restrict__ rh, Red2 R,
                                                      SolverScalars* S) {
     __shared__ double smem[64];
+    pdl_wait();
+    pdl_launch();
     if (S->done || S->pause) {
         // stopped earlier in this iteration: end the graph loop
         if (a.cond_max && blockIdx.x == 0 && threadIdx.x == 0 && threadIdx.y == 0)
@@ -938,6 +958,23 @@ static int kchunks(const Dims& d) {
     return (d.kp + KVec<T>::V * BX - 1) / (KVec<T>::V * BX);
 }
 
+// a kernel launch, with programmatic stream serialisation when `pdl`
+template <typename... P, typename... A>
+static void launch(bool pdl, void (*kern)(P...), dim3 grid, dim3 block, size_t smem,
+                   cudaStream_t st, A... args) {
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cfg.attrs = at;
+    cfg.numAttrs = pdl ? 1 : 0;
+    cudaLaunchKernelEx(&cfg, kern, args...);
+}
+
 // blocks of a reducing kernel: all resident blocks (tasks = 0: persistent,
 // each warp strides over many tasks), or enough blocks for `tasks` warp
 // tasks per warp (tasks = 1: one task per warp, as many blocks as tasks / 8),
@@ -960,14 +997,14 @@ static void sten(const SolverArgs& a, const Coef<T>& c, const SolverBufs& B, Sol
     if (RED) {
         static int full = 0;
         if (!full) full = persistent_grid(k_sten<T, OP, MODE>);
-        k_sten<T, OP, MODE><<<red_grid(a, full, a.nkt, 1), dim3(BX, BY), 0, st>>>(
-            a, c, B, w.red, w.S);
+        launch(a.pdl, k_sten<T, OP, MODE>, dim3(red_grid(a, full, a.nkt, 1)), dim3(BX, BY), 0,
+               st, a, c, B, w.red, w.S);
     } else {
         // at most 256 threads: the kernels are compiled with __launch_bounds__(256)
         const int by = a.by >= 1 && a.by <= 256 / BX ? a.by : BY;
         const int ni = OP == OP_SW1 ? a.ni : 1;
         const dim3 grid(a.nkt, (a.d.jp + by - 1) / by, (a.d.ip + ni - 1) / ni);
-        k_sten<T, OP, MODE><<<grid, dim3(BX, by), 0, st>>>(a, c, B, w.red, w.S);
+        launch(a.pdl, k_sten<T, OP, MODE>, grid, dim3(BX, by), 0, st, a, c, B, w.red, w.S);
     }
 }
 
@@ -990,12 +1027,19 @@ static void precond3(const SolverArgs& a, const Coef<float>& c, const SolverBufs
     const int nch = std::max(1, std::min((a.d.ip + 7) / 8, sm_count() / nstrips));
     const int ni = (a.d.ip + nch - 1) / nch;
     const dim3 grid(nstrips, (a.d.ip + ni - 1) / ni);
-    auto go = [&](auto kern) { kern<<<grid, PW * 32, PRECOND3_SMEM, st>>>(a, c, B, S, ni); };
+    auto go = [&](auto kern) {
+        launch(a.pdl, kern, grid, dim3(PW * 32), PRECOND3_SMEM, st, a, c, B,
+               (const SolverScalars*)S, ni);
+    };
     if (mode == 0)
         a.cheb ? go(k_precond3<0, true>) : go(k_precond3<0, false>);
     else
         a.cheb ? go(k_precond3<1, true>) : go(k_precond3<1, false>);
 }
+
+// programmatic edges inside the graph-driven iterations (probed once)
+static int g_pdl_graphs = 0;
+static bool probe_pdl_graphs();
 
 void solver_init() {
     const int sm = (int)PRECOND3_SMEM;
@@ -1003,6 +1047,11 @@ void solver_init() {
     cudaFuncSetAttribute(k_precond3<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
     cudaFuncSetAttribute(k_precond3<0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
     cudaFuncSetAttribute(k_precond3<1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    static bool probed = false;
+    if (!probed) {
+        probed = true;
+        g_pdl_graphs = probe_pdl_graphs() ? 1 : 0;
+    }
 }
 
 template <typename T>
@@ -1014,16 +1063,18 @@ static void launch_iteration(const SolverArgs& a, const Coef<T>& c, SolverWork<T
     B.rh = w.rh;
     B.vh = w.vh;
     const bool fused = fused_ok<T>(a);
+    SolverArgs a0 = a;  // the first kernel follows no kernel of this iteration
+    a0.pdl = 0;
     // phase B: precondition(s <- t), p = s + bet p, v1 = A p
     if (fused) {
         if constexpr (std::is_same<T, float>::value) {
             B.out = w.p;
-            precond3(a, c, B, w.S, 0, st);
+            precond3(a0, c, B, w.S, 0, st);
         }
     } else {
         B.out = w.sA;
         B.sweep = 1;
-        sten<T, OP_SW1, 0>(a, c, B, w, st, P_JACOBI);
+        sten<T, OP_SW1, 0>(a0, c, B, w, st, P_JACOBI);
         B.sin = w.sA;
         B.out = w.sB;
         B.sweep = 2;
@@ -1066,8 +1117,9 @@ static void launch_iteration(const SolverArgs& a, const Coef<T>& c, SolverWork<T
         ProfScope ps(P_UPDATE, st);
         static int full = 0;
         if (!full) full = persistent_grid(k_bicg_update<T>);
-        k_bicg_update<T><<<red_grid(a, full, a.nkt), dim3(BX, BY), 0, st>>>(a, c, x, w.p, w.sA, w.r, w.v1, w.t, w.cr,
-                                                     w.rh, w.red, w.S);
+        launch(a.pdl, k_bicg_update<T>, dim3(red_grid(a, full, a.nkt)), dim3(BX, BY), 0, st, a,
+               c, x, (const T*)w.p, (const T*)w.sA, w.r, (const T*)w.v1, (const T*)w.t,
+               (const T*)w.cr, w.rh, w.red, w.S);
     }
 }
 
@@ -1163,6 +1215,41 @@ bool side_streams(SolveGraph& G) {
 
 }  // namespace
 
+__global__ void k_pdl_probe() {
+    pdl_wait();
+    pdl_launch();
+}
+
+// Whether this runtime takes a programmatic edge between two kernels captured
+// into the body of a WHILE node, as the graph-driven solves place them.  A
+// graph of that shape is instantiated, never launched; without the edges the
+// solves launch each kernel after its predecessor.
+static bool probe_pdl_graphs() {
+    cudaStream_t s = nullptr;
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t ge = nullptr;
+    cudaGraphConditionalHandle h{};
+    bool good = ok(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking)) &&
+                ok(cudaGraphCreate(&g, 0)) && ok(cudaGraphConditionalHandleCreate(&h, g, 0, 0));
+    cudaGraphNodeParams p = {};
+    p.type = cudaGraphNodeTypeConditional;
+    p.conditional.handle = h;
+    p.conditional.type = cudaGraphCondTypeWhile;
+    p.conditional.size = 1;
+    cudaGraphNode_t node;
+    good = good && ok(cudaGraphAddNode(&node, g, nullptr, 0, &p));
+    good = good && capture_into(s, p.conditional.phGraph_out[0], [&](cudaStream_t s2) {
+               launch(false, k_pdl_probe, dim3(1), dim3(32), 0, s2);
+               launch(true, k_pdl_probe, dim3(1), dim3(32), 0, s2);
+           });
+    good = good && ok(cudaGraphInstantiate(&ge, g, 0));
+    if (ge) cudaGraphExecDestroy(ge);
+    if (g) cudaGraphDestroy(g);
+    if (s) cudaStreamDestroy(s);
+    cudaGetLastError();
+    return good;
+}
+
 // Weights of the Chebyshev-weighted sweeps: the preconditioned operator is
 // 1 - R(D^-1 A) with R(mu) = prod_m (1 - mu / theta_m), theta_m the four
 // roots of the degree-4 Chebyshev polynomial on [lo, 2]
@@ -1231,6 +1318,7 @@ int solver_run(SolverWork<T>& w, const Dims& d, T* x, const T* b, const T* sw, c
         SolverArgs ai = a;  // the update kernel sets the loop's condition
         ai.cond = hw;
         ai.cond_max = max_rounds;
+        ai.pdl = g_pdl_graphs;
         good = good && capture_into(G.side[0], body[0], [&](cudaStream_t s2) {
                    launch_iteration<T>(ai, c, w, x, s2);
                });
@@ -1543,6 +1631,7 @@ int refine_run(SolverWork<float>& wf, SolverWork<double>& wd, const Dims& d, dou
                    g2 = g2 && capture_cond_node(s, hi, cudaGraphCondTypeWhile, 1, in);
                    ai.cond = hi;
                    ai.cond_max = max_rounds;
+                   ai.pdl = g_pdl_graphs;
                    g2 = g2 && capture_into(G.side[1], in[0], [&](cudaStream_t s2) {
                             launch_iteration<float>(ai, cf, wf, dx, s2);
                         });
