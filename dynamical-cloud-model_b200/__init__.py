@@ -121,6 +121,7 @@ def library():
             "dcm_profile_enable": [P, C.c_int],
             "dcm_profile_read": [P, _dp, C.POINTER(C.c_longlong), C.c_int],
             "dcm_solver_graphs": [P, C.c_int],
+            "dcm_solver_graph_info": [P, C.POINTER(C.c_int)],
             "dcm_tune": [P, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
                          C.POINTER(C.c_int), C.POINTER(C.c_int)],
             "dcm_set_launch_shape": [P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int],
@@ -153,7 +154,8 @@ EXPORTS = ("dcm_create", "dcm_destroy", "dcm_status_string", "dcm_last_error",
            "dcm_divergence_calc", "dcm_advance_scalar_fields_3d", "dcm_exchange_full",
            "dcm_exchange_along_dim", "dcm_exchange_along_dim_wo", "dcm_state_upload",
            "dcm_driver_start", "dcm_step", "dcm_state_download", "dcm_profile_enable",
-           "dcm_profile_read", "dcm_horizontal_means_noalloc", "dcm_solver_graphs", "dcm_tune",
+           "dcm_profile_read", "dcm_horizontal_means_noalloc", "dcm_solver_graphs",
+           "dcm_solver_graph_info", "dcm_tune",
            "dcm_set_launch_shape", "dcm_ensemble_create", "dcm_ensemble_destroy", "dcm_ensemble_member",
            "dcm_ensemble_step", "dcm_ensemble_last_error", "dcm_exchange_full_wo",
            "dcm_calculate_subgrid_3d", "dcm_output_open", "dcm_output_write",
@@ -462,8 +464,18 @@ class DynamicalCore:
         return stats
 
     def solver_graphs(self, on=True):
-        """Graph-driven pressure solves (default) or the host-polled loop."""
-        self._check(self.lib.dcm_solver_graphs(self.h, int(bool(on))))
+        """Graph-driven pressure solves (True or 1, the default), the same graphs
+        without programmatic dependent launch (2), or the host-polled loop
+        (False or 0)."""
+        mode = on if isinstance(on, int) and not isinstance(on, bool) else int(bool(on))
+        self._check(self.lib.dcm_solver_graphs(self.h, mode))
+
+    def solver_graph_info(self):
+        """Whether the graph-driven solves launch their iteration kernels with
+        programmatic dependent launch."""
+        v = C.c_int(0)
+        self._check(self.lib.dcm_solver_graph_info(self.h, C.byref(v)))
+        return dict(programmatic_launch=bool(v.value))
 
     def profile(self, on=True):
         """Enable (and reset) or disable per-kernel-class event timing."""

@@ -92,7 +92,9 @@ struct dcm_handle {
     // captured pressure solves (FP64 and mixed), rebuilt when their
     // arguments change
     SolveGraph g64, g32;
-    bool graphs = true;  // graph-driven solver loops (else host-polled)
+    // solver loops: 1 graph-driven, 2 graph-driven without programmatic
+    // dependent launch, 0 host-polled
+    int graphs = 1;
     // launch shape of the solver kernels per precision (dcm_tune; [0] FP64,
     // [1] the FP32 iterations of the mixed form): warps per sweep block, warp
     // tasks per warp of the reducing kernels (0 = fill the GPU), marching depth
@@ -234,6 +236,7 @@ SolverWork<double> solver_work(dcm_handle* h) {
     w.red.partials = h->partials; w.red.gpartials = h->gpartials; w.red.gtick = h->gtick;
     w.red.ticket = h->ticket2;
     w.graph = h->graphs ? &h->g64 : nullptr;
+    w.pdl = h->graphs == 1;
     w.by = h->tune_by[0];
     w.tasks = h->tune_tasks[0];
     w.ni = h->tune_ni[0];
@@ -987,6 +990,7 @@ SolverWork<float> solver_work_f(dcm_handle* h) {
     w.red.partials = h->partials; w.red.gpartials = h->gpartials; w.red.gtick = h->gtick;
     w.red.ticket = h->ticket2;
     w.graph = h->graphs ? &h->g32 : nullptr;
+    w.pdl = h->graphs == 1;
     w.by = h->tune_by[1];
     w.tasks = h->tune_tasks[1];
     w.ni = h->tune_ni[1];
@@ -1436,7 +1440,16 @@ extern "C" int dcm_state_download(dcm_handle* h, dcm_fields* f) {
 // =============================================================================
 extern "C" int dcm_solver_graphs(dcm_handle* h, int on) {
     CHECK_H();
-    h->graphs = on != 0;
+    const int mode = on == 0 ? 0 : on == 2 ? 2 : 1;
+    if (mode != h->graphs) h->generation += 1;  // an ensemble recaptures its steps
+    h->graphs = mode;
+    return DCM_OK;
+}
+
+extern "C" int dcm_solver_graph_info(dcm_handle* h, int* programmatic) {
+    CHECK_H();
+    if (!programmatic) return DCM_E_ARG;
+    *programmatic = h->graphs == 1 && solver_pdl_available() ? 1 : 0;
     return DCM_OK;
 }
 

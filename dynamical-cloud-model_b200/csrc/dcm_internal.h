@@ -95,11 +95,17 @@ struct SolverWork {
     // unweighted sweeps)
     int cheb = 0;
     double cheb_lo = 0.05;
+    // graph-driven iterations launch their kernels with programmatic
+    // dependent launch (where the runtime takes it; solver_pdl_available)
+    int pdl = 1;
 };
 
-// one-time setup of the solver kernels (shared-memory limits); called at
-// handle creation, outside any stream capture
+// one-time setup of the solver kernels (shared-memory limits, the probe of
+// programmatic launches in graphs); called at handle creation, outside any
+// stream capture
 void solver_init();
+// whether graph-driven iterations can use programmatic dependent launch
+bool solver_pdl_available();
 
 // per-field scalars of one MPDATA call
 struct MpScalars {

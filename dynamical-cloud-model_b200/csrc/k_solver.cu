@@ -1054,6 +1054,8 @@ void solver_init() {
     }
 }
 
+bool solver_pdl_available() { return g_pdl_graphs != 0; }
+
 template <typename T>
 static void launch_iteration(const SolverArgs& a, const Coef<T>& c, SolverWork<T>& w, T* x,
                              cudaStream_t st) {
@@ -1318,7 +1320,7 @@ int solver_run(SolverWork<T>& w, const Dims& d, T* x, const T* b, const T* sw, c
         SolverArgs ai = a;  // the update kernel sets the loop's condition
         ai.cond = hw;
         ai.cond_max = max_rounds;
-        ai.pdl = g_pdl_graphs;
+        ai.pdl = g_pdl_graphs && w.pdl;
         good = good && capture_into(G.side[0], body[0], [&](cudaStream_t s2) {
                    launch_iteration<T>(ai, c, w, x, s2);
                });
@@ -1331,8 +1333,9 @@ int solver_run(SolverWork<T>& w, const Dims& d, T* x, const T* b, const T* sw, c
         SolveGraph& G = *w.graph;
         const void* kp[6] = {x, b, sw, dzn, w.r, w.S};
         const double kd[3] = {tol, sc_floor, 0.0};
-        // launch shape: by < 16, tasks < 16, ni < 64, fuse < 2
-        const int shape = a.by + 16 * a.tasks + 256 * a.ni + 16384 * a.fuse;
+        // launch shape: by < 16, tasks < 16, ni < 64, fuse < 2, pdl < 2
+        const int shape =
+            a.by + 16 * a.tasks + 256 * a.ni + 16384 * a.fuse + 65536 * (w.pdl ? 1 : 0);
         const int ki[6] = {itmax, wo, post ? 1 : 0, (int)sizeof(T) + 16 * shape,
                            d.ip * 4096 + d.jp, d.kp};
         if (!G.matches(kp, kd, ki)) {
@@ -1631,7 +1634,7 @@ int refine_run(SolverWork<float>& wf, SolverWork<double>& wd, const Dims& d, dou
                    g2 = g2 && capture_cond_node(s, hi, cudaGraphCondTypeWhile, 1, in);
                    ai.cond = hi;
                    ai.cond_max = max_rounds;
-                   ai.pdl = g_pdl_graphs;
+                   ai.pdl = g_pdl_graphs && wf.pdl;
                    g2 = g2 && capture_into(G.side[1], in[0], [&](cudaStream_t s2) {
                             launch_iteration<float>(ai, cf, wf, dx, s2);
                         });
@@ -1651,8 +1654,8 @@ int refine_run(SolverWork<float>& wf, SolverWork<double>& wd, const Dims& d, dou
         SolveGraph& G = *wf.graph;
         const void* kp[6] = {x, b, sw, dzn, dx, wf.S};
         const double kd[3] = {tol, delta, af.cheb ? wf.cheb_lo : 0.0};
-        const int shape =
-            af.by + 16 * af.tasks + 256 * af.ni + 16384 * af.fuse + 32768 * af.cheb;
+        const int shape = af.by + 16 * af.tasks + 256 * af.ni + 16384 * af.fuse +
+                          32768 * af.cheb + 65536 * (wf.pdl ? 1 : 0);
         const int ki[6] = {itmax, max_updates, 1, 16 * shape, d.ip * 4096 + d.jp, d.kp};
         if (!G.matches(kp, kd, ki)) {
             G.release();

@@ -9,7 +9,9 @@ Cases: warm_bubble (256x256x128), sheared_convection (512x512x256, 8 tracers),
 kelvin_helmholtz (128x1x64), or warm_bubble_IPxJPxKP /
 sheared_convection_IPxJPxKP for other sizes.  --host-loop drives the
 pressure solve from the host (the same kernels; a profiler sees every
-launch, which it cannot inside the graph-driven solve's conditional loop).
+launch, which it cannot inside the graph-driven solve's conditional loop);
+--graphs 2 keeps the graphs but launches without programmatic dependent
+launch.
 --output FILE writes the reference's netCDF output before every
 --output-every steps and reports the host time of each write call.
 --precond 1 gives the mixed form Chebyshev-weighted sweeps on
@@ -59,6 +61,9 @@ def main():
     ap.add_argument("--precision", type=int, default=1, choices=[0, 1])
     ap.add_argument("--steps", type=int, default=1)
     ap.add_argument("--host-loop", action="store_true")
+    ap.add_argument("--graphs", type=int, default=1, choices=[0, 1, 2],
+                    help="solver loops: 1 graph-driven, 2 graph-driven without programmatic "
+                         "dependent launch, 0 host-polled (as --host-loop)")
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--viscous", action="store_true")
     ap.add_argument("--precond", type=int, default=0, choices=[0, 1])
@@ -76,8 +81,8 @@ def main():
     from dcm_b200 import cases
     c = make_case(cases, args.case)
     core = dcm.DynamicalCore(c.grid, device=args.device)
-    if args.host_loop:
-        core.solver_graphs(False)
+    if args.host_loop or args.graphs != 1:
+        core.solver_graphs(0 if args.host_loop else args.graphs)
     if args.fuse is not None:
         core.set_launch_shape(1, fuse=args.fuse)
     kw = dict(nq=c.nq, c_s=c.c_s, c_e=c.c_e) if c.nq else {}

@@ -316,14 +316,23 @@ int dcm_horizontal_means_noalloc(int ip, int jp, int kp, const double *u,
 int dcm_profile_enable(dcm_handle *h, int on);
 int dcm_profile_read(dcm_handle *h, double *ms, long long *launches, int ncat);
 /* Pressure-solve driver (default 1).  1: each solve is one CUDA graph whose
- * iteration loop is a conditional WHILE node driven by the device scalars
- * (and, in the mixed form, an IF/ELSE node choosing an FP64 reliable update
- * or an FP32 iteration), captured once and relaunched while its arguments
- * stay the same.  0: the host launches iterations in chunks of 4 and polls
- * the device scalars between chunks.  Both launch the same kernels in the
- * same order and give bit-identical results; while event timing is enabled
- * the host-driven loop is used. */
+ * iteration loop is a conditional WHILE node, set by the last kernel of
+ * every iteration from the device scalars (in the mixed form: a WHILE node of
+ * FP64 update cycles, each holding a WHILE node of FP32 iterations and an IF
+ * node for the FP64 reliable update), captured once and relaunched while its
+ * arguments stay the same; the kernels of an iteration are launched with
+ * programmatic dependent launch where the runtime takes it.  2: the same
+ * graphs without programmatic dependent launch.  0: the host launches
+ * iterations in chunks of 4 and polls the device scalars between chunks.
+ * All launch the same kernels in the same order and give bit-identical
+ * results; while event timing is enabled the host-driven loop is used. */
 int dcm_solver_graphs(dcm_handle *h, int on);
+
+/* *programmatic = 1 when this handle's graph-driven solves launch their
+ * iteration kernels with programmatic dependent launch (mode 1 of
+ * dcm_solver_graphs, and the runtime accepted such launches inside a WHILE
+ * node when the first handle was created), else 0. */
+int dcm_solver_graph_info(dcm_handle *h, int *programmatic);
 
 /* ---- solver launch-shape autotuner (no counterpart in the reference) ---- */
 /* Chooses, for this handle's grid shape and the given precision (0 FP64,

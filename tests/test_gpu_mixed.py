@@ -71,24 +71,28 @@ def test_mixed_tracers(dcm, orc):
 
 @pytest.mark.parametrize("precision", [0, 1])
 def test_graph_and_host_loops_agree(dcm, precision):
-    """The graph-driven solve (conditional WHILE / IF nodes) and the
-    host-polled loop launch the same kernels in the same order: identical
-    fields and iteration counts, step after step."""
+    """The graph-driven solve (conditional WHILE / IF nodes; with programmatic
+    dependent launch and without) and the host-polled loop launch the same
+    kernels in the same order: identical fields and iteration counts, step
+    after step.  On a B200 the runtime takes programmatic launches inside the
+    WHILE nodes, so mode 1 uses them."""
     c = small_bubble()
     out = []
-    for graphs in (True, False):
+    for mode in (1, 2, 0):
         core = dcm.DynamicalCore(c.grid)
-        core.solver_graphs(graphs)
+        core.solver_graphs(mode)
+        assert core.solver_graph_info()["programmatic_launch"] == (mode == 1)
         core.upload_state(c.state, c.dt, ptol=c.ptol, kord=c.kord, monotone=c.monotone,
-                          precision=precision)
+                          precision=precision, precond=precision)
         core.driver_start()
         its = [core.step(1).iters_last for _ in range(3)]
         out.append((its, core.download_state()))
         core.close()
-    (ia, fa), (ib, fb) = out
-    assert ia == ib
-    for n in ("u", "v", "w", "th", "p", "psrc"):
-        assert np.array_equal(fa[n], fb[n]), n
+    ia, fa = out[0]
+    for ib, fb in out[1:]:
+        assert ia == ib
+        for n in ("u", "v", "w", "th", "p", "psrc"):
+            assert np.array_equal(fa[n], fb[n]), n
 
 
 @pytest.mark.parametrize("precond", [0, 1])
