@@ -137,8 +137,9 @@ __device__ __forceinline__ T s0val(const T* __restrict__ rh, const T* __restrict
 __device__ __forceinline__ float sweep_div(float a, float b) { return __fdividef(a, b); }
 __device__ __forceinline__ double sweep_div(double a, double b) { return a / b; }
 
-// One Chebyshev-weighted sweep at a point, with every rounding explicit so
-// that the fused and the separate sweeps agree bit for bit:
+// One Chebyshev-weighted sweep at a point, every rounding of the update
+// explicit (the fused and the separate sweeps differ only in how the
+// compiler contracts the operator's products):
 //     res = sc x + w (s0 - sc (A x)/a_p),   q = (A x)/a_p
 // sc = w1 on the first sweep (its operand is w1 s0, applied here by
 // linearity instead of to the seven operand values), 1 on the others.
