@@ -1415,6 +1415,10 @@ template int solver_run<float>(SolverWork<float>&, const Dims&, float*, const fl
 // (dynamics.f90:370-428).
 
 // r = b - A x (FP64) -> r32, r32/a_p; FIRST also cr = r32 and (b,b).
+// Warp tasks as in sten_task: 2 x 32 consecutive k-levels (one 16-byte
+// vector per lane) of row j, marching over a.ni planes with the i
+// neighbours in registers; k neighbours by shuffle and, at the warp's ends,
+// one scalar load each; Neumann mirror at k = 1, kp.
 template <bool FIRST>
 __global__ void __launch_bounds__(256) k_ru_residual(SolverArgs a, Coef<double> c,
                                                      Coef<float> cf,
@@ -1425,45 +1429,107 @@ __global__ void __launch_bounds__(256) k_ru_residual(SolverArgs a, Coef<double> 
                                                      float* __restrict__ cr32, Red2 R,
                                                      SolverScalars* S) {
     __shared__ double smem[96];
+    constexpr int V = KVec<double>::V;
     const Dims& d = a.d;
     const int ip = d.ip, jp = d.jp, kp = d.kp;
+    const int K = d.K, KJ = d.K * d.J;
+    const int ni = a.ni, nib = (ip + ni - 1) / ni;
     double acc[3] = {0.0, 0.0, 0.0};
     const int lane = threadIdx.x;
     // a first residual, or a restart after a breakdown: cr = r
     const bool reset = FIRST || S->restart != 0;
     for (TaskIter t(blockIdx.x * blockDim.y + threadIdx.y, gridDim.x * blockDim.y, a.nkt, jp);
-         t.i <= ip; t.next()) {
-        const int j = 1 + t.jr, i = t.i;
-        const int k = 1 + t.kt * BX + lane;
-        const int km = min(k, kp);
-        const double xc = x[d.at(km, j, i)];
-        double xd = __shfl_up_sync(0xffffffffu, xc, 1);
-        double xu = __shfl_down_sync(0xffffffffu, xc, 1);
-        if (lane == 0) xd = x[d.at(max(km - 1, 1), j, i)];
-        if (lane == BX - 1) xu = x[d.at(min(km + 1, kp), j, i)];
-        if (k > kp) continue;
-        const double xm = x[d.at(k, j, i == 1 ? ip : i - 1)], xp = x[d.at(k, j, i == ip ? 1 : i + 1)];
-        const double xs = x[d.at(k, j == 1 ? jp : j - 1, i)], xn = x[d.at(k, j == jp ? 1 : j + 1, i)];
-        const double ae = ld(c.ae + i), aw = ld(c.aw + i), an = ld(c.an + j), as = ld(c.as + j),
-                     au = ld(c.au + k), ad = ld(c.ad + k);
-        const double ap = -ae - aw - an - as - au - ad;
-        const double Ax = aw * xm + ae * xp + as * xs + an * xn + ad * xd + au * xu + ap * xc;
-        const int o = d.at(k, j, i);
-        const double bv = b[o];
-        const double rv = bv - Ax;
-        const float rf = (float)rv;
-        r32[o] = rf;
-        rh32[o] = rf / diag_ap(cf, k, j, i);
-        float crf;
-        if (reset) {
-            cr32[o] = rf;
-            crf = rf;
-        } else {
-            crf = cr32[o];
+         t.i <= nib; t.next()) {
+        const int j = 1 + t.jr, i0 = 1 + (t.i - 1) * ni, iend = min(i0 + ni - 1, ip);
+        const int k0 = 1 + V * (t.kt * BX + lane);
+        const bool live = k0 <= kp;
+        const int nvalid = live ? min(V, kp - k0 + 1) : 0;
+        const int kl = live ? k0 : 1;  // idle lanes read the column start
+        const int col = kl + K * j;
+        const int dsj = (j == 1 ? jp - 1 : -1) * K, dnj = (j == jp ? 1 - jp : 1) * K;
+        double au[V], ad[V];
+        vld(c.au + kl, au);
+        vld(c.ad + kl, ad);
+        const double an = ld(c.an + j), as = ld(c.as + j);
+        const float anf = ld(cf.an + j), asf = ld(cf.as + j);
+        float auf[V], adf[V];
+#pragma unroll
+        for (int q = 0; q < V; q++) {
+            auf[q] = ld(cf.au + min(kl + q, kp));
+            adf[q] = ld(cf.ad + min(kl + q, kp));
         }
-        acc[0] += bv * bv;
-        acc[1] += rv * rv;
-        acc[2] += (double)rf * (double)crf;
+        double xw[V], xc[V], xe[V];
+        vld(x + col + KJ * (i0 == 1 ? ip : i0 - 1), xw);
+        vld(x + col + KJ * i0, xc);
+        for (int i = i0; i <= iend; i++) {
+            const int o = col + KJ * i;
+            double xs[V], xn[V], bv[V];
+            vld(x + col + KJ * (i == ip ? 1 : i + 1), xe);
+            vld(x + o + dsj, xs);
+            vld(x + o + dnj, xn);
+            vld(b + o, bv);
+            if (i < iend) {  // the next plane's streamed columns into L2
+                const int on = o + KJ;
+                prefetch_l2(x + col + KJ * (i + 1 == ip ? 1 : i + 2));
+                prefetch_l2(x + on + dsj);
+                prefetch_l2(x + on + dnj);
+                prefetch_l2(b + on);
+            }
+            double prev = __shfl_up_sync(0xffffffffu, xc[V - 1], 1);
+            double next = __shfl_down_sync(0xffffffffu, xc[0], 1);
+            if (lane == 0 && live && k0 > 1) prev = x[o - 1];
+            if (lane == BX - 1 && live && k0 + V <= kp) next = x[o + V];
+            const double ae = ld(c.ae + i), aw = ld(c.aw + i);
+            // diag_ap(cf, k, j, i), left to right
+            const float s4f = -ld(cf.ae + i) - ld(cf.aw + i) - anf - asf;
+            float crv[V] = {0.0f, 0.0f};
+            if (!reset && live) {
+                if (nvalid == V) {
+                    const float2 c2 = *reinterpret_cast<const float2*>(cr32 + o);
+                    crv[0] = c2.x;
+                    crv[1] = c2.y;
+                } else {
+                    crv[0] = cr32[o];
+                }
+            }
+            float rf[V], rhf[V];
+#pragma unroll
+            for (int q = 0; q < V; q++) {
+                const int kk = k0 + q;
+                double xd = q == 0 ? prev : xc[q - 1];
+                double xu = q == V - 1 ? next : xc[q + 1];
+                xd = kk == 1 ? xc[q] : xd;
+                xu = kk == kp ? xc[q] : xu;
+                const double ap = -ae - aw - an - as - au[q] - ad[q];
+                const double Ax = aw * xw[q] + ae * xe[q] + as * xs[q] + an * xn[q] +
+                                  ad[q] * xd + au[q] * xu + ap * xc[q];
+                const double rv = bv[q] - Ax;
+                rf[q] = (float)rv;
+                rhf[q] = rf[q] / (s4f - auf[q] - adf[q]);
+                if (reset) crv[q] = rf[q];
+                if (q < nvalid) {
+                    acc[0] += bv[q] * bv[q];
+                    acc[1] += rv * rv;
+                    acc[2] += (double)rf[q] * (double)crv[q];
+                }
+            }
+            if (live) {
+                if (nvalid == V) {
+                    *reinterpret_cast<float2*>(r32 + o) = make_float2(rf[0], rf[1]);
+                    *reinterpret_cast<float2*>(rh32 + o) = make_float2(rhf[0], rhf[1]);
+                    if (reset) *reinterpret_cast<float2*>(cr32 + o) = make_float2(rf[0], rf[1]);
+                } else {
+                    r32[o] = rf[0];
+                    rh32[o] = rhf[0];
+                    if (reset) cr32[o] = rf[0];
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < V; q++) {
+                xw[q] = xc[q];
+                xc[q] = xe[q];
+            }
+        }
     }
     block_reduce<R_SUM, 3>(acc, smem);
     double s[3];
@@ -1559,13 +1625,13 @@ int refine_run(SolverWork<float>& wf, SolverWork<double>& wd, const Dims& d, dou
     a.itmax = itmax;
     a.tol = tol;
     a.sc_floor = 0.01;
-    a.nkt = (d.kp + BX - 1) / BX;  // scalar warp tasks of the FP64 residual
+    a.nkt = kchunks<double>(d);  // vector warp tasks of the FP64 residual
     a.max_updates = max_updates;
     a.max_cycle = 250;
     a.by = wf.by;
     a.tasks = wf.tasks;
     a.max_blocks = wf.max_blocks;
-    a.ni = 1;                      // the FP64 residual does not march
+    a.ni = 4;                      // planes a warp task of the FP64 residual marches over
     a.fuse = 0;
     no_cheb(a);
     SolverArgs af = a;             // vector warp tasks of the FP32 iterations
@@ -1581,7 +1647,7 @@ int refine_run(SolverWork<float>& wf, SolverWork<double>& wd, const Dims& d, dou
     const Coef<float> cf = coef_of(wf);
     static int gfull = 0;
     if (!gfull) gfull = persistent_grid(k_ru_residual<false>);
-    const int g = red_grid(a, gfull, a.nkt);
+    const int g = red_grid(a, gfull, a.nkt, a.ni);
     const dim3 gi = interior_grid(d, d.kp), bl(BX, BY);
     auto begin = [&](cudaStream_t s) {
         cudaMemsetAsync(dx, 0, d.n() * sizeof(float), s);
