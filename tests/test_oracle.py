@@ -109,6 +109,42 @@ def test_bicgstab_manufactured_solution(orc, g):
     assert np.max(np.abs(d)) < 1e-6 * np.max(np.abs(ps))
 
 
+@pytest.mark.parametrize("stretched", [False, True])
+def test_bicgstab_matches_independent_restatement(orc, g, stretched):
+    """The oracle's solve against an array-at-a-time numpy restatement of
+    set_mat_a, mat_ax, precondition, bicgstab and inn_prod
+    (tests/bicgstab_np.py): the same iterations and the same pressure, halo
+    included, bit for bit.  A warm start from a random x; on the stretched
+    grid every coefficient table varies along its axis."""
+    import dataclasses
+
+    import bicgstab_np
+
+    rng = np.random.default_rng(11)
+    if stretched:
+        def spacing(n, d):
+            return d * rng.uniform(0.7, 1.4, size=n + 2)
+        g = dataclasses.replace(g, dx=spacing(g.ip, 100.0), dxn=spacing(g.ip, 100.0),
+                                dy=spacing(g.jp, 100.0), dyn=spacing(g.jp, 100.0),
+                                dz=spacing(g.kp, 80.0), dzn=spacing(g.kp, 80.0))
+    o = orc.OracleCore(g)
+    kp, jp, ip = g.kp, g.jp, g.ip
+    X = 2 * np.pi * np.arange(ip + 2) / ip
+    Z = np.pi * (np.arange(kp + 2) - 0.5) / kp
+    ps = np.asfortranarray(np.cos(Z)[:, None, None] * np.sin(X)[None, None, :] *
+                           (1 + rng.uniform(-0.3, 0.3, size=(1, jp + 2, 1))))
+    b = fz(g)
+    o.mat_ax(ps.copy(order="F"), b)
+    x0 = rand_field(g, rng, -0.5, 0.5)
+    sw = rand_field(g, rng, -0.1, 0.1)
+    x_c, x_np = x0.copy(order="F"), x0.copy(order="F")
+    st, it, err = o.bicgstab(x_c, b.copy(order="F"), sw, 1e-10)
+    st2, it2, err2 = bicgstab_np.bicgstab(g, x_np, b.copy(order="F"), sw, 1e-10)
+    assert (st, it) == (st2, it2) and st == 0 and it > 5
+    assert err == err2
+    assert np.array_equal(x_c, x_np)
+
+
 def test_bicgstab_itmax_reports_noconv(orc, g):
     rng = np.random.default_rng(5)
     o = orc.OracleCore(g)
