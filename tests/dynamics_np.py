@@ -1,0 +1,80 @@
+"""Array-at-a-time numpy restatements of four routines of the reference's time
+step on one rank, independent checks of the oracle's C restatement:
+
+* advance_momentum (dynamics.f90:1019-1099);
+* divergence_calc (diagnostics.f90:120-153);
+* adv_ref_state (pamm/sfvt/advection_3d.F90:1148-1218);
+* first_order_upstream_3d (pamm/sfvt/advection_3d.F90:39-116).
+
+Arrays are a(0:kp+1, 0:jp+1, 0:ip+1) in Fortran order, 1-D metrics
+a(0:n+1).  Every expression keeps the reference's evaluation order (Fortran
+evaluates operators of equal precedence left to right), so the results are
+bit for bit the reference's arithmetic in IEEE double without fused
+multiply-adds.
+"""
+import numpy as np
+
+I = slice(1, -1)  # interior along an axis
+
+
+def _k(a):
+    """a 1-D metric over levels as a (n, 1, 1) column"""
+    return a[:, None, None]
+
+
+def advance_momentum(g, dt, u, v, w, zu, zv, zw, su, sv, sw, p):
+    """u, v, w at levels 0..kp of the interior columns, in place."""
+    kp = g.kp
+    K = slice(0, kp + 1)
+    rn = _k(g.rhoan[K])
+    u[K, I, I] = zu[K, I, I] + ((su[K, I, I] - (p[K, I, 2:] - p[K, I, I]) /
+                                 g.dxn[None, None, 1:-1]) * dt) / rn
+    v[K, I, I] = zv[K, I, I] + ((sv[K, I, I] - (p[K, 2:, I] - p[K, I, I]) /
+                                 g.dyn[None, 1:-1, None]) * dt) / rn
+    w[K, I, I] = zw[K, I, I] + ((sw[K, I, I] - (p[1:kp + 2, I, I] - p[K, I, I]) /
+                                 _k(g.dzn[K])) * dt) / _k(g.rhoa[K])
+
+
+def divergence_calc(g, u, v, w, div):
+    """div at the interior points, in place."""
+    rn = _k(g.rhoan[1:-1])
+    div[I, I, I] = (rn * (u[I, I, I] - u[I, I, :-2]) / g.dx[None, None, :-2] +
+                    rn * (v[I, I, I] - v[I, :-2, I]) / g.dy[None, :-2, None] +
+                    (_k(g.rhoa[1:-1]) * w[I, I, I] - _k(g.rhoa[:-2]) * w[:-2, I, I]) /
+                    _k(g.dz[:-2]))
+
+
+def adv_ref_state(g, dt, w, psi, psi_ref):
+    """psi at levels 1..kp of every column, halo columns included, in place."""
+    kp = g.kp
+    K, Km, Kp = slice(1, kp + 1), slice(0, kp), slice(2, kp + 2)
+    pr = psi_ref
+    psi[K] = psi[K] - dt * (0.5 / _k(g.dz[Km]) * w[Km] * _k(g.rhoa[Km]) * _k(pr[K] - pr[Km]) +
+                            0.5 / _k(g.dz[K]) * w[K] * _k(g.rhoa[K]) * _k(pr[Kp] - pr[K])) / \
+        _k(g.rhoan[K])
+
+
+def first_order_upstream_3d(g, dt, u, v, w, psi, neumann=0):
+    """Donor-cell update of psi at the interior points, in place."""
+    dxn = g.dxn[None, None, 1:-1]
+    dyn = g.dyn[None, 1:-1, None]
+    dzn, ra, rn = _k(g.dzn[1:-1]), _k(g.rhoa), _k(g.rhoan[1:-1])
+    c = psi[I, I, I]
+    uc, ul = u[I, I, I], u[I, I, :-2]
+    vc, vl = v[I, I, I], v[I, :-2, I]
+    wc, wl = w[I, I, I], w[:-2, I, I]
+    fx_r = ((uc + np.abs(uc)) * c + (uc - np.abs(uc)) * psi[I, I, 2:]) * dt / (2.0 * dxn)
+    fx_l = ((ul + np.abs(ul)) * psi[I, I, :-2] + (ul - np.abs(ul)) * c) * dt / (2.0 * dxn)
+    fy_r = ((vc + np.abs(vc)) * c + (vc - np.abs(vc)) * psi[I, 2:, I]) * dt / (2.0 * dyn)
+    fy_l = ((vl + np.abs(vl)) * psi[I, :-2, I] + (vl - np.abs(vl)) * c) * dt / (2.0 * dyn)
+    fz_r = ((wc + np.abs(wc)) * ra[1:-1] * c + (wc - np.abs(wc)) * ra[1:-1] * psi[2:, I, I]) * \
+        dt / (2.0 * dzn * rn)
+    fz_l = ((wl + np.abs(wl)) * ra[:-2] * psi[:-2, I, I] + (wl - np.abs(wl)) * ra[:-2] * c) * \
+        dt / (2.0 * dzn * rn)
+    if neumann == 1:
+        fz_l[0] = fz_r[0]
+        fz_r[-1] = fz_l[-1]
+    elif neumann == 2:
+        fz_l[0] = -fz_r[0]
+        fz_r[-1] = -fz_l[-1]
+    psi[I, I, I] = c - (fx_r - fx_l) - (fy_r - fy_l) - (fz_r - fz_l)
