@@ -1,10 +1,13 @@
-"""Array-at-a-time numpy restatements of four routines of the reference's time
+"""Array-at-a-time numpy restatements of five routines of the reference's time
 step on one rank, independent checks of the oracle's C restatement:
 
 * advance_momentum (dynamics.f90:1019-1099);
 * divergence_calc (diagnostics.f90:120-153);
 * adv_ref_state (pamm/sfvt/advection_3d.F90:1148-1218);
-* first_order_upstream_3d (pamm/sfvt/advection_3d.F90:39-116).
+* first_order_upstream_3d (pamm/sfvt/advection_3d.F90:39-116);
+* sources with viscous = .false. (dynamics.f90:639-1000): the centred
+  momentum sources and buoyancy, damping, forcing and subsidence, the
+  exchanges, the boundary rows and the Poisson right-hand side.
 
 Arrays are a(0:kp+1, 0:jp+1, 0:ip+1) in Fortran order, 1-D metrics
 a(0:n+1).  Every expression keeps the reference's evaluation order (Fortran
@@ -13,6 +16,10 @@ bit for bit the reference's arithmetic in IEEE double without fused
 multiply-adds.
 """
 import numpy as np
+
+from helpers import cases
+
+GRAV = 9.81  # dynamics.f90:18
 
 I = slice(1, -1)  # interior along an axis
 
@@ -78,3 +85,71 @@ def first_order_upstream_3d(g, dt, u, v, w, psi, neumann=0):
         fz_l[0] = -fz_r[0]
         fz_r[-1] = -fz_l[-1]
     psi[I, I, I] = c - (fx_r - fx_l) - (fy_r - fy_l) - (fz_r - fz_l)
+
+
+def sources(g, ubar, vbar, wbar, thbar, zu, zv, zw, u, v, w, th, su, sv, sw, sth, rhs,
+            forcing=None):
+    """su, sv, sw, sth and rhs in place (viscous = .false.)."""
+    kp = g.kp
+    K, Km, Kp = slice(1, kp + 1), slice(0, kp), slice(2, kp + 2)
+    J, Jm, Jp = I, slice(0, -2), slice(2, None)
+    Im, Ip = slice(0, -2), slice(2, None)
+    rn, ra = _k(g.rhoan[K]), _k(g.rhoa[K])
+    dx_i, dx_im = g.dx[None, None, I], g.dx[None, None, Im]
+    dxn_i, dxn_im = g.dxn[None, None, I], g.dxn[None, None, Im]
+    dy_j, dy_jm = g.dy[None, J, None], g.dy[None, Jm, None]
+    dyn_j, dyn_jm = g.dyn[None, J, None], g.dyn[None, Jm, None]
+    dz_k, dz_km = _k(g.dz[K]), _k(g.dz[Km])
+    dzn_k, dzn_km = _k(g.dzn[K]), _k(g.dzn[Km])
+    su[K, J, I] = rn * (
+        (u[K, J, Im] * (u[K, J, I] + u[K, J, Im]) - u[K, J, Ip] * (u[K, J, I] + u[K, J, Ip])) /
+        (2.0 * (dx_i + dx_im)) +
+        (u[K, Jm, I] * (v[K, Jm, I] + v[K, Jm, Ip]) - u[K, Jp, I] * (v[K, J, I] + v[K, J, Ip])) /
+        (2.0 * (dyn_j + dyn_jm)) +
+        (u[Km, J, I] * (w[Km, J, I] + w[Km, J, Ip]) - u[Kp, J, I] * (w[K, J, I] + w[K, J, Ip])) /
+        (2.0 * (dzn_k + dzn_km)))
+    sv[K, J, I] = rn * (
+        (v[K, J, Im] * (u[K, J, Im] + u[K, Jp, Im]) - v[K, J, Ip] * (u[K, J, I] + u[K, Jp, I])) /
+        (2.0 * (dxn_i + dxn_im)) +
+        (v[K, Jm, I] * (v[K, J, I] + v[K, Jm, I]) - v[K, Jp, I] * (v[K, J, I] + v[K, Jp, I])) /
+        (2.0 * (dy_j + dy_jm)) +
+        (v[Km, J, I] * (w[Km, J, I] + w[Km, Jp, I]) - v[Kp, J, I] * (w[K, J, I] + w[K, Jp, I])) /
+        (2.0 * (dzn_k + dzn_km)))
+    tb = thbar
+    sw[K, J, I] = ra * (
+        ((w[K, J, Im] * (u[K, J, Im] + u[Kp, J, Im]) - w[K, J, Ip] * (u[K, J, I] + u[Kp, J, I])) /
+         (2.0 * (dxn_i + dxn_im)) +
+         (w[K, Jm, I] * (v[K, Jm, I] + v[Kp, Jm, I]) - w[K, Jp, I] * (v[K, J, I] + v[Kp, J, I])) /
+         (2.0 * (dyn_j + dyn_jm)) +
+         (w[Km, J, I] * (w[K, J, I] + w[Km, J, I]) - w[Kp, J, I] * (w[K, J, I] + w[Kp, J, I])) /
+         (2.0 * (dz_k + dz_km))) +
+        GRAV * (th[K, J, I] + th[Kp, J, I]) /
+        (2.0 * _k(g.theta[K]) + _k(tb[K]) + _k(tb[Kp])))
+    f = forcing or {}
+    if f.get("damping_layer"):
+        dfn, df = _k(f["dampfacn"][K]), _k(f["dampfac"][K])
+        su[K, J, I] = su[K, J, I] + rn * dfn * (zu[K, J, I] - _k(ubar[K]))
+        sv[K, J, I] = sv[K, J, I] + rn * dfn * (zv[K, J, I] - _k(vbar[K]))
+        sw[K, J, I] = sw[K, J, I] + ra * df * (zw[K, J, I] - 0.0)
+        sth[K, J, I] = sth[K, J, I] + dfn * (th[K, J, I] - 0.0)
+    if f.get("forcing"):
+        tau = f.get("forcing_tau", 1.0)
+        su[K, J, I] = su[K, J, I] - rn * (zu[K, J, I] - _k(f["u_force"][K])) / tau
+        sv[K, J, I] = sv[K, J, I] - rn * (zv[K, J, I] - _k(f["v_force"][K])) / tau
+    if f.get("divergence"):
+        sw[K, J, I] = sw[K, J, I] - rn * (_k(wbar[K]) - _k(f["w_subs"][K]))
+    for a in (su, sv, sw, sth):
+        cases.exchange_full(a, 0.0, 0.0)
+    su[0] = -su[1]
+    sv[0] = -sv[1]
+    sw[0] = 0.0
+    sw[kp:kp + 2] = 0.0
+    su[kp:kp + 2] = 0.0
+    sv[kp:kp + 2] = 0.0
+    K1, K1m = slice(1, kp + 2), slice(0, kp + 1)
+    rhs[K1, J, I] = ((su[K1, J, I] - su[K1, J, Im]) / dx_im +
+                     (sv[K1, J, I] - sv[K1, Jm, I]) / dy_jm +
+                     (sw[K1, J, I] - sw[K1m, J, I]) / _k(g.dz[K1m]))
+    rhs[0, J, I] = ((su[0, J, I] - su[0, J, Im]) / g.dx[None, Im] +
+                    (sv[0, J, I] - sv[0, Jm, I]) / g.dy[Jm, None] +
+                    (sw[0, J, I] + sw[1, J, I]) / g.dz[1])

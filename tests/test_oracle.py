@@ -241,7 +241,8 @@ def _stretched(g, rng):
                                dy=spacing(g.jp, 100.0), dyn=spacing(g.jp, 100.0),
                                dz=spacing(g.kp, 80.0), dzn=spacing(g.kp, 80.0),
                                rhoa=rng.uniform(0.8, 1.2, size=g.kp + 2),
-                               rhoan=rng.uniform(0.8, 1.2, size=g.kp + 2))
+                               rhoan=rng.uniform(0.8, 1.2, size=g.kp + 2),
+                               theta=rng.uniform(295.0, 305.0, size=g.kp + 2))
 
 
 def test_step_routines_match_independent_restatement(orc, g):
@@ -308,3 +309,33 @@ def test_mpdata_matches_independent_restatement(orc, g, kord, monotone, neumann)
     assert np.array_equal(p1, p2) and not np.array_equal(p1, psi)
     for a, b in zip((u, v, w), winds):
         assert np.array_equal(a, b)  # the winds are inputs only
+
+
+@pytest.mark.parametrize("damping", [False, True])
+def test_sources_match_independent_restatement(orc, g, damping):
+    """sources with viscous = .false. against an array-at-a-time numpy
+    restatement (tests/dynamics_np.py), with damping, forcing and subsidence
+    off and on: su, sv, sw, sth and the Poisson right-hand side, halos and
+    rows included, bit for bit."""
+    import dynamics_np as dn
+
+    rng = np.random.default_rng(14 + damping)
+    g = _stretched(g, rng)
+    o = orc.OracleCore(g)
+    u, v, w = velocities(g, rng, 1.0)
+    th = rand_field(g, rng, -0.5, 2.0)
+    zu, zv, zw = (rand_field(g, rng) for _ in range(3))
+    K2 = g.kp + 2
+    bars = [rng.uniform(-1, 1, K2) for _ in range(4)]
+    forcing = None
+    if damping:
+        forcing = dict(damping_layer=1, forcing=1, divergence=1,
+                       dampfacn=rng.uniform(-0.01, 0, K2), dampfac=rng.uniform(-0.01, 0, K2),
+                       u_force=rng.uniform(-1, 1, K2), v_force=rng.uniform(-1, 1, K2),
+                       w_subs=rng.uniform(-0.01, 0.01, K2), forcing_tau=600.0)
+    outs = [rand_field(g, rng) for _ in range(5)]  # su sv sw sth rhs (inout)
+    outs2 = [a.copy(order="F") for a in outs]
+    o.sources(*bars, zu, zv, zw, u, v, w, th, *outs, forcing=forcing)
+    dn.sources(g, *bars, zu, zv, zw, u, v, w, th, *outs2, forcing=forcing)
+    for name, x, y in zip(("su", "sv", "sw", "sth", "rhs"), outs, outs2):
+        assert np.array_equal(x, y), name
