@@ -339,3 +339,25 @@ def test_sources_match_independent_restatement(orc, g, damping):
     dn.sources(g, *bars, zu, zv, zw, u, v, w, th, *outs2, forcing=forcing)
     for name, x, y in zip(("su", "sv", "sw", "sth", "rhs"), outs, outs2):
         assert np.array_equal(x, y), name
+
+
+def test_driver_step_matches_independent_restatement(orc):
+    """Three dry time steps of the oracle's model_driver (every phase of the
+    u, zu, tu rotation) against the numpy restatement of the step
+    (tests/driver_np.py), which chains the numpy restatements of its
+    routines: every field, role and level mean, halos included, bit for
+    bit, and the same iterations."""
+    import driver_np
+
+    c = small_bubble(ip=12, jp=10, kp=8)
+    m = orc.OracleModel(c.grid, c.state, c.dt, ptol=c.ptol, kord=c.kord, monotone=c.monotone)
+    d = driver_np.Driver(c.grid, c.state, c.dt, ptol=c.ptol, kord=c.kord, monotone=c.monotone)
+    m.driver_start()
+    d.start()
+    for n in range(3):
+        it, err = m.step(1)
+        d.step()
+        assert (it, err) == (d.iters, d.err), n
+        a, b = m.fields(), d.fields()
+        for name in b:
+            assert np.array_equal(a[name], b[name]), (n, name)
