@@ -1,6 +1,6 @@
 """Array-at-a-time numpy restatement of the reference's mpdata_3d
-(pamm/sfvt/advection_3d.F90:219-714) on one rank, an independent check of
-the oracle's C restatement:
+(pamm/sfvt/advection_3d.F90:219-714) and mpdata_vec_3d (:1250-1753) on one
+rank, an independent check of the oracle's C restatement:
 
 * the positive-definite shift by the global minimum (:271-285);
 * for each pass after the first, the antidiffusive velocities of the
@@ -10,7 +10,10 @@ the oracle's C restatement:
   eqs. 18-20), whose bounds also take the field as it was at entry (the copy
   psi_store);
 * the donor-cell pass (first_order_upstream_3d) and exchange_full of the
-  field after every pass (:683-700).
+  field after every pass (:683-700);
+* mpdata_vec_3d: the same passes with the velocities and bounds of the
+  category's first field, the donor cell and the exchange for every field,
+  and a shift per field by the minimum of its interior.
 
 Every expression keeps the reference's parenthesisation and left-to-right
 evaluation, so the result is bit for bit the reference's arithmetic in IEEE
@@ -166,21 +169,15 @@ def _limited(g, dt, ut, vt, wt, psi, po, us, vs, ws):
                    m3(one, bu[K, J, I], bd[Kp, J, I]) * mn(wt[K, J, I], 0.0))
 
 
-def mpdata_3d(g, dt, u, v, w, psi_in, lbc, ubc, kord, monotone, neumann=0):
-    """psi_in advanced in place; returns the shifted-back (lbc, ubc)."""
-    kp, jp, ip = g.kp, g.jp, g.ip
-    mn = min(float(psi_in.min()), lbc, ubc)
-    psi_in -= mn
-    lbc -= mn
-    ubc -= mn
-    if float(np.sum(psi_in[1:kp + 1, 1:jp + 1, 1:ip + 1])) < SMALL:
-        psi_in += mn
-        return lbc + mn, ubc + mn
+def _mpdata(g, dt, u, v, w, fields, kord, monotone, neumann, bcs):
+    """The passes of mpdata_3d / mpdata_vec_3d on shifted fields: the
+    antidiffusive velocities and the limiter from fields[0], the donor cell
+    and the exchange of every field with its (lbc, ubc) in bcs."""
     s1 = [np.zeros_like(u, order="F") for _ in range(3)]
     s2 = [np.zeros_like(u, order="F") for _ in range(3)]
     vel, sav = [u, v, w], s1
-    psi = psi_in.copy(order="F") if kord > 1 else None
-    po = psi_in
+    psi = fields[0].copy(order="F") if kord > 1 else None
+    po = fields[0]
     it2 = 0
     for it in range(1, kord + 1):
         if it > 1:
@@ -195,8 +192,42 @@ def mpdata_3d(g, dt, u, v, w, psi_in, lbc, ubc, kord, monotone, neumann=0):
             vel, sav = s2, s1
             for a in vel:
                 cases.exchange_full(a, 0.0, 0.0)
-        dynamics_np.first_order_upstream_3d(g, dt, *vel, po, neumann)
-        if it <= kord and kord >= 1:
-            cases.exchange_full(po, lbc, ubc)
+        for f, (lb, ub) in zip(fields, bcs):
+            dynamics_np.first_order_upstream_3d(g, dt, *vel, f, neumann)
+            if it <= kord and kord >= 1:
+                cases.exchange_full(f, lb, ub)
+
+
+def mpdata_3d(g, dt, u, v, w, psi_in, lbc, ubc, kord, monotone, neumann=0):
+    """psi_in advanced in place; returns the shifted-back (lbc, ubc)."""
+    kp, jp, ip = g.kp, g.jp, g.ip
+    mn = min(float(psi_in.min()), lbc, ubc)  # the whole array, halo included (:271)
+    psi_in -= mn
+    lbc -= mn
+    ubc -= mn
+    if float(np.sum(psi_in[1:kp + 1, 1:jp + 1, 1:ip + 1])) >= SMALL:
+        _mpdata(g, dt, u, v, w, [psi_in], kord, monotone, neumann, [(lbc, ubc)])
     psi_in += mn
     return lbc + mn, ubc + mn
+
+
+def mpdata_vec_3d(g, dt, u, v, w, fields, lbc, ubc, kord, monotone, neumann=0):
+    """mpdata_vec_3d (advection_3d.F90:1250-1753): the fields of one category
+    advanced in place with the velocities of the first; lbc, ubc (arrays)
+    updated in place.  Each field is shifted by the minimum of its interior
+    and its boundary values (:1299-1306)."""
+    kp, jp, ip = g.kp, g.jp, g.ip
+    mins = []
+    for n, f in enumerate(fields):
+        mn = min(float(f[1:kp + 1, 1:jp + 1, 1:ip + 1].min()), lbc[n], ubc[n])
+        f -= mn
+        lbc[n] -= mn
+        ubc[n] -= mn
+        mins.append(mn)
+    if float(np.sum(fields[0][1:kp + 1, 1:jp + 1, 1:ip + 1])) >= SMALL:
+        _mpdata(g, dt, u, v, w, fields, kord, monotone, neumann,
+                [(lbc[n], ubc[n]) for n in range(len(fields))])
+    for n, f in enumerate(fields):
+        f += mins[n]
+        lbc[n] += mins[n]
+        ubc[n] += mins[n]

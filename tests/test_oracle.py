@@ -361,3 +361,28 @@ def test_driver_step_matches_independent_restatement(orc):
         a, b = m.fields(), d.fields()
         for name in b:
             assert np.array_equal(a[name], b[name]), (n, name)
+
+
+@pytest.mark.parametrize("kord,monotone", [(2, False), (3, True)])
+def test_mpdata_vec_matches_independent_restatement(orc, g, kord, monotone):
+    """mpdata_vec_3d (a category of 3 fields advected with the velocities and
+    bounds of its first) against the numpy restatement
+    (tests/mpdata_np.py): every field, halo included, and the boundary
+    values, bit for bit."""
+    import mpdata_np
+
+    rng = np.random.default_rng(31 + kord)
+    g = _stretched(g, rng)
+    o = orc.OracleCore(g)
+    u, v, w = velocities(g, rng, 0.4)
+    fields = [rand_field(g, rng, lo, 2.0) for lo in (-0.5, 0.0, 1.0)]
+    stack = orc._fortran_stack(fields)
+    mine = [f.copy(order="F") for f in fields]
+    lb1, ub1 = np.array([0.3, 0.0, 1.5]), np.array([-0.7, 0.2, 1.1])
+    lb2, ub2 = lb1.copy(), ub1.copy()
+    o.mpdata_vec_3d(0.8, u, v, w, stack, lb1, ub1, kord, monotone)
+    mpdata_np.mpdata_vec_3d(g, 0.8, u, v, w, mine, lb2, ub2, kord, monotone)
+    assert np.array_equal(lb1, lb2) and np.array_equal(ub1, ub2)
+    for q in range(3):
+        assert np.array_equal(stack[q], mine[q]), q
+        assert not np.array_equal(mine[q], fields[q]), q
