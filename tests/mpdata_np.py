@@ -231,3 +231,12 @@ def mpdata_vec_3d(g, dt, u, v, w, fields, lbc, ubc, kord, monotone, neumann=0):
         f += mins[n]
         lbc[n] += mins[n]
         ubc[n] += mins[n]
+
+
+def mpdata_3d_add(g, dt, u, v, w, psi_in, psi_1d, lbc, ubc, kord, monotone, neumann=0):
+    """mpdata_3d_add (advection_3d.F90:139-190): psi_1d(k) added to every level
+    of the field (halo included), mpdata_3d, and subtracted again."""
+    psi_in += psi_1d[:, None, None]
+    lbc, ubc = mpdata_3d(g, dt, u, v, w, psi_in, lbc, ubc, kord, monotone, neumann)
+    psi_in -= psi_1d[:, None, None]
+    return lbc, ubc
