@@ -2,12 +2,14 @@
 (driver_code.f90:280-295 and 304-676), chaining the numpy restatements of its
 routines; an independent check of the oracle's step.
 
-Per step n (advection_scheme = 1, moisture, radiation, land surface, the
-subgrid model and the forcings off):
+Per step n (advection_scheme = 1; radiation, land surface, the subgrid
+model, the forcings and the microphysics off; passive q categories
+optional):
   sth = 0; horizontal_means; divergence_calc; sources;
   exchange_along_dim_wo(psrc); bicgstab(p, psrc); exchange_along_dim_wo(p);
   adv_ref_state(th) + exchange_full(th, 0, 0); mpdata_3d(th, t1, t2);
-  advance_momentum(2 dt, tu, tv, tw); advance_scalar_fields_3d(th);
+  mpdata_vec_3d of each q category (with sq = 0);
+  advance_momentum(2 dt, tu, tv, tw); advance_scalar_fields_3d(th, q);
   the 0.99 / 0.01 filter of u and zu; the rotation of the u, zu, tu roles by
   n mod 3; exchange_full(u, v, w, 0, 0) and the velocity rows.
 horizontal_means forms every level's mean (the reference's Allreduce count
@@ -43,8 +45,11 @@ def horizontal_means(a):
 
 
 class Driver:
-    def __init__(self, g, state, dt, ptol=1e-10, kord=3, monotone=True):
+    def __init__(self, g, state, dt, ptol=1e-10, kord=3, monotone=True, c_s=(), c_e=()):
         self.g, self.dt, self.ptol, self.kord, self.monotone = g, dt, ptol, kord, monotone
+        self.cats = list(zip(c_s, c_e))
+        self.q = [np.asfortranarray(a).copy(order="F") for a in state.q] if c_s else []
+        self.q1, self.q2 = np.zeros(len(self.q)), np.zeros(len(self.q))
         sh = g.shape
         self.buf = {n: np.asfortranarray(getattr(state, n)).copy(order="F")
                     for n in ("u", "v", "w", "zu", "zv", "zw", "tu", "tv", "tw")}
@@ -94,9 +99,14 @@ class Driver:
         cases.exchange_full(self.th, 0.0, 0.0)
         self.t1, self.t2 = mpdata_np.mpdata_3d(g, dt, u, v, w, self.th, self.t1, self.t2,
                                                self.kord, self.monotone, 0)
+        for cs, ce in self.cats:  # driver_code.f90:577-597
+            mpdata_np.mpdata_vec_3d(g, dt, u, v, w, self.q[cs - 1:ce], self.q1[cs - 1:ce],
+                                    self.q2[cs - 1:ce], self.kord, self.monotone, 0)
         dynamics_np.advance_momentum(g, 2.0 * dt, tu, tv, tw, zu, zv, zw, self.su, self.sv,
                                      self.sw, self.p)
         self.th[...] = self.th + self.sth * dt
+        for a in self.q:  # sq = 0: the driver zeroes it and nothing adds to it here
+            a[...] = a + 0.0 * dt
         for a, za in ((u, zu), (v, zv), (w, zw)):
             tmp = 0.99 * a + 0.01 * za
             za[...] = 0.01 * a + 0.99 * za
@@ -129,4 +139,6 @@ class Driver:
             out[n] = getattr(self, n)
         for n, a in zip(("ubar", "vbar", "wbar", "thbar"), self.bars):
             out[n] = a
+        if self.q:
+            out["q"] = self.q
         return out
