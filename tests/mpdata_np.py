@@ -169,7 +169,55 @@ def _limited(g, dt, ut, vt, wt, psi, po, us, vs, ws):
                    m3(one, bu[K, J, I], bd[Kp, J, I]) * mn(wt[K, J, I], 0.0))
 
 
-def _mpdata(g, dt, u, v, w, fields, kord, monotone, neumann, bcs):
+def _limited_sfvt(g, dt, ut, vt, wt, psi, po, us, vs, ws):
+    """The limiter variant of sfvt/advection_3d.F90:544-704: bounds per
+    direction from the three cells along it, no density weights, and
+    dx(i-1), dy(j-1), dz(k-1) in the denominators."""
+    kp = g.kp
+    K, Km, Kp = slice(1, kp + 1), slice(0, kp), slice(2, kp + 2)
+    J, Jm, Jp = slice(1, -1), slice(0, -2), slice(2, None)
+    I, Im, Ip = slice(1, -1), slice(0, -2), slice(2, None)
+    mx, mn = np.maximum, np.minimum
+
+    def bounds(a, b, c):
+        vals = [psi[a], psi[b], psi[c], po[a], po[b], po[c]]
+        return np.maximum.reduce(vals), np.minimum.reduce(vals)
+    C = (K, J, I)
+    imax, imin = bounds((K, J, Im), C, (K, J, Ip))
+    jmax, jmin = bounds((K, Jm, I), C, (K, Jp, I))
+    kmax, kmin = bounds((Km, J, I), C, (Kp, J, I))
+    dx, dy, dz = g.dx[None, None, Im], g.dy[None, Jm, None], _k(g.dz[Km])
+    p0 = po[C]
+    denom1 = (dt * ((mx(ut[K, J, Im], 0.0) * po[K, J, Im] - mn(ut[C], 0.0) * po[K, J, Ip]) / dx +
+                    (mx(vt[K, Jm, I], 0.0) * po[K, Jm, I] - mn(vt[C], 0.0) * po[K, Jp, I]) / dy +
+                    (mx(wt[Km, J, I], 0.0) * po[Km, J, I] - mn(wt[C], 0.0) * po[Kp, J, I]) / dz +
+                    SMALL))
+    denom2 = (dt * ((mx(ut[C], 0.0) * p0 - mn(ut[K, J, Im], 0.0) * p0) / dx +
+                    (mx(vt[C], 0.0) * p0 - mn(vt[K, Jm, I], 0.0) * p0) / dy +
+                    (mx(wt[C], 0.0) * p0 - mn(wt[Km, J, I], 0.0) * p0) / dz +
+                    SMALL))
+    beta = {}
+    for name, hi, lo in (("i", imax, imin), ("j", jmax, jmin), ("k", kmax, kmin)):
+        up = np.zeros_like(po, order="F")
+        down = np.zeros_like(po, order="F")
+        up[C] = (hi - p0) / denom1
+        down[C] = (p0 - lo) / denom2
+        bicgstab_np.exchange_along_dim(up, 0.0, 0.0)
+        bicgstab_np.exchange_along_dim(down, 0.0, 0.0)
+        beta[name] = (up, down)
+
+    def m3(a, b, c):
+        return np.minimum(np.minimum(a, b), c)
+    (iu, idn), (ju, jdn), (ku, kdn) = beta["i"], beta["j"], beta["k"]
+    us[C] = (m3(1.0, idn[C], iu[K, J, Ip]) * mx(ut[C], 0.0) +
+             m3(1.0, iu[C], idn[K, J, Ip]) * mn(ut[C], 0.0))
+    vs[C] = (m3(1.0, jdn[C], ju[K, Jp, I]) * mx(vt[C], 0.0) +
+             m3(1.0, ju[C], jdn[K, Jp, I]) * mn(vt[C], 0.0))
+    ws[C] = (m3(1.0, kdn[C], ku[Kp, J, I]) * mx(wt[C], 0.0) +
+             m3(1.0, ku[C], kdn[Kp, J, I]) * mn(wt[C], 0.0))
+
+
+def _mpdata(g, dt, u, v, w, fields, kord, monotone, neumann, bcs, limiter=0):
     """The passes of mpdata_3d / mpdata_vec_3d on shifted fields: the
     antidiffusive velocities and the limiter from fields[0], the donor cell
     and the exchange of every field with its (lbc, ubc) in bcs."""
@@ -188,7 +236,7 @@ def _mpdata(g, dt, u, v, w, fields, kord, monotone, neumann, bcs):
                 cases.exchange_full(a, 0.0, 0.0)
         if it > 1 and monotone:
             it2 += 1
-            _limited(g, dt, *vel, psi, po, *sav)
+            (_limited_sfvt if limiter else _limited)(g, dt, *vel, psi, po, *sav)
             vel, sav = s2, s1
             for a in vel:
                 cases.exchange_full(a, 0.0, 0.0)
@@ -198,15 +246,16 @@ def _mpdata(g, dt, u, v, w, fields, kord, monotone, neumann, bcs):
                 cases.exchange_full(f, lb, ub)
 
 
-def mpdata_3d(g, dt, u, v, w, psi_in, lbc, ubc, kord, monotone, neumann=0):
-    """psi_in advanced in place; returns the shifted-back (lbc, ubc)."""
+def mpdata_3d(g, dt, u, v, w, psi_in, lbc, ubc, kord, monotone, neumann=0, limiter=0):
+    """psi_in advanced in place; returns the shifted-back (lbc, ubc).
+    limiter = 1 takes the sfvt/ variant of the FCT limiter."""
     kp, jp, ip = g.kp, g.jp, g.ip
     mn = min(float(psi_in.min()), lbc, ubc)  # the whole array, halo included (:271)
     psi_in -= mn
     lbc -= mn
     ubc -= mn
     if float(np.sum(psi_in[1:kp + 1, 1:jp + 1, 1:ip + 1])) >= SMALL:
-        _mpdata(g, dt, u, v, w, [psi_in], kord, monotone, neumann, [(lbc, ubc)])
+        _mpdata(g, dt, u, v, w, [psi_in], kord, monotone, neumann, [(lbc, ubc)], limiter)
     psi_in += mn
     return lbc + mn, ubc + mn
 

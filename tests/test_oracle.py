@@ -287,24 +287,27 @@ def test_step_routines_match_independent_restatement(orc, g):
         assert np.array_equal(q1, q2) and not np.array_equal(q1, q0), neumann
 
 
-@pytest.mark.parametrize("kord,monotone,neumann", [(1, False, 0), (2, False, 0), (3, False, 1),
-                                                   (2, True, 0), (3, True, 0), (3, True, 2)])
-def test_mpdata_matches_independent_restatement(orc, g, kord, monotone, neumann):
+@pytest.mark.parametrize("kord,monotone,neumann,limiter",
+                         [(1, False, 0, 0), (2, False, 0, 0), (3, False, 1, 0), (2, True, 0, 0),
+                          (3, True, 0, 0), (3, True, 2, 0), (2, True, 0, 1), (3, True, 1, 1)])
+def test_mpdata_matches_independent_restatement(orc, g, kord, monotone, neumann, limiter):
     """mpdata_3d against an array-at-a-time numpy restatement
     (tests/mpdata_np.py): the advected field, halo included, and the shifted
     boundary values, bit for bit, on a grid with varying spacings and
     densities and with random winds (halos included)."""
     import mpdata_np
 
-    rng = np.random.default_rng(13 + kord + 10 * neumann + (100 if monotone else 0))
+    rng = np.random.default_rng(13 + kord + 10 * neumann + (100 if monotone else 0) +
+                                1000 * limiter)
     g = _stretched(g, rng)
     o = orc.OracleCore(g)
     u, v, w = velocities(g, rng, 0.4)
     psi = rand_field(g, rng, -0.5, 2.0)
     p1, p2 = psi.copy(order="F"), psi.copy(order="F")
     winds = [a.copy(order="F") for a in (u, v, w)]
-    lb1, ub1 = o.mpdata_3d(0.8, u, v, w, p1, 0.3, -0.7, kord, monotone, neumann)
-    lb2, ub2 = mpdata_np.mpdata_3d(g, 0.8, u, v, w, p2, 0.3, -0.7, kord, monotone, neumann)
+    lb1, ub1 = o.mpdata_3d(0.8, u, v, w, p1, 0.3, -0.7, kord, monotone, neumann, limiter)
+    lb2, ub2 = mpdata_np.mpdata_3d(g, 0.8, u, v, w, p2, 0.3, -0.7, kord, monotone, neumann,
+                                   limiter)
     assert (lb1, ub1) == (lb2, ub2)
     assert np.array_equal(p1, p2) and not np.array_equal(p1, psi)
     for a, b in zip((u, v, w), winds):
