@@ -39,6 +39,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <mutex>
 #include <type_traits>
 
 #include "dcm_internal.h"
@@ -936,12 +937,13 @@ static Coef<T> coef_of(const SolverWork<T>& w) {
 }
 
 static int sm_count() {
-    static int sms = 0;
-    if (!sms) {
-        int dev = 0;
+    // function-local statics are initialised once, thread-safely
+    static const int sms = [] {
+        int dev = 0, n = 0;
         cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    }
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        return n;
+    }();
     return sms;
 }
 
@@ -996,8 +998,7 @@ static void sten(const SolverArgs& a, const Coef<T>& c, const SolverBufs& B, Sol
     ProfScope ps(cat, st);
     constexpr bool RED = OP == OP_SETUP || OP == OP_MATC || OP == OP_MATP;
     if (RED) {
-        static int full = 0;
-        if (!full) full = persistent_grid(k_sten<T, OP, MODE>);
+        static const int full = persistent_grid(k_sten<T, OP, MODE>);
         launch(a.pdl, k_sten<T, OP, MODE>, dim3(red_grid(a, full, a.nkt, 1)), dim3(BX, BY), 0,
                st, a, c, B, w.red, w.S);
     } else {
@@ -1048,11 +1049,8 @@ void solver_init() {
     cudaFuncSetAttribute(k_precond3<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
     cudaFuncSetAttribute(k_precond3<0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
     cudaFuncSetAttribute(k_precond3<1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-    static bool probed = false;
-    if (!probed) {
-        probed = true;
-        g_pdl_graphs = probe_pdl_graphs() ? 1 : 0;
-    }
+    static std::once_flag probed;  // handles may be created from several threads
+    std::call_once(probed, [] { g_pdl_graphs = probe_pdl_graphs() ? 1 : 0; });
 }
 
 bool solver_pdl_available() { return g_pdl_graphs != 0; }
@@ -1118,8 +1116,7 @@ static void launch_iteration(const SolverArgs& a, const Coef<T>& c, SolverWork<T
     // phase D
     {
         ProfScope ps(P_UPDATE, st);
-        static int full = 0;
-        if (!full) full = persistent_grid(k_bicg_update<T>);
+        static const int full = persistent_grid(k_bicg_update<T>);
         launch(a.pdl, k_bicg_update<T>, dim3(red_grid(a, full, a.nkt)), dim3(BX, BY), 0, st, a,
                c, x, (const T*)w.p, (const T*)w.sA, w.r, (const T*)w.v1, (const T*)w.t,
                (const T*)w.cr, w.rh, w.red, w.S);
@@ -1645,8 +1642,7 @@ int refine_run(SolverWork<float>& wf, SolverWork<double>& wd, const Dims& d, dou
     Coef<double> cd;
     cd.ae = wd.ae; cd.aw = wd.aw; cd.an = wd.an; cd.as = wd.as; cd.au = wd.au; cd.ad = wd.ad;
     const Coef<float> cf = coef_of(wf);
-    static int gfull = 0;
-    if (!gfull) gfull = persistent_grid(k_ru_residual<false>);
+    static const int gfull = persistent_grid(k_ru_residual<false>);
     const int g = red_grid(a, gfull, a.nkt, a.ni);
     const dim3 gi = interior_grid(d, d.kp), bl(BX, BY);
     auto begin = [&](cudaStream_t s) {
