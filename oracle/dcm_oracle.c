@@ -5,6 +5,11 @@
  * TEST INFRASTRUCTURE ONLY (the checker and the timed CPU baseline).  The
  * product never links it.  PARITY UNPINNED: the Fortran reference cannot be
  * compiled in this image and ships no golden vectors; see dcm_oracle.h.
+ * Instead, independent numpy restatements of the same Fortran, array
+ * statement by array statement (tests/*_np.py), agree with this file bit
+ * for bit: the pressure solve, sources, advance_momentum, divergence_calc,
+ * adv_ref_state, the donor cell, the three MPDATA entry points with both
+ * limiters, and the whole dry time step of model_driver (tests/test_oracle.py).
  *
  * Every routine restates one reference routine statement by statement, in
  * the reference's evaluation order (Fortran evaluates a+b+c and a*b/c left to
