@@ -6,7 +6,7 @@
  * product never links it.  PARITY UNPINNED: the Fortran reference cannot be
  * compiled in this image and ships no golden vectors; see dcm_oracle.h.
  * Instead, independent numpy restatements of the same Fortran, array
- * statement by array statement (tests/*_np.py), agree with this file bit
+ * statement by array statement (the tests/..._np.py files), agree with this file bit
  * for bit: the pressure solve, sources, advance_momentum, divergence_calc,
  * adv_ref_state, the donor cell, the three MPDATA entry points with both
  * limiters, and the whole dry time step of model_driver (tests/test_oracle.py).
