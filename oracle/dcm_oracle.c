@@ -9,7 +9,8 @@
  * statement by array statement (the tests/..._np.py files), agree with this file bit
  * for bit: the pressure solve, sources, advance_momentum, divergence_calc,
  * adv_ref_state, the donor cell, the three MPDATA entry points with both
- * limiters, and the whole dry time step of model_driver (tests/test_oracle.py).
+ * limiters, the subgrid model (dcm_oracle_sgm.c) and the whole dry time step
+ * of model_driver (tests/test_oracle.py).
  *
  * Every routine restates one reference routine statement by statement, in
  * the reference's evaluation order (Fortran evaluates a+b+c and a*b/c left to

@@ -2,7 +2,16 @@
 (sgm/subgrid_3d.f90:38-493), written array-at-a-time, used only to
 cross-check the C restatement in oracle/.  Fields are a[k, j, i] with halo 1
 (shape (kp+2, jp+2, ip+2)); 1-D metrics are halo-inclusive."""
+import math
+
 import numpy as np
+
+_pow_c = np.frompyfunc(math.pow, 2, 1)
+
+
+def _pow(x, e):
+    """x**e elementwise by the C library's pow"""
+    return _pow_c(x, e).astype(np.float64)
 
 PRN, SUBB, SUBC, SUBG, SUBH, SUBR, RIC = 0.95, 40.0, 16.0, 1.2, 0.0, 4.0, 0.25
 GRAV, SMALL, KVON = 9.81, 1.e-10, 0.4
@@ -97,10 +106,12 @@ def subgrid(g, lamsq, z0, z0th, u, v, w, zu, zv, zw, th, vism, vist, strain, tau
     fh = np.zeros_like(rip)
     neg = rip < 0.0
     mid = (rip >= 0.0) & (rip < RIC)
-    fm[neg] = np.sqrt(1.0 - SUBC * rip[neg])
-    fh[neg] = SUBA * np.sqrt(1.0 - SUBB * rip[neg])
-    fm[mid] = (1.0 - rip[mid] / RIC) ** SUBR * (1.0 - SUBH * rip[mid])
-    fh[mid] = SUBF * (1.0 - rip[mid] / RIC) ** SUBR * (1.0 - SUBG * rip[mid])
+    # real exponents (**0.5, **SUBR) through the C library's pow, as compiled
+    # Fortran evaluates them (numpy's vectorised power may differ by an ulp)
+    fm[neg] = _pow(1.0 - SUBC * rip[neg], 0.5)
+    fh[neg] = SUBA * _pow(1.0 - SUBB * rip[neg], 0.5)
+    fm[mid] = _pow(1.0 - rip[mid] / RIC, SUBR) * (1.0 - SUBH * rip[mid])
+    fh[mid] = SUBF * _pow(1.0 - rip[mid] / RIC, SUBR) * (1.0 - SUBG * rip[mid])
     vism[K, J, I] = mk(lamsq) * np.sqrt(t) * fm
     vist[K, J, I] = mk(lamsq) * np.sqrt(t) * fh * mk(g.rhoa)
     vism[kp - 1:kp + 1] = 0.0
@@ -111,7 +122,7 @@ def subgrid(g, lamsq, z0, z0th, u, v, w, zu, zv, zw, th, vism, vist, strain, tau
     vmag = 0.5 * np.sqrt((u1[J, I] + u1[J, 0:ip]) ** 2 + (v1[J, I] + v1[0:jp, I]) ** 2) + SMALL
     dth = th1[J, I] + g.thetan[1] - g.theta[0]
     rib = GRAV * dth * (z1 - z0) ** 2 / (g.theta[0] * vmag ** 2 * (z1 - z0th))
-    lg = np.log(z1 / z0)
+    lg = math.log(z1 / z0)
     kv2 = KVON ** 2
     gm = np.where(rib <= 0.0,
                   1.0 - 9.4 * rib / (1.0 + 70.0 * kv2 * np.sqrt(np.abs(rib * z1 / z0)) / lg ** 2),
