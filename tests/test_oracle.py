@@ -156,12 +156,18 @@ def test_bicgstab_itmax_reports_noconv(orc, g):
 
 
 def test_horizontal_means_match_numpy(orc, g):
+    """Level means against numpy: to round-off against numpy's own mean, and
+    bit for bit against the reference's sequential sum
+    (driver_np.horizontal_means)."""
+    import driver_np
+
     rng = np.random.default_rng(6)
     f = [rand_field(g, rng) for _ in range(4)]
     bars = orc.OracleCore(g).horizontal_means(*f)
     for a, bar in zip(f, bars[:4]):
         ref = a[:, 1:-1, 1:-1].mean(axis=(1, 2))
         assert relerr(bar, ref) < 1e-14
+        assert np.array_equal(bar, driver_np.horizontal_means(a))
 
 
 def test_step_projection_is_divergence_free(orc):
