@@ -2,8 +2,8 @@
 (driver_code.f90:280-295 and 304-676), chaining the numpy restatements of its
 routines; an independent check of the oracle's step.
 
-Per step n (advection_scheme = 1; radiation, land surface, the subgrid
-model, the forcings and the microphysics off; passive q categories
+Per step n (advection_scheme = 1; radiation, land surface, the forcings
+and the microphysics off; passive q categories and the subgrid model
 optional):
   sth = 0; horizontal_means; divergence_calc; sources;
   exchange_along_dim_wo(psrc); bicgstab(p, psrc); exchange_along_dim_wo(p);
@@ -45,8 +45,15 @@ def horizontal_means(a):
 
 
 class Driver:
-    def __init__(self, g, state, dt, ptol=1e-10, kord=3, monotone=True, c_s=(), c_e=()):
+    def __init__(self, g, state, dt, ptol=1e-10, kord=3, monotone=True, c_s=(), c_e=(),
+                 viscous=None):
         self.g, self.dt, self.ptol, self.kord, self.monotone = g, dt, ptol, kord, monotone
+        # viscous = dict(lamsq, z0, z0th): the subgrid model inside sources, with
+        # vism, vist and strain kept between steps
+        self.viscous = None
+        if viscous:
+            self.viscous = dict(viscous, **{n: np.zeros(g.shape, order="F")
+                                           for n in ("vism", "vist", "strain")})
         self.cats = list(zip(c_s, c_e))
         self.q = [np.asfortranarray(a).copy(order="F") for a in state.q] if c_s else []
         self.q1, self.q2 = np.zeros(len(self.q)), np.zeros(len(self.q))
@@ -89,7 +96,7 @@ class Driver:
         self.bars = [horizontal_means(a) for a in (u, v, w, self.th)]
         dynamics_np.divergence_calc(g, u, v, w, self.div)
         dynamics_np.sources(g, *self.bars, zu, zv, zw, u, v, w, self.th, self.su, self.sv,
-                            self.sw, self.sth, self.psrc)
+                            self.sw, self.sth, self.psrc, viscous=self.viscous)
         exchange_along_dim_wo(self.psrc)
         st, self.iters, self.err = bicgstab_np.bicgstab(g, self.p, self.psrc, self.sw,
                                                         self.ptol)
@@ -141,4 +148,7 @@ class Driver:
             out[n] = a
         if self.q:
             out["q"] = self.q
+        if self.viscous:
+            for n in ("vism", "vist", "strain"):
+                out[n] = self.viscous[n]
         return out

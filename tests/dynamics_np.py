@@ -5,9 +5,10 @@ step on one rank, independent checks of the oracle's C restatement:
 * divergence_calc (diagnostics.f90:120-153);
 * adv_ref_state (pamm/sfvt/advection_3d.F90:1148-1218);
 * first_order_upstream_3d (pamm/sfvt/advection_3d.F90:39-116);
-* sources with viscous = .false. (dynamics.f90:639-1000): the centred
-  momentum sources and buoyancy, damping, forcing and subsidence, the
-  exchanges, the boundary rows and the Poisson right-hand side.
+* sources (dynamics.f90:639-1000): the centred momentum sources and
+  buoyancy, damping, forcing and subsidence, the exchanges (or, with
+  viscous = .true., the subgrid model), the boundary rows and the Poisson
+  right-hand side.
 
 Arrays are a(0:kp+1, 0:jp+1, 0:ip+1) in Fortran order, 1-D metrics
 a(0:n+1).  Every expression keeps the reference's evaluation order (Fortran
@@ -88,8 +89,11 @@ def first_order_upstream_3d(g, dt, u, v, w, psi, neumann=0):
 
 
 def sources(g, ubar, vbar, wbar, thbar, zu, zv, zw, u, v, w, th, su, sv, sw, sth, rhs,
-            forcing=None):
-    """su, sv, sw, sth and rhs in place (viscous = .false.)."""
+            forcing=None, viscous=None):
+    """su, sv, sw, sth and rhs in place.  viscous = dict(lamsq, z0, z0th, vism,
+    vist, strain): viscous = .true., the subgrid model (tests/subgrid_np.py)
+    in place of the four exchanges (dynamics.f90:878-893), with zeroed stress
+    temporaries."""
     kp = g.kp
     K, Km, Kp = slice(1, kp + 1), slice(0, kp), slice(2, kp + 2)
     J, Jm, Jp = I, slice(0, -2), slice(2, None)
@@ -138,8 +142,16 @@ def sources(g, ubar, vbar, wbar, thbar, zu, zv, zw, u, v, w, th, su, sv, sw, sth
         sv[K, J, I] = sv[K, J, I] - rn * (zv[K, J, I] - _k(f["v_force"][K])) / tau
     if f.get("divergence"):
         sw[K, J, I] = sw[K, J, I] - rn * (_k(wbar[K]) - _k(f["w_subs"][K]))
-    for a in (su, sv, sw, sth):
-        cases.exchange_full(a, 0.0, 0.0)
+    if viscous:
+        import subgrid_np
+
+        vs = viscous
+        taus = [np.zeros_like(su, order="F") for _ in range(6)]
+        subgrid_np.subgrid(g, vs["lamsq"], vs["z0"], vs["z0th"], u, v, w, zu, zv, zw, th,
+                           vs["vism"], vs["vist"], vs["strain"], taus, su, sv, sw, sth)
+    else:
+        for a in (su, sv, sw, sth):
+            cases.exchange_full(a, 0.0, 0.0)
     su[0] = -su[1]
     sv[0] = -sv[1]
     sw[0] = 0.0

@@ -439,3 +439,51 @@ def test_driver_step_with_tracers_matches_independent_restatement(orc):
                     assert np.array_equal(a["q"][q], b["q"][q]), (n, q)
             else:
                 assert np.array_equal(a[name], b[name]), (n, name)
+
+
+def test_viscous_sources_match_independent_restatement(orc, g):
+    """sources with viscous = .true. (the subgrid model in place of the
+    exchanges) against the numpy restatements: su, sv, sw, sth, the
+    right-hand side, vism, vist and strain bit for bit."""
+    import dynamics_np as dn
+
+    rng = np.random.default_rng(51)
+    o = orc.OracleCore(g)
+    a = subgrid_inputs(g, 52)
+    lamsq = cases.mixing_length_sq(g, 0.23, 0.1)
+    bars = [rng.uniform(-1, 1, g.kp + 2) for _ in range(3)] + [rng.uniform(-0.5, 0.5, g.kp + 2)]
+    outs = [rand_field(g, rng) for _ in range(5)]  # su sv sw sth rhs
+    outs2 = [x.copy(order="F") for x in outs]
+    vis1 = {n: fz(g) for n in ("vism", "vist", "strain")}
+    vis2 = {n: fz(g) for n in ("vism", "vist", "strain")}
+    o.sources_viscous(*bars, a["zu"], a["zv"], a["zw"], a["u"], a["v"], a["w"], a["th"], *outs,
+                      lamsq, 0.1, 0.1, vis1["vism"], vis1["vist"], vis1["strain"])
+    dn.sources(g, *bars, a["zu"], a["zv"], a["zw"], a["u"], a["v"], a["w"], a["th"], *outs2,
+               viscous=dict(lamsq=lamsq, z0=0.1, z0th=0.1, **vis2))
+    for name, x, y in zip(("su", "sv", "sw", "sth", "rhs"), outs, outs2):
+        assert np.array_equal(x, y), name
+    for n in vis1:
+        assert np.array_equal(vis1[n], vis2[n]) and np.any(vis1[n]), n
+
+
+def test_viscous_driver_step_matches_independent_restatement(orc):
+    """Three viscous time steps of the oracle's model_driver against the
+    numpy driver with the subgrid model in sources: every field, role, mean
+    and the subgrid fields, bit for bit."""
+    import driver_np
+
+    c = small_bubble(ip=12, jp=10, kp=8)
+    vis = dict(lamsq=cases.mixing_length_sq(c.grid, 0.23, 0.1), z0=0.1, z0th=0.1)
+    kw = dict(ptol=c.ptol, kord=c.kord, monotone=c.monotone, viscous=vis)
+    m = orc.OracleModel(c.grid, c.state, c.dt, **kw)
+    d = driver_np.Driver(c.grid, c.state, c.dt, **kw)
+    m.driver_start()
+    d.start()
+    for n in range(3):
+        it, err = m.step(1)
+        d.step()
+        assert (it, err) == (d.iters, d.err), n
+        a, b = m.fields(), d.fields()
+        for name in b:
+            ref = m.f[name] if name in ("vism", "vist", "strain") else a[name]
+            assert np.array_equal(ref, b[name]), (n, name)
