@@ -17,7 +17,10 @@
 using namespace dcm;
 
 namespace dcm {
-Profiler* g_prof = nullptr;
+// per host thread: a handle is driven by one thread at a time, and a launch
+// made by another thread (another handle, the allocation-free entry point)
+// must never touch this handle's profiler
+thread_local Profiler* g_prof = nullptr;
 }
 
 namespace {
@@ -99,6 +102,10 @@ struct dcm_handle {
     // [1] the FP32 iterations of the mixed form): warps per sweep block, warp
     // tasks per warp of the reducing kernels (0 = fill the GPU), marching depth
     int tune_by[2] = {8, 8}, tune_tasks[2] = {0, 0}, tune_ni[2] = {4, 4}, tune_fuse[2] = {0, 1};
+    // dcm_solver_limits: round budget of graph-driven solves (0: default) and
+    // the FP64 breakdown threshold (< 0: the reference's tiny)
+    int round_budget = 0;
+    double tiny = -1.0;
     // bumped whenever captured pointers or launch shapes change (state
     // upload, tuning); an ensemble rebuilds its step graphs when it moves
     unsigned generation = 0;
@@ -242,6 +249,8 @@ SolverWork<double> solver_work(dcm_handle* h) {
     w.ni = h->tune_ni[0];
     w.fuse = 0;
     w.max_blocks = (int)std::min<size_t>(h->npartials / 3, (size_t)1 << 30);
+    w.round_budget = h->round_budget;
+    w.tiny = h->tiny;
     return w;
 }
 
@@ -998,6 +1007,7 @@ SolverWork<float> solver_work_f(dcm_handle* h) {
     w.max_blocks = (int)std::min<size_t>(h->npartials / 3, (size_t)1 << 30);
     w.cheb = h->cfg.precond == 1 ? 1 : 0;
     w.cheb_lo = h->cfg.precond_lo > 0.0 ? h->cfg.precond_lo : 0.05;
+    w.round_budget = h->round_budget;
     return w;
 }
 
@@ -1443,6 +1453,15 @@ extern "C" int dcm_solver_graphs(dcm_handle* h, int on) {
     const int mode = on == 0 ? 0 : on == 2 ? 2 : 1;
     if (mode != h->graphs) h->generation += 1;  // an ensemble recaptures its steps
     h->graphs = mode;
+    return DCM_OK;
+}
+
+extern "C" int dcm_solver_limits(dcm_handle* h, int max_rounds, double tiny) {
+    CHECK_H();
+    if (max_rounds < 0 || !(tiny == tiny)) return fail(h, DCM_E_ARG, "solver_limits");
+    if (max_rounds != h->round_budget || tiny != h->tiny) h->generation += 1;
+    h->round_budget = max_rounds;
+    h->tiny = tiny < 0.0 ? -1.0 : tiny;
     return DCM_OK;
 }
 

@@ -98,6 +98,12 @@ struct SolverWork {
     // graph-driven iterations launch their kernels with programmatic
     // dependent launch (where the runtime takes it; solver_pdl_available)
     int pdl = 1;
+    // failure-path limits: rounds a graph-driven solve may run before it
+    // stops with DCM_E_TIMEOUT (0: itmax + 1, or itmax + max_updates + 1 in
+    // the mixed form), and the breakdown threshold of omega in an FP64 solve
+    // (< 0: the reference's tiny)
+    int round_budget = 0;
+    double tiny = -1.0;
 };
 
 // one-time setup of the solver kernels (shared-memory limits, the probe of

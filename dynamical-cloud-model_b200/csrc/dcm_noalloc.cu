@@ -52,6 +52,9 @@ extern "C" int dcm_horizontal_means_noalloc(int ip, int jp, int kp, const double
     if (!u || !v || !w || !th || !means) return DCM_E_ARG;
     const dcm::Dims d = dcm::make_dims(ip, jp, kp);
     if (d.n() >= (size_t)1 << 31) return DCM_E_ARG;
+    // an error still pending from the caller's own work is left for the
+    // caller's own check (not consumed here), and nothing is queued on top
+    if (cudaPeekAtLastError() != cudaSuccess) return DCM_E_CUDA;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return DCM_E_CUDA;
     cudaError_t e = cudaSuccess;
@@ -66,5 +69,7 @@ extern "C" int dcm_horizontal_means_noalloc(int ip, int jp, int kp, const double
     dcm::Metrics<double> none{};  // the divergence is not formed here
     dcm::launch_means_div<double, double>(d, none, u, v, w, th, nullptr, 0, means, nullptr, partials,
                                   ticket, st);
+    // no error was pending before the launches, so this reads (and clears)
+    // only their own launch status
     return cudaGetLastError() == cudaSuccess ? DCM_OK : DCM_E_CUDA;
 }

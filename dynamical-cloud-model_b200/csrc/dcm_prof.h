@@ -56,8 +56,10 @@ struct Profiler {
     }
 };
 
-// the profiler of the handle currently running (set by the C-ABI layer)
-extern Profiler* g_prof;
+// the profiler of the handle this host thread is running (set by the C-ABI
+// layer around dcm_step, null elsewhere); one per thread, so launches that
+// other threads make are never counted or timed into it
+extern thread_local Profiler* g_prof;
 
 struct ProfScope {
     int cat;

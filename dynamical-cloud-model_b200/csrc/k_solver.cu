@@ -91,6 +91,9 @@ struct SolverArgs {
     int cond_max = 0;
     // launch with programmatic stream serialisation (pdl_wait)
     int pdl = 0;
+    // |omega| below this ends an FP64 solve with DCM_E_BREAKDOWN; the
+    // reference's tiny is the default-real literal 1.e-16 (dynamics.f90:321)
+    double tiny = (double)1.e-16f;
 };
 
 // a_p exactly as set_mat_a forms it (dynamics.f90:93-95)
@@ -481,7 +484,7 @@ __device__ __forceinline__ void reduce_tail(const SolverArgs& a, double (&acc)[N
             S->tt = s[0];
             S->ts = s[NV - 1];
             S->omg = S->ts / S->tt;               // :412
-            const double tiny = (double)1.e-16f;  // default-real literal, :321
+            const double tiny = a.tiny;  // default-real literal 1.e-16, :321
             if (S->ru && !(fabs(S->omg) >= tiny)) {
                 S->restart = (isfinite(s[0]) && isfinite(s[NV - 1])) ? 1 : 2;
                 S->pause = 1;
@@ -1289,6 +1292,7 @@ int solver_run(SolverWork<T>& w, const Dims& d, T* x, const T* b, const T* sw, c
     a.ni = w.ni >= 1 ? w.ni : 1;
     a.fuse = w.fuse;
     no_cheb(a);  // the FP64 path keeps the reference's sweeps
+    if (w.tiny >= 0.0) a.tiny = w.tiny;
     const Coef<T> c = coef_of(w);
     SolverBufs B{};
     B.x = x;
@@ -1296,7 +1300,7 @@ int solver_run(SolverWork<T>& w, const Dims& d, T* x, const T* b, const T* sw, c
     B.out = w.r;
     B.out2 = w.cr;
     B.out3 = w.rh;
-    const int max_rounds = itmax + 1;
+    const int max_rounds = w.round_budget > 0 ? w.round_budget : itmax + 1;
     auto post_launch = [&](cudaStream_t s) {
         if (post) {
             ProfScope ps(P_POST, s);
@@ -1330,11 +1334,11 @@ int solver_run(SolverWork<T>& w, const Dims& d, T* x, const T* b, const T* sw, c
     if (use_graph) {
         SolveGraph& G = *w.graph;
         const void* kp[6] = {x, b, sw, dzn, w.r, w.S};
-        const double kd[3] = {tol, sc_floor, 0.0};
+        const double kd[3] = {tol, sc_floor, a.tiny};
         // launch shape: by < 16, tasks < 16, ni < 64, fuse < 2, pdl < 2
         const int shape =
             a.by + 16 * a.tasks + 256 * a.ni + 16384 * a.fuse + 65536 * (w.pdl ? 1 : 0);
-        const int ki[6] = {itmax, wo, post ? 1 : 0, (int)sizeof(T) + 16 * shape,
+        const int ki[6] = {itmax, wo, (post ? 1 : 0) + 2 * max_rounds, (int)sizeof(T) + 16 * shape,
                            d.ip * 4096 + d.jp, d.kp};
         if (!G.matches(kp, kd, ki)) {
             G.release();
@@ -1669,7 +1673,7 @@ int refine_run(SolverWork<float>& wf, SolverWork<double>& wd, const Dims& d, dou
         ProfScope ps(P_POST, s);
         k_bicg_post<double, float><<<gi, bl, 0, s>>>(d, x, sw, dzn, wd.S, 1);
     };
-    const int max_rounds = itmax + max_updates + 1;
+    const int max_rounds = wf.round_budget > 0 ? wf.round_budget : itmax + max_updates + 1;
     // the whole mixed solve into the graph being captured on `s0`:
     //   WHILE (not done) {                           one FP64 update cycle
     //       WHILE (not done, not paused) { FP32 iteration }
@@ -1719,7 +1723,8 @@ int refine_run(SolverWork<float>& wf, SolverWork<double>& wd, const Dims& d, dou
         const double kd[3] = {tol, delta, af.cheb ? wf.cheb_lo : 0.0};
         const int shape = af.by + 16 * af.tasks + 256 * af.ni + 16384 * af.fuse +
                           32768 * af.cheb + 65536 * (wf.pdl ? 1 : 0);
-        const int ki[6] = {itmax, max_updates, 1, 16 * shape, d.ip * 4096 + d.jp, d.kp};
+        const int ki[6] = {itmax, max_updates, 1 + 2 * max_rounds, 16 * shape,
+                           d.ip * 4096 + d.jp, d.kp};
         if (!G.matches(kp, kd, ki)) {
             G.release();
             bool good = ok(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));

@@ -15,8 +15,8 @@
  * caller checks dims = [1,1,1] with dcm_check_decomposition() once.
  *
  * Every function returns a dcm_status.  Where the reference calls STOP, the
- * library returns an error code instead; the Fortran shim in
- * INTEGRATION.md prints the reference's message and stops.
+ * library returns an error code instead; a Fortran interface module over
+ * this header prints the reference's message and stops.
  */
 #ifndef DCM_H
 #define DCM_H
@@ -296,7 +296,12 @@ const char *dcm_output_last_error(const dcm_output *o);
  * device: calls whose work overlaps on the GPU race and must be serialised
  * by the caller.  The first call on each device resolves that array's
  * device address (with the device current); make that first call before any
- * stream capture.  kp > DCM_NOALLOC_MAX_KP returns DCM_E_ARG. */
+ * stream capture.  The address is kept for the life of the process: after a
+ * cudaDeviceReset the array may move, so do not call this entry point again
+ * in that process.  kp > DCM_NOALLOC_MAX_KP returns DCM_E_ARG.  A CUDA error
+ * already pending on the calling thread makes it return DCM_E_CUDA at once,
+ * queueing nothing and leaving that error pending for the caller's own
+ * check. */
 #define DCM_NOALLOC_MAX_KP 1024
 int dcm_horizontal_means_noalloc(int ip, int jp, int kp, const double *u,
                                  const double *v, const double *w,
@@ -327,6 +332,19 @@ int dcm_profile_read(dcm_handle *h, double *ms, long long *launches, int ncat);
  * All launch the same kernels in the same order and give bit-identical
  * results; while event timing is enabled the host-driven loop is used. */
 int dcm_solver_graphs(dcm_handle *h, int on);
+
+/* Limits of the pressure solve's failure paths (no counterpart in the
+ * reference; the tests use them to reach DCM_E_TIMEOUT and DCM_E_BREAKDOWN
+ * without a singular system).  max_rounds > 0 bounds a graph-driven solve
+ * (dcm_solver_graphs 1 or 2) to that many loop rounds, after which it stops
+ * with DCM_E_TIMEOUT; 0 restores the default budget, itmax + 1 rounds
+ * (itmax + reliable updates + 1 in the mixed form), which a solve that
+ * behaves never reaches.  tiny >= 0 replaces the breakdown threshold of an
+ * FP64 solve, |omega| < tiny -> DCM_E_BREAKDOWN (dynamics.f90:414-417); a
+ * negative tiny restores the reference's 1.e-16 (a default-real literal,
+ * :321).  The FP32 iterations of the mixed form keep their own restart test.
+ * Applies to every later solve of this handle (drop-in and resident). */
+int dcm_solver_limits(dcm_handle *h, int max_rounds, double tiny);
 
 /* *programmatic = 1 when this handle's graph-driven solves launch their
  * iteration kernels with programmatic dependent launch (mode 1 of

@@ -257,14 +257,20 @@ void orc_precondition(const orc_grid *g, const double *r, double *s,
     free(t);
 }
 
+/* Breakdown threshold of bicgstab.  The reference's tiny = 1.e-16 is a
+ * default-real (single precision) literal, :321; a test may raise it with
+ * orc_set_breakdown_tiny to reach the breakdown stop (:414-417) on a
+ * well-posed system.  A negative value restores the reference's. */
+static double g_tiny = -1.0;
+void orc_set_breakdown_tiny(double tiny) { g_tiny = tiny < 0.0 ? -1.0 : tiny; }
+
 /* bicgstab, dynamics.f90:293-444 */
 int orc_bicgstab(const orc_grid *g, double *x, double *b, const double *sw,
                  double tol, int test_solver, int *first_call, int itmax,
                  int *iters, double *err_out) {
     const int ip = g->ip, jp = g->jp, kp = g->kp;
     const size_t n = NTOT;
-    /* tiny = 1.e-16 is a default-real (single precision) literal, :321 */
-    const double tiny = (double)1.e-16f;
+    const double tiny = g_tiny >= 0.0 ? g_tiny : (double)1.e-16f; /* :321 */
     const int prit = 3; /* :322 */
     double sc_err, err, rho, alf, omg, bet, nrm, tt, ts;
     int status = ORC_OK;

@@ -68,6 +68,9 @@ void orc_precondition(const orc_grid *g, const double *r, double *s, int prit);
 int orc_bicgstab(const orc_grid *g, double *x, double *b, const double *sw,
                  double tol, int test_solver, int *first_call, int itmax,
                  int *iters, double *err);
+/* Breakdown threshold of |omega| for later orc_bicgstab calls (process-wide;
+ * negative: the reference's tiny).  For tests of the breakdown stop.        */
+void orc_set_breakdown_tiny(double tiny);
 
 /* ---- sources / momentum (dynamics.f90:639-1099) ---- */
 int orc_sources(const orc_grid *g, const orc_forcing *f,

@@ -74,6 +74,7 @@ def library():
         L.orc_model_step.restype = C.c_int
         L.orc_inn_prod.restype = C.c_double
         L.orc_set_threads.argtypes = [C.c_int, C.c_int]
+        L.orc_set_breakdown_tiny.argtypes = [C.c_double]
     return _lib
 
 
@@ -88,6 +89,12 @@ def _F(a):
 
 def set_threads(n, parallel_reductions=False):
     library().orc_set_threads(int(n), int(bool(parallel_reductions)))
+
+
+def set_breakdown_tiny(tiny=-1.0):
+    """Breakdown threshold of |omega| in later bicgstab calls (negative: the
+    reference's 1.e-16, dynamics.f90:321)."""
+    library().orc_set_breakdown_tiny(float(tiny))
 
 
 class OracleCore:

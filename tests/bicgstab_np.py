@@ -82,10 +82,11 @@ def precondition(c, r):
     return s
 
 
-def bicgstab(g, x, b, sw, tol, itmax=9999):
+def bicgstab(g, x, b, sw, tol, itmax=9999, tiny=TINY, trace=None):
     """Solve A x = b from the initial x (updated in place); returns
     (status, iterations, err) with status 0 (converged), 1 (no convergence
-    within itmax) or 2 (|omega| < tiny)."""
+    within itmax) or 2 (|omega| < tiny).  trace: a list that receives omega
+    of every iteration."""
     c = coefficients(g)
     kp = g.kp
     sc_err = max(math.sqrt(inn_prod(b, b)), 0.01)
@@ -114,7 +115,9 @@ def bicgstab(g, x, b, sw, tol, itmax=9999):
         tt = inn_prod(t, t)
         ts = inn_prod(t, s)
         omg = ts / tt
-        if abs(omg) < TINY:
+        if trace is not None:
+            trace.append(omg)
+        if abs(omg) < tiny:
             return 2, it, err
         x[...] = x + alf * p + omg * cs
         r = s - omg * t

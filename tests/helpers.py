@@ -78,3 +78,32 @@ def subgrid_inputs(g, seed):
               "su", "sv", "sw", "sth"):
         f[n] = rand_field(g, rng, -1.0, 1.0)
     return f
+
+
+def breakdown_system(g, seed=14):
+    """A zero-mean Poisson right-hand side and a small random warm start."""
+    rng = np.random.default_rng(seed)
+    b = fz(g)
+    b[1:-1, 1:-1, 1:-1] = rng.normal(size=(g.kp, g.jp, g.ip))
+    b[1:-1, 1:-1, 1:-1] -= b[1:-1, 1:-1, 1:-1].mean()
+    return b, rand_field(g, rng, -0.01, 0.01)
+
+
+def breakdown_threshold(bicgstab_np, g, x0, b, later, n=12):
+    """A breakdown threshold and the iteration it stops the solve in.  Not
+    later: far above any |omega| (iteration 1).  later: the geometric mean of
+    |omega_m| and the smallest earlier |omega|, for the first iteration m > 1
+    whose |omega| is below every earlier one (omega from the numpy
+    restatement of the reference's solve); the gap is far wider than the
+    round-off between implementations."""
+    if not later:
+        return 1e300, 1
+    trace = []
+    bicgstab_np.bicgstab(g, x0.copy(order="F"), b.copy(order="F"), fz(g), 1e-30, itmax=n,
+                         tiny=0.0, trace=trace)
+    om = [abs(w) for w in trace]
+    for m in range(1, len(om)):
+        lo = min(om[:m])
+        if om[m] < lo * (1 - 1e-4):
+            return float(np.sqrt(om[m] * lo)), m + 1
+    raise AssertionError("no iteration with a new smallest |omega| in the first %d" % n)

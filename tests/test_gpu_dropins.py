@@ -9,7 +9,8 @@ after one time step; single routines are held tighter).
 import numpy as np
 import pytest
 
-from helpers import cases, fz, live_mask_p, rand_field, relerr, small_bubble, velocities
+from helpers import (breakdown_system, breakdown_threshold, cases, fz, live_mask_p, rand_field,
+                     relerr, small_bubble, velocities)
 
 pytestmark = pytest.mark.gpu
 
@@ -250,3 +251,74 @@ def test_bicgstab_early_return(setup):
     assert it == it2 == 0 and err == err2 == 0.0
     m = live_mask_p(g)
     assert np.array_equal(x[m], x2[m])
+
+
+def _raw_bicgstab(core, x, b, sw, tol, itmax=9999):
+    """dcm_bicgstab through ctypes, returning (status, iterations) without
+    raising, so that a failure status and the iteration it came at are both
+    visible."""
+    import ctypes as C
+    it = C.c_int(-1)
+    err = C.c_double(0.0)
+    st = core.lib.dcm_bicgstab(core.h, core.F(x), core.F(b), core.F(sw), float(tol), 0,
+                               int(itmax), C.byref(it), C.byref(err))
+    return st, it.value
+
+
+@pytest.mark.parametrize("later", [False, True])
+def test_bicgstab_breakdown_status(setup, orc, dcm, later):
+    """The breakdown stop of dynamics.f90:414-417 (|omega| < tiny), reached on
+    a well-posed system by raising the threshold on both sides: above every
+    |omega| (the stop comes in iteration 1) or between the |omega| of a later
+    iteration m and the smallest earlier one (the stop comes in iteration m).
+    The oracle and the GPU stop in the same iteration with the breakdown
+    status, before that iteration's x update."""
+    import bicgstab_np
+
+    g, core, ocore = setup
+    b, x = breakdown_system(g)
+    tiny, want_it = breakdown_threshold(bicgstab_np, g, x, b, later)
+    x0 = x.copy(order="F")
+    x2, b2 = x.copy(order="F"), b.copy(order="F")
+    core.solver_limits(tiny=tiny)
+    orc.set_breakdown_tiny(tiny)
+    try:
+        st, it = _raw_bicgstab(core, x, b.copy(order="F"), fz(g), 1e-10)
+        st2, it2, _ = ocore.bicgstab(x2, b2, fz(g), 1e-10)
+    finally:
+        core.solver_limits()
+        orc.set_breakdown_tiny(-1.0)
+    assert st == dcm.DCM_E_BREAKDOWN and st2 == 2
+    assert it == it2 == want_it
+    inner = (slice(1, -1),) * 3
+    if want_it == 1:
+        assert np.array_equal(x[inner], x0[inner])
+    else:
+        assert relerr(x[inner], x2[inner]) <= 1e-9
+    # the handle is usable afterwards and back on the reference's threshold
+    it3, err3 = core.bicgstab(x, b.copy(order="F"), fz(g), 1e-10)
+    assert err3 < 1e-10 and it3 > 1
+
+
+@pytest.mark.parametrize("graphs", [1, 2])
+def test_bicgstab_timeout_status(setup, dcm, graphs):
+    """A graph-driven solve is bounded by its round budget: with a budget
+    below the iterations the solve needs, the loop ends after exactly that
+    many iterations with DCM_E_TIMEOUT (the device sets the status and the
+    WHILE node's condition; nothing waits on the host), and the next solve
+    with the default budget converges."""
+    g, core, ocore = setup
+    rng = np.random.default_rng(30)
+    b = _poisson_rhs(g, rng)
+    x = fz(g)
+    core.solver_graphs(graphs)
+    core.solver_limits(max_rounds=3)
+    try:
+        st, it = _raw_bicgstab(core, x, b.copy(order="F"), fz(g), 1e-10)
+    finally:
+        core.solver_limits()
+        core.solver_graphs(1)
+    assert st == dcm.DCM_E_TIMEOUT
+    assert it == 3
+    it2, err2 = core.bicgstab(fz(g), b.copy(order="F"), fz(g), 1e-10)
+    assert err2 < 1e-10 and it2 > 3

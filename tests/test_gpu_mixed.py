@@ -142,3 +142,29 @@ def test_chebyshev_sweeps_take_fewer_iterations(dcm):
         core.close()
     print("FP32 iterations over 3 steps", its)
     assert its[1] < 0.85 * its[0], its
+
+
+def test_mixed_solve_timeout_status(dcm):
+    """The mixed form's graph-driven solve (a WHILE loop of FP64 update cycles
+    around a WHILE loop of FP32 iterations) is bounded by the same round
+    budget: a time step whose solve needs more rounds than the budget ends
+    with DCM_E_TIMEOUT instead of hanging, and the handle runs normally once
+    the default budget is back."""
+    c = small_bubble()
+    core = dcm.DynamicalCore(c.grid)
+    try:
+        def fresh():
+            core.upload_state(c.state, c.dt, ptol=c.ptol, kord=c.kord, monotone=c.monotone,
+                              precision=1, precond=1)
+            core.driver_start()
+        fresh()
+        core.solver_limits(max_rounds=5)
+        with pytest.raises(dcm.DCMError) as e:
+            core.step(1)
+        assert e.value.status == dcm.DCM_E_TIMEOUT
+        core.solver_limits()
+        fresh()
+        st = core.step(1)
+        assert st.err_last < c.ptol and st.iters_last > 5
+    finally:
+        core.close()

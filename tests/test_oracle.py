@@ -7,7 +7,8 @@ restatements and to analytic invariants instead.
 import numpy as np
 import pytest
 
-from helpers import cases, fz, rand_field, relerr, small_bubble, subgrid_inputs, velocities
+from helpers import (breakdown_system, breakdown_threshold, cases, fz, rand_field, relerr,
+                     small_bubble, subgrid_inputs, velocities)
 
 
 @pytest.fixture(scope="module")
@@ -153,6 +154,32 @@ def test_bicgstab_itmax_reports_noconv(orc, g):
     b[1:-1, 1:-1, 1:-1] -= b[1:-1, 1:-1, 1:-1].mean()
     st, it, err = o.bicgstab(fz(g), b, fz(g), 1e-10, itmax=1)
     assert st == 1 and it == 1 and err > 1e-10
+
+
+@pytest.mark.parametrize("later", [False, True])
+def test_bicgstab_breakdown_stop(orc, g, later):
+    """The breakdown stop (dynamics.f90:414-417): with the threshold raised
+    above |omega|, the solve stops in that iteration with status 2 before the
+    iteration's x update, as the numpy restatement does.  later: the
+    threshold sits between |omega| of the first iteration m > 1 that is
+    smaller than every earlier one and the smallest earlier one, so the stop
+    comes in iteration m after m - 1 full iterations."""
+    import bicgstab_np
+
+    b, x0 = breakdown_system(g)
+    tiny, want_it = breakdown_threshold(bicgstab_np, g, x0, b, later)
+    o = orc.OracleCore(g)
+    x_c, x_np = x0.copy(order="F"), x0.copy(order="F")
+    orc.set_breakdown_tiny(tiny)
+    try:
+        st, it, err = o.bicgstab(x_c, b.copy(order="F"), fz(g), 1e-10)
+    finally:
+        orc.set_breakdown_tiny(-1.0)
+    st2, it2, err2 = bicgstab_np.bicgstab(g, x_np, b.copy(order="F"), fz(g), 1e-10, tiny=tiny)
+    assert (st, it) == (st2, it2) == (2, want_it)
+    assert np.array_equal(x_c, x_np)
+    inner = (slice(1, -1),) * 3
+    assert np.array_equal(x_c[inner], x0[inner]) == (want_it == 1)
 
 
 def test_horizontal_means_match_numpy(orc, g):
