@@ -16,6 +16,13 @@ the mixed form against the FP64 path after 1, 10 and --accuracy-steps steps
 go in `accuracy_vs_fp64`.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+    python bench.py --run-case --case NAME --steps K [--precision 0|1] ...
+
+The compact JSON line keeps the headline figures (mixed form, FP64 path,
+speed-up, accuracy after --accuracy-steps, roofline, CPU baseline,
+end-to-end); the long-form record (per-class kernel times, step models,
+accuracy tables) goes to gpurun_out/bench_details.json.
+--run-case prints one line per step of a named case (profiling driver).
 
 N > 1 (torchrun, one process per GPU): the single domain does not shard
 (whole domain on one GPU), so each rank advances its own replica of the
@@ -238,6 +245,36 @@ def field_errors(g, ref, got):
     return out
 
 
+def bench_config(case, args):
+    """The workload of a bench line, the same dict in both arms (the GPU
+    arm's mixed form and FP64 path and the reference arm's CPU restatement
+    advance the same seeded case over the same time steps)."""
+    g = case.grid
+    mb = (g.ip + 2) * (g.jp + 2) * (g.kp + 2) * 8 / 1e6
+    return {"workload": "%s: steps 1..%d from the seeded initial state" % (case.name, args.steps),
+            "grid": "%dx%dx%d" % (g.ip, g.jp, g.kp), "dt": case.dt, "kord": case.kord,
+            "monotone": bool(case.monotone), "ptol": case.ptol,
+            "tracers": int(case.nq or 0),
+            "l2": ("inputs larger than L2: one FP64 field is %.1f MB and a step streams "
+                   "about 40 resident fields" % mb) if 40 * mb > 126 else
+                  ("resident state (about 40 FP64 fields of %.2f MB) fits in the 126 MB "
+                   "L2" % mb)}
+
+
+def write_details(d, name="bench_details.json"):
+    """The long-form record (per-class kernel times, accuracy tables, step
+    models, notes) beside the compact JSON line; returns its path."""
+    out = os.path.join(ROOT, "gpurun_out")
+    try:
+        os.makedirs(out, exist_ok=True)
+        path = os.path.join(out, name)
+        with open(path, "w") as f:
+            json.dump(d, f, indent=1)
+        return os.path.relpath(path, ROOT)
+    except OSError:
+        return None
+
+
 def run_b200(args, rank, world, local_rank, dist):
     pkg = load_pkg()
     case = make_case(pkg, args.case)
@@ -306,9 +343,12 @@ def run_b200(args, rank, world, local_rank, dist):
     dom_passes = FUSED_JACOBI_PASSES if (fused and dom == "jacobi") else PASSES.get(dom, 0.0)
     dom_bytes = dom_passes * N * w32
     dom_s = dom_ms / dom_n / 1e3 if dom_n else None
-    achieved = dom_bytes / dom_s / 1e9 if dom_n else None
-    effective = (FUSED_REPLACED_PASSES * N * w32 / dom_s / 1e9
-                 if (fused and dom == "jacobi" and dom_n) else None)
+    # algorithmic bytes of one launch by the operator-fused model: a fused
+    # preconditioner launch applies the three sweeps of a phase (11.5 passes
+    # averaged over phases B and C)
+    dom_bytes_alg = (FUSED_REPLACED_PASSES * N * w32 if (fused and dom == "jacobi")
+                     else dom_bytes)
+    achieved_alg = dom_bytes_alg / dom_s / 1e9 if dom_n else None
     traffic = None
     tp = os.path.join(ROOT, "profiles", "dram_traffic.json")
     if os.path.exists(tp):
@@ -381,30 +421,17 @@ def run_b200(args, rank, world, local_rank, dist):
     core.close()
     if rank != 0:
         return None
-    return {
-        "metric": metric_of(case), "value": m32["value"], "unit": "grid-pt-steps/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": m32["ms"] / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32+f64 (FP32 fields and BiCGSTAB, FP64 pressure, residual and dots)",
-        "data": "synthetic (seeded %s, numpy PCG64 seed %d)" % (case.name, case.seed),
-        "config": {"workload": case.name + " mixed precision (FP32 + FP64 reliable updates)",
-                   "grid": [g.ip, g.jp, g.kp], "dt": case.dt, "kord": case.kord,
-                   "monotone": bool(case.monotone), "ptol": case.ptol,
-                   "timed_steps": "1..%d from the initial state" % args.steps,
-                   "bicgstab_iters_per_step": m32["iters"] / args.steps,
-                   "preconditioner": "FP32 iterations: Chebyshev-weighted Jacobi sweeps "
-                                     "(3 sweeps, interval [0.05, 2]); FP64: the "
-                                     "reference's 3 Jacobi sweeps",
-                   "tuned_launch_shape": m32["shape"],
-                   "l2": "inputs larger than L2 (about 40 fields of 34-69 MB resident)",
-                   "parallelism": "replicas" if world > 1 else "single GPU"},
-        "fp64": {"value": m64["value"], "ms_per_step": m64["ms"] / args.steps,
-                 "tuned_launch_shape": m64["shape"],
-                 "bicgstab_iters_per_step": m64["iters"] / args.steps,
-                 "gpu_launches": m64["launches"], "clocks": m64["clocks"],
-                 "step_model": step_model(m64, 8.0, ITER_PASSES),
+    sm32 = step_model(m32, w32, FUSED_ITER_PASSES if fused else ITER_PASSES)
+    sm64 = step_model(m64, 8.0, ITER_PASSES)
+    acc_last = acc.get(str(args.accuracy_steps), {})
+    details = {
+        "fp64": {"tuned_launch_shape": m64["shape"], "gpu_launches": m64["launches"],
+                 "clocks": m64["clocks"], "step_model": sm64,
                  "kernel_ms": {k: round(v[0], 3) for k, v in m64["classes"].items()}},
-        "speedup_vs_fp64": m32["value"] / m64["value"],
+        "mixed": {"tuned_launch_shape": m32["shape"], "step_model": sm32,
+                  "step_model_unfused_algorithm": step_model(m32, w32, ITER_PASSES),
+                  "kernel_ms": {k: round(v[0], 3) for k, v in classes.items()},
+                  "kernel_launches": {k: v[1] for k, v in classes.items()}},
         "mixed_reference_sweeps": {
             "value": m32ref["value"], "ms_per_step": m32ref["ms"] / args.steps,
             "bicgstab_iters_per_step": m32ref["iters"] / args.steps,
@@ -412,23 +439,39 @@ def run_b200(args, rank, world, local_rank, dist):
             "note": "the mixed form with the reference's unweighted Jacobi sweeps: the part "
                     "of the speed-up that FP32 alone gives"},
         "accuracy_vs_fp64": acc,
+        "roofline_note": "achieved = the algorithmic bytes of the three Jacobi sweeps one fused "
+                         "launch applies (11.5 N-point FP32 passes, the operator-fused model) per "
+                         "launch time; the fused kernel itself reads r/a_p, v1/a_p (and old p) "
+                         "and writes p or cs, 3.5 passes, which min_bytes_frac counts",
+        "e2e_host_ms": e2e.pop("host_ms"), "e2e_note": e2e.pop("note"),
+        "preconditioner": "FP32 iterations: Chebyshev-weighted Jacobi sweeps (3 sweeps, "
+                          "interval [0.05, 2]); FP64: the reference's 3 Jacobi sweeps",
+    }
+    min_bytes = FUSED_JACOBI_PASSES * N * w32 if (fused and dom == "jacobi") else dom_bytes
+    return {
+        "metric": metric_of(case), "value": m32["value"], "unit": "grid-pt-steps/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": m32["ms"] / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+f64",
+        "data": "synthetic (seeded %s, numpy PCG64 seed %d)" % (case.name, case.seed),
+        "fp64": {"value": m64["value"], "ms_per_step": m64["ms"] / args.steps,
+                 "iters_per_step": m64["iters"] / args.steps, "step_frac": sm64["frac"]},
+        "speedup_vs_fp64": m32["value"] / m64["value"],
+        "iters_per_step": m32["iters"] / args.steps, "step_frac": sm32["frac"],
+        "accuracy_vs_fp64_steps": args.accuracy_steps,
+        "accuracy_vs_fp64": {n: float("%.3g" % v["max"]) for n, v in acc_last.items()},
+        "config": bench_config(case, args),
+        "parallelism": "replicas" if world > 1 else "single GPU",
         "roofline": {"bound": "hbm", "kernel": dom + (" (fused preconditioner)" if fused else ""),
-                     "achieved": achieved, "peak": peak,
-                     "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
+                     "achieved": achieved_alg, "peak": peak, "unit": "GB/s",
+                     "frac": (achieved_alg / peak) if achieved_alg else None,
                      "traffic": traffic, "peak_kind": peak_kind,
-                     "bytes_per_launch": dom_bytes, "launches": dom_n,
+                     "bytes_per_launch": dom_bytes_alg, "launches": dom_n,
                      "avg_launch_us": dom_ms / dom_n * 1e3 if dom_n else None,
-                     "effective_GBs": effective,
-                     "effective_frac": (effective / peak) if effective else None,
-                     "effective_note": ("bytes of the three separate sweeps one fused launch "
-                                        "replaces (11.5 passes) per launch time; the fused "
-                                        "kernel itself is issue-bound") if fused else None,
-                     "step_model": step_model(m32, w32,
-                                              FUSED_ITER_PASSES if fused else ITER_PASSES),
-                     "step_model_unfused_algorithm": step_model(m32, w32, ITER_PASSES)},
-        "kernel_ms": {k: round(v[0], 3) for k, v in classes.items()},
+                     "min_bytes_frac": (min_bytes / dom_s / 1e9 / peak) if dom_n else None},
         "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": m32["launches"],
-        "clocks": m32["clocks"],
+        "clocks": {k: m32["clocks"].get(k) for k in ("sm_mhz", "sm_max_mhz", "reasons")},
+        "details": write_details(details),
     }
 
 
@@ -517,16 +560,28 @@ def run_ensemble(args, rank, world, local_rank, dist):
     }
 
 
-def cpu_baseline(args, case, nsteps):
+def cpu_baseline(args, case, nsteps, budget=None, warmup=0):
     """The oracle (CPU restatement of the reference, not the reference
-    binary) on the host cores, steps 1..nsteps of the same case."""
+    binary: no Fortran compiler exists here) on all host cores, steps
+    1..nsteps of the same case from its initial state, stopping early only
+    past `budget` seconds.  warmup: untimed steps of the 128x1x64
+    Kelvin-Helmholtz case first (thread pool and code paged in); the case's
+    own arrays are first touched by the untimed set-up."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
+    from dcm_b200 import cases
     cores = os.cpu_count() or 1
     oracle.set_threads(cores, True)
+    if warmup:
+        kh = cases.kelvin_helmholtz()
+        w = oracle.OracleModel(kh.grid, kh.state, kh.dt, ptol=kh.ptol, kord=kh.kord,
+                               monotone=kh.monotone)
+        w.driver_start()
+        w.step(warmup)
     m = oracle.OracleModel(case.grid, case.state, case.dt, ptol=case.ptol, kord=case.kord,
                            monotone=case.monotone)
     m.driver_start()
+    budget = args.cpu_budget if budget is None else budget
     t0 = time.perf_counter()
     done = 0
     iters = 0
@@ -534,30 +589,87 @@ def cpu_baseline(args, case, nsteps):
         it, _ = m.step(1)
         iters += it
         done += 1
-        if time.perf_counter() - t0 > args.cpu_budget:
+        if time.perf_counter() - t0 > budget:
             break
     dt = time.perf_counter() - t0
     return {"value": case.grid.npoints * done / dt, "unit": "grid-pt-steps/s", "cores": cores,
-            "kind": "port",
-            "sample": "%s steps 1..%d (%d BiCGSTAB iterations), %d OpenMP threads, "
+            "kind": "port", "steps_done": done, "ms_per_step": dt * 1e3 / done,
+            "iters_per_step": iters / done,
+            "sample": "%s steps 1..%d (%d BiCGSTAB iterations), FP64, %d OpenMP threads, "
                       "%.1f s" % (case.name, done, iters, cores, dt)}
 
 
 def run_reference(args, rank, world):
+    """The reference arm: the CPU restatement of the reference's FP64 time
+    step (oracle/) on all host cores, timing steps 1..K of the GPU arm's
+    workload from the same seeded initial state.  Rank 0 only."""
     if rank != 0:
         return None
     pkg = load_pkg()
     case = make_case(pkg, args.case)
-    cpu = cpu_baseline(args, case, args.steps)
+    cpu = cpu_baseline(args, case, args.steps, budget=args.ref_budget, warmup=args.warmup)
     return {"impl": "reference", "metric": metric_of(case), "value": cpu["value"],
-            "unit": "grid-pt-steps/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": case.name, "precision": "fp64",
-                       "timed_steps": "1..n from the initial state"},
+            "unit": "grid-pt-steps/s", "n_gpus": world, "steps": cpu["steps_done"],
+            "warmup": args.warmup, "ms_per_step": cpu["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded %s, numpy PCG64 seed %d)" % (case.name, case.seed),
+            "iters_per_step": cpu["iters_per_step"],
+            "config": bench_config(case, args),
             "cpu_baseline": cpu,
             "e2e": {"value": cpu["value"], "unit": "grid-pt-steps/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
+
+
+def run_case(args):
+    """--run-case: K time steps of a named case through the C-ABI, one line
+    per step (solver iterations, FP64 updates and restarts of the mixed
+    form, final residual, device time), for profiling single kernels
+    (ncu -k ... over a few steps) and quick checks.  --host-loop drives the
+    pressure solve from the host (the same kernels; a profiler then sees
+    every launch); --graphs 2 keeps the graphs without programmatic
+    dependent launch; --output FILE writes the reference's netCDF output
+    before every --output-every steps; --profile prints the device time per
+    kernel class over the steps after the first."""
+    pkg = load_pkg()
+    from dcm_b200 import cases
+    c = make_case(pkg, args.case)
+    core = pkg.DynamicalCore(c.grid, device=args.device)
+    if args.host_loop or args.graphs != 1:
+        core.solver_graphs(0 if args.host_loop else args.graphs)
+    if args.fuse is not None:
+        core.set_launch_shape(1, fuse=args.fuse)
+    kw = dict(nq=c.nq, c_s=c.c_s, c_e=c.c_e) if c.nq else {}
+    if args.viscous:
+        kw["viscous"] = dict(lamsq=cases.mixing_length_sq(c.grid, 0.23, 0.1), z0=0.1, z0th=0.1)
+    core.upload_state(c.state, c.dt, ptol=c.ptol, kord=c.kord, monotone=c.monotone,
+                      precision=args.precision, precond=args.precond,
+                      precond_lo=args.precond_lo, inner_tol=args.inner_tol, **kw)
+    core.driver_start()
+    out = pkg.Output(core, args.output) if args.output else None
+    t_write = []
+    for s in range(args.steps):
+        if args.profile and s == min(1, args.steps - 1):
+            core.profile(True)  # after the first step (module loading, first-call set-up)
+        if out and s % args.output_every == 0:
+            t0 = time.perf_counter()
+            out.write(s * c.dt)
+            t_write.append((time.perf_counter() - t0) * 1e3)
+        st = core.step(1)
+        print("%s precision %d step %d: %d iterations (%d updates, %d restarts), "
+              "err %.3e, %.2f ms" % (c.name, args.precision, s + 1, st.iters_last,
+                                     st.updates_last, st.restarts_last, st.err_last,
+                                     st.ms_total), flush=True)
+    if out:
+        t0 = time.perf_counter()
+        out.close()
+        print("output: %d records, host ms per write call %s, close (drain) %.1f ms" % (
+            len(t_write), " ".join("%.2f" % t for t in t_write),
+            (time.perf_counter() - t0) * 1e3), flush=True)
+    if args.profile:
+        for name, (ms, n) in core.profile_read().items():
+            if n:
+                print("  %-9s %9.3f ms  %6d launches" % (name, ms, n))
+    core.close()
 
 
 def main():
@@ -568,14 +680,42 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--case", default="warm_bubble")
     ap.add_argument("--cpu-steps", type=int, default=2)
-    ap.add_argument("--cpu-budget", type=float, default=60.0)
+    ap.add_argument("--cpu-budget", type=float, default=60.0,
+                    help="seconds of the GPU arm's bounded cpu_baseline sample")
+    ap.add_argument("--ref-budget", type=float, default=1800.0,
+                    help="safety bound (s) of the reference arm, which times all K steps")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--accuracy-steps", type=int, default=100)
     ap.add_argument("--members", type=int, default=64)
     ap.add_argument("--host-loop", action="store_true",
                     help="host-polled solver loop instead of graph-driven solves (same "
                          "kernels; lets a profiler see every solver launch)")
+    # --run-case: per-step lines of one case (profiling and quick checks)
+    ap.add_argument("--run-case", action="store_true")
+    ap.add_argument("--precision", type=int, default=1, choices=[0, 1])
+    ap.add_argument("--graphs", type=int, default=1, choices=[0, 1, 2],
+                    help="solver loops: 1 graph-driven, 2 graph-driven without programmatic "
+                         "dependent launch, 0 host-polled (as --host-loop)")
+    ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--viscous", action="store_true",
+                    help="Smagorinsky subgrid model on in sources (cvis 0.23, z0 = z0th = "
+                         "0.1 m)")
+    ap.add_argument("--precond", type=int, default=0, choices=[0, 1],
+                    help="1: the mixed form's FP32 iterations use Chebyshev-weighted sweeps "
+                         "on [--precond-lo, 2]")
+    ap.add_argument("--precond-lo", type=float, default=0.05)
+    ap.add_argument("--inner-tol", type=float, default=0.1,
+                    help="mixed form: the reliable-update factor")
+    ap.add_argument("--fuse", type=int, default=None, choices=[0, 1],
+                    help="FP32 preconditioner: separate sweeps (0) or the fused kernel (1)")
+    ap.add_argument("--profile", action="store_true")
+    ap.add_argument("--output", default=None,
+                    help="netCDF file written before every --output-every steps")
+    ap.add_argument("--output-every", type=int, default=1)
     args = ap.parse_args()
+    if args.run_case:
+        run_case(args)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
