@@ -150,6 +150,11 @@ __device__ __forceinline__ double sweep_div(double a, double b) { return a / b; 
 __device__ __forceinline__ float cheb_update(float xc, float s0, float q, float sc, float w) {
     return __fmaf_rn(w, __fsub_rn(s0, __fmul_rn(q, sc)), __fmul_rn(xc, sc));
 }
+// the same with sc = 1 (every sweep but the first): the two products by 1
+// are exact, so this is bit for bit cheb_update(xc, s0, q, 1, w)
+__device__ __forceinline__ float cheb_update1(float xc, float s0, float q, float w) {
+    return __fmaf_rn(w, __fsub_rn(s0, q), xc);
+}
 __device__ __forceinline__ double cheb_update(double xc, double s0, double q, double sc,
                                               double w) {
     return __fma_rn(w, __dsub_rn(s0, __dmul_rn(q, sc)), __dmul_rn(xc, sc));
@@ -583,6 +588,7 @@ __global__ void __launch_bounds__(256) k_sten(SolverArgs a, Coef<T> c, SolverBuf
 constexpr int PJ = 16;        // output rows per block
 constexpr int PW = PJ + 6;    // warps per block
 constexpr int PD = 3;         // planes of r/a_p, v1/a_p (and old p) copied ahead
+constexpr int PR = 3;         // planes of 1/a_p kept (formed by stage 1, used by 2 and 3)
 
 // 16-byte asynchronous global -> shared copy (cp.async, L2 only) and its
 // group bookkeeping: a lane reads back only the slots it filled itself, so
@@ -604,6 +610,7 @@ __global__ void __launch_bounds__(PW * 32, 1)
     // [PD][rh, vh, p][warp][lane]
     extern __shared__ float4 sbuf[];
     float4* ring = sbuf + 3 * 2 * PW * 32;
+    float4* rring = ring + PD * 3 * PW * 32;  // [PR][warp][lane]: 1/a_p of a plane
     pdl_wait();
     pdl_launch();
     if (S->done || S->pause) return;
@@ -621,9 +628,22 @@ __global__ void __launch_bounds__(PW * 32, 1)
     const int i0 = 1 + blockIdx.y * ni, i1 = min(i0 + ni - 1, ip);
     const int K = d.K, KJ = d.K * d.J;
     const int col = (live ? k0 : 1) + K * jw;
+    // the k part of a_p per lane, the same in every warp: kept in shared
+    // memory (stage 1 reads it once per step), written by warp 0 before the
+    // first step's barrier (stage 1 starts at the third step)
+    __shared__ float4 s_apk[32];
     float au[4], ad[4];
     vld(c.au + (live ? k0 : 1), au);
     vld(c.ad + (live ? k0 : 1), ad);
+    if (w == 0)
+        s_apk[lane] = make_float4(-au[0] - ad[0], -au[1] - ad[1], -au[2] - ad[2], -au[3] - ad[3]);
+    // Neumann rows (dynamics.f90:206-211): the mirrored neighbour equals the
+    // centre, so its difference term vanishes; zeroing its coefficient here
+    // replaces a select per element and sweep
+    if (k0 == 1) ad[0] = 0.0f;
+#pragma unroll
+    for (int e = 0; e < 4; e++)
+        if (k0 + e == kp) au[e] = 0.0f;
     const float an = ld(c.an + jw), as = ld(c.as + jw);
     const float bet = (float)S->bet, omg = (float)S->omg, alf = (float)S->alf;
     const bool first = S->it == 0 || S->fresh;
@@ -671,30 +691,49 @@ __global__ void __launch_bounds__(PW * 32, 1)
     };
     // one Jacobi sweep at plane q: res = xc + s0c - (A x)/a_p (the
     // reference's sweep), or with CHEB cheb_update(xc, s0c, (A x)/a_p, sc, wv);
-    // A in the FP32 difference form of sten_task
-    auto sweep = [&](int iq, const float (&xm)[4], const float (&xc)[4], const float (&xp)[4],
-                     const float4 xs4, const float4 xn4, const float (&s0c)[4], float (&res)[4],
-                     float sc, float wv) {
+    // A in the FP32 difference form of sten_task.  (A x)/a_p is formed as
+    // (A x) * (1/a_p): stage 1 (FIRST) forms 1/a_p of its plane and keeps it
+    // in this lane's slot of the 1/a_p ring, where stages 2 and 3 find it
+    // one and two steps later (a lane reads back only its own slot).
+    auto sweep = [&](auto first_c, int iq, const float (&xm)[4], const float (&xc)[4],
+                     const float (&xp)[4], const float4 xs4, const float4 xn4,
+                     const float (&s0c)[4], float (&res)[4], float sc, float wv, float4& rslot4) {
+        constexpr bool FIRST = decltype(first_c)::value;
         const float ae = ld(c.ae + iq), aw = ld(c.aw + iq);
-        const float sij = -ae - aw - an - as;
         const float xs[4] = {xs4.x, xs4.y, xs4.z, xs4.w}, xn[4] = {xn4.x, xn4.y, xn4.z, xn4.w};
-        float prev = __shfl_up_sync(0xffffffffu, xc[3], 1);
-        float next = __shfl_down_sync(0xffffffffu, xc[0], 1);
+        float ri[4];
+        if (FIRST) {
+            const float sij = -ae - aw - an - as;
+            const float4 k4 = s_apk[lane];
+            const float apk[4] = {k4.x, k4.y, k4.z, k4.w};
+#pragma unroll
+            for (int e = 0; e < 4; e++) ri[e] = __fdividef(1.0f, sij + apk[e]);
+            rslot4 = make_float4(ri[0], ri[1], ri[2], ri[3]);
+        } else {
+            const float4 r4 = rslot4;
+            ri[0] = r4.x;
+            ri[1] = r4.y;
+            ri[2] = r4.z;
+            ri[3] = r4.w;
+        }
+        const float prev = __shfl_up_sync(0xffffffffu, xc[3], 1);
+        const float next = __shfl_down_sync(0xffffffffu, xc[0], 1);
 #pragma unroll
         for (int e = 0; e < 4; e++) {
-            const int kk = k0 + e;
-            float xd = e == 0 ? prev : xc[e - 1];
-            float xu = e == 3 ? next : xc[e + 1];
-            xd = kk == 1 ? xc[e] : xd;
-            xu = kk == kp ? xc[e] : xu;
-            const float ap = sij - au[e] - ad[e];
+            const float xd = e == 0 ? prev : xc[e - 1];
+            const float xu = e == 3 ? next : xc[e + 1];
             const float c0 = xc[e];
             const float Ax = aw * (xm[e] - c0) + ae * (xp[e] - c0) + as * (xs[e] - c0) +
                              an * (xn[e] - c0) + ad[e] * (xd - c0) + au[e] * (xu - c0);
-            const float q = sweep_div(Ax, ap);
-            res[e] = CHEB ? cheb_update(xc[e], s0c[e], q, sc, wv) : xc[e] + s0c[e] - q;
+            const float q = Ax * ri[e];
+            if (CHEB)
+                res[e] = FIRST ? cheb_update(xc[e], s0c[e], q, sc, wv)
+                               : cheb_update1(xc[e], s0c[e], q, wv);
+            else
+                res[e] = xc[e] + s0c[e] - q;
         }
     };
+    auto rinv_slot = [&](int r) -> float4& { return rring[(r * PW + w) * 32 + lane]; };
     float R0[4][4], R1[3][4], R2[3][4];  // s0 at b..b+3, s1 at b..b+2, s2 at b-1..b+1
 #pragma unroll
     for (int r = 0; r < 4; r++)
@@ -707,6 +746,10 @@ __global__ void __launch_bounds__(PW * 32, 1)
 #pragma unroll
     for (int t = 0; t < PD; t++) fetch(t);
     int q1 = wrapn(bstart + 1, ip), q2 = wrapn(bstart + 2, ip);  // planes b+1, b+2 wrapped
+    // 1/a_p ring slots: plane b (stage 3), b+1 (stage 2), b+2 (stage 1)
+    int r3 = 0, r2 = 1, r1 = 2;
+    using yes = std::integral_constant<bool, true>;
+    using no = std::integral_constant<bool, false>;
     for (int b = bstart; b <= i1; b++) {
         const int t = b - bstart;
         const int cur = t & 1, prv = cur ^ 1;
@@ -715,19 +758,19 @@ __global__ void __launch_bounds__(PW * 32, 1)
         s0_at(t, R0[3]);
         // stage 1: s1 at plane b+2 (j neighbours: s0 at b+2 from the last step)
         if (st1 && b >= i0 - 4) {
-            sweep(q2, R0[1], R0[2], R0[3], slot(0, prv, w - 1), slot(0, prv, w + 1), R0[2],
-                  R1[2], w1, w2);
+            sweep(yes{}, q2, R0[1], R0[2], R0[3], slot(0, prv, w - 1), slot(0, prv, w + 1), R0[2],
+                  R1[2], w1, w2, rinv_slot(r1));
         }
         // stage 2: s2 at plane b+1
         if (st2 && b >= i0 - 2) {
-            sweep(q1, R1[0], R1[1], R1[2], slot(1, prv, w - 1), slot(1, prv, w + 1), R0[1],
-                  R2[2], 1.0f, w3);
+            sweep(no{}, q1, R1[0], R1[1], R1[2], slot(1, prv, w - 1), slot(1, prv, w + 1), R0[1],
+                  R2[2], 1.0f, w3, rinv_slot(r2));
         }
         // stage 3: s3 at plane b, the output
         if (outrow && b >= i0) {
             float s3[4];
-            sweep(b, R2[0], R2[1], R2[2], slot(2, prv, w - 1), slot(2, prv, w + 1), R0[0], s3,
-                  1.0f, w4);
+            sweep(no{}, b, R2[0], R2[1], R2[2], slot(2, prv, w - 1), slot(2, prv, w + 1), R0[0],
+                  s3, 1.0f, w4, rinv_slot(r3));
             const int o = col + KJ * b;
             if (MODE == 0) {
                 if (first) {
@@ -749,6 +792,12 @@ __global__ void __launch_bounds__(PW * 32, 1)
         fetch(t + PD);  // into the ring slot step t has finished with
         q1 = q2;
         q2 = q2 == ip ? 1 : q2 + 1;
+        {  // plane b+3 (stage 1's next plane) takes the slot plane b used
+            const int rr = r3;
+            r3 = r2;
+            r2 = r1;
+            r1 = rr;
+        }
         __syncthreads();
 #pragma unroll
         for (int e = 0; e < 4; e++) {
@@ -1013,7 +1062,7 @@ static void sten(const SolverArgs& a, const Coef<T>& c, const SolverBufs& B, Sol
     }
 }
 
-constexpr size_t PRECOND3_SMEM = sizeof(float4) * (3 * 2 + PD * 3) * PW * 32;
+constexpr size_t PRECOND3_SMEM = sizeof(float4) * (3 * 2 + PD * 3 + PR) * PW * 32;
 
 // the fused preconditioner applies (FP32, one k-chunk per column)
 template <typename T>
