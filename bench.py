@@ -638,6 +638,7 @@ def run_case(args):
         core.solver_graphs(0 if args.host_loop else args.graphs)
     if args.fuse is not None:
         core.set_launch_shape(1, fuse=args.fuse)
+    core.set_mpdata_shape(bool(args.mp_fuse), args.mp_rows)
     kw = dict(nq=c.nq, c_s=c.c_s, c_e=c.c_e) if c.nq else {}
     if args.viscous:
         kw["viscous"] = dict(lamsq=cases.mixing_length_sq(c.grid, 0.23, 0.1), z0=0.1, z0th=0.1)
@@ -708,6 +709,11 @@ def main():
                     help="mixed form: the reliable-update factor")
     ap.add_argument("--fuse", type=int, default=None, choices=[0, 1],
                     help="FP32 preconditioner: separate sweeps (0) or the fused kernel (1)")
+    ap.add_argument("--mp-fuse", type=int, default=0, choices=[0, 1],
+                    help="MPDATA: one fused kernel per antidiffusive iteration (1) or one "
+                         "kernel per stage (0)")
+    ap.add_argument("--mp-rows", type=int, default=32,
+                    help="MPDATA: cap on the fused kernel's rows per block")
     ap.add_argument("--profile", action="store_true")
     ap.add_argument("--output", default=None,
                     help="netCDF file written before every --output-every steps")

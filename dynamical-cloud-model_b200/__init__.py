@@ -123,6 +123,7 @@ def library():
             "dcm_solver_graphs": [P, C.c_int],
             "dcm_solver_graph_info": [P, C.POINTER(C.c_int)],
             "dcm_solver_limits": [P, C.c_int, C.c_double],
+            "dcm_set_mpdata_shape": [P, C.c_int, C.c_int],
             "dcm_tune": [P, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
                          C.POINTER(C.c_int), C.POINTER(C.c_int)],
             "dcm_set_launch_shape": [P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int],
@@ -156,7 +157,7 @@ EXPORTS = ("dcm_create", "dcm_destroy", "dcm_status_string", "dcm_last_error",
            "dcm_exchange_along_dim", "dcm_exchange_along_dim_wo", "dcm_state_upload",
            "dcm_driver_start", "dcm_step", "dcm_state_download", "dcm_profile_enable",
            "dcm_profile_read", "dcm_horizontal_means_noalloc", "dcm_solver_graphs",
-           "dcm_solver_graph_info", "dcm_solver_limits", "dcm_tune",
+           "dcm_solver_graph_info", "dcm_solver_limits", "dcm_set_mpdata_shape", "dcm_tune",
            "dcm_set_launch_shape", "dcm_ensemble_create", "dcm_ensemble_destroy", "dcm_ensemble_member",
            "dcm_ensemble_step", "dcm_ensemble_last_error", "dcm_exchange_full_wo",
            "dcm_calculate_subgrid_3d", "dcm_output_open", "dcm_output_write",
@@ -470,6 +471,11 @@ class DynamicalCore:
         (False or 0)."""
         mode = on if isinstance(on, int) and not isinstance(on, bool) else int(bool(on))
         self._check(self.lib.dcm_solver_graphs(self.h, mode))
+
+    def set_mpdata_shape(self, fuse=False, max_rows=32):
+        """MPDATA iterations as one kernel per stage (default) or one fused
+        kernel each; max_rows caps the fused kernel's rows per block."""
+        self._check(self.lib.dcm_set_mpdata_shape(self.h, int(bool(fuse)), int(max_rows)))
 
     def solver_limits(self, max_rounds=0, tiny=-1.0):
         """Failure-path limits of later solves: a round budget of the

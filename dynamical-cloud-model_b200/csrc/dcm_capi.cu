@@ -106,6 +106,9 @@ struct dcm_handle {
     // the FP64 breakdown threshold (< 0: the reference's tiny)
     int round_budget = 0;
     double tiny = -1.0;
+    // dcm_set_mpdata_shape: fused antidiffusive iterations (off by default:
+    // slower on B200, see dcm.h), their row cap
+    int mp_fuse = 0, mp_rows = 32;
     // bumped whenever captured pointers or launch shapes change (state
     // upload, tuning); an ensemble rebuilds its step graphs when it moves
     unsigned generation = 0;
@@ -297,6 +300,8 @@ bool mpdata_work(dcm_handle* h, int nq, MpBufs& b) {
     b.w.M = h->M;
     b.w.Mone = h->M + NQMAX;
     b.w.Mzero = h->M + NQMAX + 1;
+    b.w.fuse = h->mp_fuse;
+    b.w.fuse_rows = h->mp_rows;
     return true;
 }
 
@@ -375,6 +380,7 @@ extern "C" int dcm_create(const dcm_grid* g, int device, dcm_handle** out) {
     CK(cudaSetDevice(device));
     CK(cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking));
     solver_init();
+    mpdata_init();
     CK(cudaEventCreate(&h->ev0));
     CK(cudaEventCreate(&h->ev1));
     const size_t I2 = g->ip + 2, J2 = g->jp + 2, K2 = g->kp + 2;
@@ -986,6 +992,8 @@ bool mpdata_work_t(dcm_handle* h, int nq, MpBufsT<T>& b) {
     b.w.M = h->M;
     b.w.Mone = h->M + NQMAX;
     b.w.Mzero = h->M + NQMAX + 1;
+    b.w.fuse = h->mp_fuse;
+    b.w.fuse_rows = h->mp_rows;
     return true;
 }
 
@@ -1453,6 +1461,16 @@ extern "C" int dcm_solver_graphs(dcm_handle* h, int on) {
     const int mode = on == 0 ? 0 : on == 2 ? 2 : 1;
     if (mode != h->graphs) h->generation += 1;  // an ensemble recaptures its steps
     h->graphs = mode;
+    return DCM_OK;
+}
+
+extern "C" int dcm_set_mpdata_shape(dcm_handle* h, int fuse, int max_rows) {
+    CHECK_H();
+    if (max_rows < 3 || max_rows > 32) return fail(h, DCM_E_ARG, "set_mpdata_shape: max_rows");
+    const int f = fuse ? 1 : 0;
+    if (f != h->mp_fuse || max_rows != h->mp_rows) h->generation += 1;
+    h->mp_fuse = f;
+    h->mp_rows = max_rows;
     return DCM_OK;
 }
 

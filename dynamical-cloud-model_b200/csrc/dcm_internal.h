@@ -132,7 +132,15 @@ struct MpdataWork {
     MpScalars* M;      // [nq]
     MpScalars* Mone;   // early = 1 (used when kord < 1)
     MpScalars* Mzero;  // all zero
+    // antidiffusive iterations fused into one kernel each (k_mpdata_iter);
+    // fuse_rows caps its rows per block (32 = no cap)
+    int fuse = 0;
+    int fuse_rows = 32;
 };
+
+// one-time setup of the MPDATA kernels (shared-memory limits of the fused
+// iteration); called at handle creation, outside any stream capture
+void mpdata_init();
 
 // Jacobi-preconditioned BiCGSTAB (dynamics.f90:293-444) on x, b in the
 // pitched layout.  With w.graph set (and event profiling off) the whole solve

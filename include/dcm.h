@@ -333,6 +333,20 @@ int dcm_profile_read(dcm_handle *h, double *ms, long long *launches, int ncat);
  * results; while event timing is enabled the host-driven loop is used. */
 int dcm_solver_graphs(dcm_handle *h, int on);
 
+/* MPDATA launch shape (no counterpart in the reference).  fuse = 0 (the
+ * default): one kernel per stage of an antidiffusive iteration
+ * (antidiffusive velocities, betas, limited velocities, donor cell).
+ * fuse = 1: each antidiffusive iteration of mpdata_3d / mpdata_vec_3d with
+ * the linked limiter (or without the limiter) runs as one kernel that
+ * forms those four stages plane by plane in shared memory, so that only the
+ * limited velocities and the new field reach memory (9 field passes per
+ * iteration instead of 27).  On a B200 the fused form is 2-3.4x slower: the
+ * antidiffusive velocities read about 40 neighbour values per point and
+ * depend on L1, which the fused kernel's shared-memory planes take.
+ * max_rows (3..32) caps the rows of a block of the fused kernel (32: as many
+ * as its shared memory holds).  Both give the same arithmetic per point. */
+int dcm_set_mpdata_shape(dcm_handle *h, int fuse, int max_rows);
+
 /* Limits of the pressure solve's failure paths (no counterpart in the
  * reference; the tests use them to reach DCM_E_TIMEOUT and DCM_E_BREAKDOWN
  * without a singular system).  max_rounds > 0 bounds a graph-driven solve
