@@ -620,6 +620,56 @@ def run_reference(args, rank, world):
                     "d2h_bytes_per_step": 0}}
 
 
+def accuracy_vs_oracle(args):
+    """--accuracy-vs-oracle N: the mixed form (as the benchmark runs it) and
+    the FP64 path on the GPU, and the oracle's FP64 restatement of the
+    reference on all host cores, each N steps from the same seeded state;
+    per-field max and RMS errors (relative to max|oracle|; p on its live
+    cells with the mean removed) after 1, 10 and N steps, one JSON line.
+    The oracle's dot products are summed per thread (its fast mode), which
+    moves its own result by the summation-order spread only."""
+    pkg = load_pkg()
+    case = make_case(pkg, args.case)
+    g = case.grid
+    n = args.accuracy_vs_oracle
+    marks = sorted({1, 10, n})
+    kw = dict(ptol=case.ptol, kord=case.kord, monotone=case.monotone)
+
+    def keep(f):
+        return {k: np.array(f[k], copy=True) for k in ("u", "v", "w", "th", "p")}
+
+    snaps = {}
+    for prec in (1, 0):
+        core = pkg.DynamicalCore(g, device=args.device)
+        core.upload_state(case.state, case.dt, precision=prec, **kw,
+                          **(dict(precond=1, precond_lo=0.05) if prec else {}))
+        core.driver_start()
+        done = 0
+        for mk in marks:
+            core.step(mk - done)
+            done = mk
+            snaps[(prec, mk)] = keep(core.download_state())
+        core.close()
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    oracle.set_threads(os.cpu_count() or 1, True)
+    m = oracle.OracleModel(g, case.state, case.dt, **kw)
+    m.driver_start()
+    t0 = time.perf_counter()
+    done = 0
+    out = {"case": case.name, "steps": n, "oracle_threads": os.cpu_count(), "errors": {}}
+    for mk in marks:
+        m.step(mk - done)
+        done = mk
+        ref = keep(m.fields())
+        out["errors"][str(mk)] = {
+            "mixed_vs_oracle": field_errors(g, ref, snaps[(1, mk)]),
+            "fp64_vs_oracle": field_errors(g, ref, snaps[(0, mk)]),
+            "mixed_vs_fp64": field_errors(g, snaps[(0, mk)], snaps[(1, mk)])}
+    out["oracle_s"] = time.perf_counter() - t0
+    print(json.dumps(out), flush=True)
+
+
 def run_case(args):
     """--run-case: K time steps of a named case through the C-ABI, one line
     per step (solver iterations, FP64 updates and restarts of the mixed
@@ -718,9 +768,14 @@ def main():
     ap.add_argument("--output", default=None,
                     help="netCDF file written before every --output-every steps")
     ap.add_argument("--output-every", type=int, default=1)
+    ap.add_argument("--accuracy-vs-oracle", type=int, default=0,
+                    help="N: errors of both forms against the oracle after 1, 10, N steps")
     args = ap.parse_args()
     if args.run_case:
         run_case(args)
+        return
+    if args.accuracy_vs_oracle:
+        accuracy_vs_oracle(args)
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
