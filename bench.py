@@ -757,8 +757,9 @@ def main():
     ap.add_argument("--precond-lo", type=float, default=0.05)
     ap.add_argument("--inner-tol", type=float, default=0.1,
                     help="mixed form: the reliable-update factor")
-    ap.add_argument("--fuse", type=int, default=None, choices=[0, 1],
-                    help="FP32 preconditioner: separate sweeps (0) or the fused kernel (1)")
+    ap.add_argument("--fuse", type=int, default=None, choices=[0, 1, 2],
+                    help="FP32 preconditioner: separate sweeps (0), the fused kernel (1), or "
+                         "the fused kernel with phase C's matvec as a fourth stage (2)")
     ap.add_argument("--mp-fuse", type=int, default=0, choices=[0, 1],
                     help="MPDATA: one fused kernel per antidiffusive iteration (1) or one "
                          "kernel per stage (0)")

@@ -1634,11 +1634,13 @@ extern "C" int dcm_tune(dcm_handle* h, int precision, int use_cache, int* by, in
                 for (int ni = 0; ni < 4; ni++)
                     if (!consider(BYS[bi], TASKS[ti], DEPTHS[ni], 0))
                         return fail(h, DCM_E_CUDA, "tune: a candidate launch shape failed");
-        // the fused preconditioner (FP32): the sweep shape does not apply
+        // the fused preconditioner (FP32), without (1) and with (2) phase C's
+        // matvec as its fourth stage: the sweep shape does not apply
         if (precision == 1)
-            for (int ti = 0; ti < 3; ti++)
-                if (!consider(8, TASKS[ti], 4, 1))
-                    return fail(h, DCM_E_CUDA, "tune: a candidate launch shape failed");
+            for (int fv = 1; fv <= 2; fv++)
+                for (int ti = 0; ti < 3; ti++)
+                    if (!consider(8, TASKS[ti], 4, fv))
+                        return fail(h, DCM_E_CUDA, "tune: a candidate launch shape failed");
         tune_store(sms, h->d, precision, b0, t0, n0, f0, best);
     }
     h->tune_by[precision] = b0;
@@ -1657,7 +1659,7 @@ extern "C" int dcm_set_launch_shape(dcm_handle* h, int precision, int by, int ta
                                     int fuse) {
     CHECK_H();
     if ((precision != 0 && precision != 1) || by < 1 || by > 8 || tasks < 0 || tasks > 15 ||
-        depth < 1 || depth > 63 || (fuse != 0 && fuse != 1))
+        depth < 1 || depth > 63 || fuse < 0 || fuse > 2)
         return fail(h, DCM_E_ARG, "set_launch_shape: bad argument");
     h->tune_by[precision] = by;
     h->tune_tasks[precision] = tasks;

@@ -79,6 +79,7 @@ struct SolverArgs {
     int max_blocks;   // blocks a reducing kernel may use (partials capacity)
     int ni;           // i-planes a stencil warp task marches over
     int fuse;         // FP32: the three sweeps of a phase as one kernel (k_precond3)
+    int fuse_mv = 0;  // with fuse: phase C's matvec as the fused kernel's fourth stage
     // Chebyshev-weighted sweeps (mixed form only): x1 = cw[0] s0, then
     // x_m+1 = x_m + cw[m] (s0 - (A x_m)/a_p), m = 1..3, in place of the
     // reference's x1 = s0, x_m+1 = x_m + s0 - (A x_m)/a_p
@@ -603,14 +604,37 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 
 __device__ __forceinline__ int wrapn(int q, int n) { return ((q - 1) % n + n) % n + 1; }
 
-template <int MODE, bool CHEB>
-__global__ void __launch_bounds__(PW * 32, 1)
-    k_precond3(SolverArgs a, Coef<float> c, SolverBufs B, const SolverScalars* S, int ni) {
-    // [stage 0..2][buffer 0..1][warp][lane], then the copy-ahead ring
-    // [PD][rh, vh, p][warp][lane]
+// MV (phase C only): a fourth stage forms t = A cs at plane b-1 of the
+// output rows with the dots (t,t) and (t,s), s = r - alf v1 (the matvec of
+// :409-413 that otherwise runs as its own kernel), so the block keeps one
+// more halo row each side (stage 3 runs on the rows j0-1 .. j0+PJ, whose cs
+// it keeps in shared memory only) and marches one plane further.
+template <int MODE, bool MV>
+constexpr int precond3_warps() { return MV ? PJ + 8 : PW; }
+template <int MODE, bool MV>
+constexpr size_t precond3_smem() {
+    // [stage slots][2][warp][lane] + copy-ahead [PD][arrays][warp][lane]
+    // + 1/a_p ring [PR][warp][lane], float4 each
+    return sizeof(float4) * ((MV ? 4 : 3) * 2 + PD * (MODE == 0 ? 3 : 2) + PR) *
+           precond3_warps<MODE, MV>() * 32;
+}
+
+template <int MODE, bool CHEB, bool MV = false>
+__global__ void __launch_bounds__(precond3_warps<MODE, MV>() * 32, 1)
+    k_precond3(SolverArgs a, Coef<float> c, SolverBufs B, SolverScalars* S, int ni, Red2 R) {
+    static_assert(!MV || MODE == 1, "the fused matvec stage is phase C's");
+    constexpr int PWK = precond3_warps<MODE, MV>();
+    constexpr int HW = MV ? 4 : 3;              // rows before the first output row
+    constexpr int NSL = MV ? 4 : 3;             // stages with shared slots
+    constexpr int NARR = MODE == 0 ? 3 : 2;     // streamed arrays: r/a_p, v1/a_p (, old p)
+    constexpr int E = MV ? 1 : 0;               // extra planes of lead
+    // [stage 0..NSL-1][buffer 0..1][warp][lane], then the copy-ahead ring
+    // [PD][rh, vh (, p)][warp][lane], then the 1/a_p ring
     extern __shared__ float4 sbuf[];
-    float4* ring = sbuf + 3 * 2 * PW * 32;
-    float4* rring = ring + PD * 3 * PW * 32;  // [PR][warp][lane]: 1/a_p of a plane
+    float4* ring = sbuf + NSL * 2 * PWK * 32;
+    float4* rring = ring + PD * NARR * PWK * 32;  // [PR][warp][lane]: 1/a_p of a plane
+    __shared__ double red_smem[64];
+    double acc[2] = {0.0, 0.0};  // MV: (t,t), (t,s)
     pdl_wait();
     pdl_launch();
     if (S->done || S->pause) return;
@@ -621,10 +645,11 @@ __global__ void __launch_bounds__(PW * 32, 1)
     const bool live = k0 <= kp;
     const int nvalid = live ? min(4, kp - k0 + 1) : 0;
     const int j0 = 1 + blockIdx.x * PJ;
-    const int jrow = j0 - 3 + w;
+    const int jrow = j0 - HW + w;
     const int jw = wrapn(jrow, jp);
-    const bool outrow = w >= 3 && w < 3 + PJ && jrow <= jp;
-    const bool st1 = w >= 1 && w <= PW - 2, st2 = w >= 2 && w <= PW - 3;
+    const bool outrow = w >= HW && w < HW + PJ && jrow <= jp;
+    const bool st1 = w >= 1 && w <= PWK - 2, st2 = w >= 2 && w <= PWK - 3;
+    const bool st3 = MV ? (w >= 3 && w <= PWK - 4) : outrow;
     const int i0 = 1 + blockIdx.y * ni, i1 = min(i0 + ni - 1, ip);
     const int K = d.K, KJ = d.K * d.J;
     const int col = (live ? k0 : 1) + K * jw;
@@ -655,14 +680,14 @@ __global__ void __launch_bounds__(PW * 32, 1)
     const float* __restrict__ vh = (const float*)B.vh;
     float* __restrict__ out = (float*)B.out;
     auto slot = [&](int stage, int buf, int warp) -> float4& {
-        return sbuf[((stage * 2 + buf) * PW + warp) * 32 + lane];
+        return sbuf[((stage * 2 + buf) * PWK + warp) * 32 + lane];
     };
     auto f4 = [](const float (&v)[4]) { return make_float4(v[0], v[1], v[2], v[3]); };
     auto rslot = [&](int step, int arr) -> float4& {
-        return ring[(((step % PD) * 3 + arr) * PW + w) * 32 + lane];
+        return ring[(((step % PD) * NARR + arr) * PWK + w) * 32 + lane];
     };
     // copy-ahead of step t: r/a_p and v1/a_p at plane b+3, old p at plane b
-    const int bstart = i0 - 6, nsteps = i1 - bstart + 1;
+    const int bstart = i0 - 6 - E, bend = i1 + E, nsteps = bend - bstart + 1;
     int qf = wrapn(bstart + 3, ip);  // plane of the next fetch, wrapped into 1..ip
     auto fetch = [&](int t) {
         if (t < nsteps) {
@@ -733,7 +758,7 @@ __global__ void __launch_bounds__(PW * 32, 1)
                 res[e] = xc[e] + s0c[e] - q;
         }
     };
-    auto rinv_slot = [&](int r) -> float4& { return rring[(r * PW + w) * 32 + lane]; };
+    auto rinv_slot = [&](int r) -> float4& { return rring[(r * PWK + w) * 32 + lane]; };
     float R0[4][4], R1[3][4], R2[3][4];  // s0 at b..b+3, s1 at b..b+2, s2 at b-1..b+1
 #pragma unroll
     for (int r = 0; r < 4; r++)
@@ -750,26 +775,31 @@ __global__ void __launch_bounds__(PW * 32, 1)
     int r3 = 0, r2 = 1, r1 = 2;
     using yes = std::integral_constant<bool, true>;
     using no = std::integral_constant<bool, false>;
-    for (int b = bstart; b <= i1; b++) {
+    float xm4[4] = {0.0f, 0.0f, 0.0f, 0.0f};  // MV: own cs at plane b-2
+    const float* __restrict__ rr = (const float*)B.r;
+    const float* __restrict__ rv1 = (const float*)B.v1;
+    float* __restrict__ tout = (float*)B.out2;
+    for (int b = bstart; b <= bend; b++) {
         const int t = b - bstart;
         const int cur = t & 1, prv = cur ^ 1;
         cp_async_wait<PD - 1>();  // this lane's copies of step t have landed
         // stage 0: s0 at plane b+3
         s0_at(t, R0[3]);
         // stage 1: s1 at plane b+2 (j neighbours: s0 at b+2 from the last step)
-        if (st1 && b >= i0 - 4) {
+        if (st1 && b >= i0 - 4 - E) {
             sweep(yes{}, q2, R0[1], R0[2], R0[3], slot(0, prv, w - 1), slot(0, prv, w + 1), R0[2],
                   R1[2], w1, w2, rinv_slot(r1));
         }
         // stage 2: s2 at plane b+1
-        if (st2 && b >= i0 - 2) {
+        if (st2 && b >= i0 - 2 - E) {
             sweep(no{}, q1, R1[0], R1[1], R1[2], slot(1, prv, w - 1), slot(1, prv, w + 1), R0[1],
                   R2[2], 1.0f, w3, rinv_slot(r2));
         }
         // stage 3: s3 at plane b, the output
-        if (outrow && b >= i0) {
-            float s3[4];
-            sweep(no{}, b, R2[0], R2[1], R2[2], slot(2, prv, w - 1), slot(2, prv, w + 1), R0[0],
+        float s3[4];
+        if (st3 && b >= i0 - E) {
+            const int qb = MV ? wrapn(b, ip) : b;
+            sweep(no{}, qb, R2[0], R2[1], R2[2], slot(2, prv, w - 1), slot(2, prv, w + 1), R0[0],
                   s3, 1.0f, w4, rinv_slot(r3));
             const int o = col + KJ * b;
             if (MODE == 0) {
@@ -783,7 +813,43 @@ __global__ void __launch_bounds__(PW * 32, 1)
                     for (int e = 0; e < 4; e++) s3[e] = s3[e] + bet * po[e];
                 }
             }
-            if (live) vst(out + o, s3, nvalid);
+            if (MV) slot(3, cur, w) = f4(s3);
+            if (live && outrow && b >= i0 && b <= i1) vst(out + o, s3, nvalid);
+        }
+        // stage 4 (MV): t = A cs at plane b-1 of the output rows, (t,t), (t,s)
+        if (MV && outrow && b >= i0) {
+            const float4 c4 = slot(3, prv, w);  // own cs at plane b-1
+            const float xc[4] = {c4.x, c4.y, c4.z, c4.w};
+            if (b >= i0 + 1) {
+                const int qm = wrapn(b - 1, ip);
+                const float ae = ld(c.ae + qm), aw = ld(c.aw + qm);
+                const float4 xs4 = slot(3, prv, w - 1), xn4 = slot(3, prv, w + 1);
+                const float xs[4] = {xs4.x, xs4.y, xs4.z, xs4.w};
+                const float xn[4] = {xn4.x, xn4.y, xn4.z, xn4.w};
+                const float prev = __shfl_up_sync(0xffffffffu, xc[3], 1);
+                const float next = __shfl_down_sync(0xffffffffu, xc[0], 1);
+                const int o = col + KJ * qm;
+                float rv[4], v1v[4], t[4];
+                vld(rr + o, rv);
+                vld(rv1 + o, v1v);
+#pragma unroll
+                for (int e = 0; e < 4; e++) {
+                    const float xd = e == 0 ? prev : xc[e - 1];
+                    const float xu = e == 3 ? next : xc[e + 1];
+                    const float c0 = xc[e];
+                    // the FP32 difference form of sten_task (mat_ax, :219-222)
+                    t[e] = aw * (xm4[e] - c0) + ae * (s3[e] - c0) + as * (xs[e] - c0) +
+                           an * (xn[e] - c0) + ad[e] * (xd - c0) + au[e] * (xu - c0);
+                    const float sv = rv[e] - alf * v1v[e];  // s of :404
+                    if (e < nvalid) {
+                        acc[0] += (double)t[e] * (double)t[e];
+                        acc[1] += (double)t[e] * (double)sv;
+                    }
+                }
+                if (live) vst(tout + o, t, nvalid);
+            }
+#pragma unroll
+            for (int e = 0; e < 4; e++) xm4[e] = xc[e];
         }
         // this step's values for the neighbours' next step
         slot(0, cur, w) = f4(R0[3]);
@@ -811,6 +877,7 @@ __global__ void __launch_bounds__(PW * 32, 1)
         }
     }
     cp_async_wait<0>();
+    if (MV) reduce_tail<OP_MATC, 2>(a, acc, R, red_smem, S);  // omega, :411-417
 }
 
 // Condition of a graph-driven loop: one more iteration while the solve has
@@ -1062,7 +1129,6 @@ static void sten(const SolverArgs& a, const Coef<T>& c, const SolverBufs& B, Sol
     }
 }
 
-constexpr size_t PRECOND3_SMEM = sizeof(float4) * (3 * 2 + PD * 3 + PR) * PW * 32;
 
 // the fused preconditioner applies (FP32, one k-chunk per column)
 template <typename T>
@@ -1073,22 +1139,31 @@ static bool fused_ok(const SolverArgs& a) {
 // one fused preconditioner launch: PJ-row strips x i-chunks, at most one
 // block per SM so that the chunks (and their 6-plane warm-up) are as long as
 // the SM count allows, and no chunk shorter than 8 planes
+// mv: phase C with the matvec t = A cs and its dots as a fourth stage
 static void precond3(const SolverArgs& a, const Coef<float>& c, const SolverBufs& B,
-                     SolverScalars* S, int mode, cudaStream_t st) {
+                     SolverScalars* S, int mode, bool mv, const Red2& R, cudaStream_t st) {
     ProfScope ps(P_JACOBI, st);
     const int nstrips = (a.d.jp + PJ - 1) / PJ;
     // chunks of at least 8 planes (each carries a 6-plane warm-up)
     const int nch = std::max(1, std::min((a.d.ip + 7) / 8, sm_count() / nstrips));
     const int ni = (a.d.ip + nch - 1) / nch;
     const dim3 grid(nstrips, (a.d.ip + ni - 1) / ni);
-    auto go = [&](auto kern) {
-        launch(a.pdl, kern, grid, dim3(PW * 32), PRECOND3_SMEM, st, a, c, B,
-               (const SolverScalars*)S, ni);
+    auto go = [&](auto kern, int warps, size_t smem) {
+        launch(a.pdl, kern, grid, dim3(warps * 32), smem, st, a, c, B, S, ni, R);
     };
-    if (mode == 0)
-        a.cheb ? go(k_precond3<0, true>) : go(k_precond3<0, false>);
-    else
-        a.cheb ? go(k_precond3<1, true>) : go(k_precond3<1, false>);
+    if (mode == 0) {
+        constexpr int wp = precond3_warps<0, false>();
+        constexpr size_t sm = precond3_smem<0, false>();
+        a.cheb ? go(k_precond3<0, true>, wp, sm) : go(k_precond3<0, false>, wp, sm);
+    } else if (!mv) {
+        constexpr int wp = precond3_warps<1, false>();
+        constexpr size_t sm = precond3_smem<1, false>();
+        a.cheb ? go(k_precond3<1, true>, wp, sm) : go(k_precond3<1, false>, wp, sm);
+    } else {
+        constexpr int wp = precond3_warps<1, true>();
+        constexpr size_t sm = precond3_smem<1, true>();
+        a.cheb ? go(k_precond3<1, true, true>, wp, sm) : go(k_precond3<1, false, true>, wp, sm);
+    }
 }
 
 // programmatic edges inside the graph-driven iterations (probed once)
@@ -1096,11 +1171,16 @@ static int g_pdl_graphs = 0;
 static bool probe_pdl_graphs();
 
 void solver_init() {
-    const int sm = (int)PRECOND3_SMEM;
-    cudaFuncSetAttribute(k_precond3<0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-    cudaFuncSetAttribute(k_precond3<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-    cudaFuncSetAttribute(k_precond3<0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-    cudaFuncSetAttribute(k_precond3<1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    const int sm0 = (int)precond3_smem<0, false>(), sm1 = (int)precond3_smem<1, false>(),
+              sm1m = (int)precond3_smem<1, true>();
+    cudaFuncSetAttribute(k_precond3<0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm0);
+    cudaFuncSetAttribute(k_precond3<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm1);
+    cudaFuncSetAttribute(k_precond3<0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm0);
+    cudaFuncSetAttribute(k_precond3<1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm1);
+    cudaFuncSetAttribute(k_precond3<1, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         sm1m);
+    cudaFuncSetAttribute(k_precond3<1, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         sm1m);
     static std::once_flag probed;  // handles may be created from several threads
     std::call_once(probed, [] { g_pdl_graphs = probe_pdl_graphs() ? 1 : 0; });
 }
@@ -1122,7 +1202,7 @@ static void launch_iteration(const SolverArgs& a, const Coef<T>& c, SolverWork<T
     if (fused) {
         if constexpr (std::is_same<T, float>::value) {
             B.out = w.p;
-            precond3(a0, c, B, w.S, 0, st);
+            precond3(a0, c, B, w.S, 0, false, w.red, st);
         }
     } else {
         B.out = w.sA;
@@ -1144,10 +1224,12 @@ static void launch_iteration(const SolverArgs& a, const Coef<T>& c, SolverWork<T
     sten<T, OP_MATP, 0>(a, c, B, w, st, P_MATVEC);
     // phase C: precondition(cs <- s), t = A cs
     B.sin = nullptr;
+    const bool mv = fused && a.fuse_mv;
     if (fused) {
         if constexpr (std::is_same<T, float>::value) {
             B.out = w.sA;
-            precond3(a, c, B, w.S, 1, st);
+            B.out2 = w.t;
+            precond3(a, c, B, w.S, 1, mv, w.red, st);
         }
     } else {
         B.out = w.sA;
@@ -1162,9 +1244,11 @@ static void launch_iteration(const SolverArgs& a, const Coef<T>& c, SolverWork<T
         B.sweep = 3;
         sten<T, OP_SW, 1>(a, c, B, w, st, P_JACOBI);
     }
-    B.sin = w.sA;
-    B.out = w.t;
-    sten<T, OP_MATC, 1>(a, c, B, w, st, P_MATVEC);
+    if (!mv) {
+        B.sin = w.sA;
+        B.out = w.t;
+        sten<T, OP_MATC, 1>(a, c, B, w, st, P_MATVEC);
+    }
     // phase D
     {
         ProfScope ps(P_UPDATE, st);
@@ -1340,6 +1424,7 @@ int solver_run(SolverWork<T>& w, const Dims& d, T* x, const T* b, const T* sw, c
     a.max_blocks = w.max_blocks;
     a.ni = w.ni >= 1 ? w.ni : 1;
     a.fuse = w.fuse;
+    a.fuse_mv = w.fuse == 2 ? 1 : 0;
     no_cheb(a);  // the FP64 path keeps the reference's sweeps
     if (w.tiny >= 0.0) a.tiny = w.tiny;
     const Coef<T> c = coef_of(w);
@@ -1384,7 +1469,7 @@ int solver_run(SolverWork<T>& w, const Dims& d, T* x, const T* b, const T* sw, c
         SolveGraph& G = *w.graph;
         const void* kp[6] = {x, b, sw, dzn, w.r, w.S};
         const double kd[3] = {tol, sc_floor, a.tiny};
-        // launch shape: by < 16, tasks < 16, ni < 64, fuse < 2, pdl < 2
+        // launch shape: by < 16, tasks < 16, ni < 64, fuse < 4, pdl < 2
         const int shape =
             a.by + 16 * a.tasks + 256 * a.ni + 16384 * a.fuse + 65536 * (w.pdl ? 1 : 0);
         const int ki[6] = {itmax, wo, (post ? 1 : 0) + 2 * max_rounds, (int)sizeof(T) + 16 * shape,
@@ -1414,7 +1499,7 @@ int solver_run(SolverWork<T>& w, const Dims& d, T* x, const T* b, const T* sw, c
         if (g_prof) {
             g_prof->add(P_SETUP, 1);
             g_prof->add(P_JACOBI, (fused_ok<T>(a) ? 2 : 6) * r);
-            g_prof->add(P_MATVEC, 2 * r);
+            g_prof->add(P_MATVEC, (fused_ok<T>(a) && a.fuse_mv ? 1 : 2) * r);
             g_prof->add(P_UPDATE, r);
             g_prof->add(P_OTHER, 1);
             if (post) g_prof->add(P_POST, 1);
@@ -1688,6 +1773,7 @@ int refine_run(SolverWork<float>& wf, SolverWork<double>& wd, const Dims& d, dou
     af.nkt = kchunks<float>(d);
     af.ni = wf.ni >= 1 ? wf.ni : 1;
     af.fuse = wf.fuse;
+    af.fuse_mv = wf.fuse == 2 ? 1 : 0;
     if (wf.cheb) {
         af.cheb = 1;
         cheb_weights(wf.cheb_lo, af.cw);
@@ -1771,7 +1857,7 @@ int refine_run(SolverWork<float>& wf, SolverWork<double>& wd, const Dims& d, dou
         const void* kp[6] = {x, b, sw, dzn, dx, wf.S};
         const double kd[3] = {tol, delta, af.cheb ? wf.cheb_lo : 0.0};
         const int shape = af.by + 16 * af.tasks + 256 * af.ni + 16384 * af.fuse +
-                          32768 * af.cheb + 65536 * (wf.pdl ? 1 : 0);
+                          65536 * af.cheb + 131072 * (wf.pdl ? 1 : 0);
         const int ki[6] = {itmax, max_updates, 1 + 2 * max_rounds, 16 * shape,
                            d.ip * 4096 + d.jp, d.kp};
         if (!G.matches(kp, kd, ki)) {
@@ -1821,7 +1907,7 @@ int refine_run(SolverWork<float>& wf, SolverWork<double>& wd, const Dims& d, dou
         const long long itr = hS_in->rounds, u = hS_in->ru_runs, cyc = hS_in->cycles;
         g_prof->add(P_SETUP, u + 1);
         g_prof->add(P_JACOBI, (fused_ok<float>(af) ? 2 : 6) * itr);
-        g_prof->add(P_MATVEC, 2 * itr);
+        g_prof->add(P_MATVEC, (fused_ok<float>(af) && af.fuse_mv ? 1 : 2) * itr);
         g_prof->add(P_UPDATE, itr + u + 1);
         g_prof->add(P_POST, 1);
         g_prof->add(P_OTHER, 3 * cyc + 3);

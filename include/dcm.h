@@ -374,7 +374,10 @@ int dcm_solver_graph_info(dcm_handle *h, int *programmatic);
  * each warp striding over many tasks; 1, 2 = that many tasks per warp), the
  * depth, the number of i-planes the first Jacobi sweep marches over (1, 2,
  * 4, 8), and in FP32 whether the three sweeps of each preconditioner
- * application run fused in one kernel (fuse: columns of at most 128 levels).
+ * application run fused in one kernel (fuse 1: columns of at most 128
+ * levels), and whether that kernel of phase C also forms t = A cs with its
+ * dots (t,t), (t,s) as a fourth stage (fuse 2; otherwise the matvec is a
+ * kernel of its own).
  * It times 12 BiCGSTAB iterations of each candidate on a synthetic
  * right-hand side and applies the fastest to the handle for that precision
  * (each precision keeps its own launch shape).  With use_cache the result is
@@ -386,8 +389,8 @@ int dcm_solver_graph_info(dcm_handle *h, int *programmatic);
 int dcm_tune(dcm_handle *h, int precision, int use_cache, int *by, int *tasks,
              int *depth, int *fuse);
 /* Sets the launch shape of one precision explicitly (same meaning and ranges
- * as dcm_tune's results; by <= 8, depth <= 63, fuse only for precision 1).
- * Default: by 8, tasks 0, depth 4, fuse 1 (FP32) / 0 (FP64). */
+ * as dcm_tune's results; by <= 8, depth <= 63, fuse 0..2 only for
+ * precision 1).  Default: by 8, tasks 0, depth 4, fuse 1 (FP32) / 0 (FP64). */
 int dcm_set_launch_shape(dcm_handle *h, int precision, int by, int tasks,
                          int depth, int fuse);
 

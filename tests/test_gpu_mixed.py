@@ -95,18 +95,21 @@ def test_graph_and_host_loops_agree(dcm, precision):
             assert np.array_equal(fa[n], fb[n]), n
 
 
+@pytest.mark.parametrize("fused", [1, 2])
 @pytest.mark.parametrize("precond", [0, 1])
-@pytest.mark.parametrize("shape", [(24, 20, 16), (9, 30, 37), (1, 16, 14), (40, 1, 12)])
-def test_fused_preconditioner_matches_unfused(dcm, shape, precond):
+@pytest.mark.parametrize("shape", [(24, 20, 16), (9, 30, 37), (1, 16, 14), (40, 1, 12),
+                                   (19, 37, 128)])
+def test_fused_preconditioner_matches_unfused(dcm, shape, precond, fused):
     """The fused three-sweep preconditioner (FP32) performs each point's
     arithmetic of the three separate sweeps, unweighted and Chebyshev
-    weighted: the two launch shapes give the same iterations and fields to
-    FP32 round-off, on strips and chunks that wrap (jp < 20, ip = 1) and on
-    ragged columns."""
+    weighted, and with fused = 2 phase C's matvec t = A cs and its dots as a
+    fourth stage: the launch shapes give the same iterations and fields to
+    FP32 round-off, on strips and chunks that wrap (jp < 20, ip = 1), on
+    ragged columns and on full 128-level columns."""
     ip, jp, kp = shape
     c = cases.warm_bubble(ip=ip, jp=jp, kp=kp, dxyz=50.0, radius=200.0, zc=200.0, seed=41)
     out = []
-    for fuse in (1, 0):
+    for fuse in (fused, 0):
         core = dcm.DynamicalCore(c.grid)
         core.set_launch_shape(1, fuse=fuse)
         core.upload_state(c.state, c.dt, ptol=c.ptol, kord=c.kord, precision=1,
