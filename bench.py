@@ -328,7 +328,8 @@ def run_b200(args, rank, world, local_rank, dist):
         return dict(ms=ms, iters=st.iters_total, launches=launches, clocks=clk,
                     classes=classes, value=world * N * args.steps / (ms / 1e3),
                     shape={"warps_per_sweep_block": shape[0], "tasks_per_warp": shape[1],
-                           "march_depth": shape[2], "fused_preconditioner": bool(shape[3])})
+                           "march_depth": shape[2], "fused_preconditioner": shape[3],
+                           "levels_per_lane": shape[4]})
 
     m32 = measure(1)
     m32ref = measure(1, precond={})  # mixed form with the reference's sweeps

@@ -125,8 +125,8 @@ def library():
             "dcm_solver_limits": [P, C.c_int, C.c_double],
             "dcm_set_mpdata_shape": [P, C.c_int, C.c_int],
             "dcm_tune": [P, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
-                         C.POINTER(C.c_int), C.POINTER(C.c_int)],
-            "dcm_set_launch_shape": [P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int],
+                         C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)],
+            "dcm_set_launch_shape": [P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int],
             "dcm_ensemble_create": [C.c_int, C.c_void_p, C.c_int, C.POINTER(C.c_void_p)],
             "dcm_ensemble_destroy": [P],
             "dcm_ensemble_member": [P, C.c_int, C.POINTER(C.c_void_p)],
@@ -229,18 +229,25 @@ class DynamicalCore:
 
     def tune(self, precision=1, use_cache=True):
         """Autotune the solver launch shape for this grid (dcm_tune); returns
-        (warps per sweep block, warp tasks per warp, marching depth, fused)."""
-        by, tasks, depth, fuse = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        (warps per sweep block, warp tasks per warp, marching depth, fused,
+        levels per lane)."""
+        by, tasks, depth, fuse, vec = C.c_int(), C.c_int(), C.c_int(), C.c_int(), C.c_int()
         self._check(self.lib.dcm_tune(self.h, int(precision), int(bool(use_cache)), C.byref(by),
-                                      C.byref(tasks), C.byref(depth), C.byref(fuse)))
-        return by.value, tasks.value, depth.value, fuse.value
+                                      C.byref(tasks), C.byref(depth), C.byref(fuse),
+                                      C.byref(vec)))
+        return by.value, tasks.value, depth.value, fuse.value, vec.value
 
-    def set_launch_shape(self, precision, by=8, tasks=0, depth=4, fuse=None):
-        """Set the solver launch shape of one precision (dcm_set_launch_shape)."""
+    def set_launch_shape(self, precision, by=8, tasks=0, depth=4, fuse=None, vec=None):
+        """Set the solver launch shape of one precision (dcm_set_launch_shape).
+        fuse: 0 separate sweeps, 1 fused preconditioner, 2 fused with phase
+        C's matvec (FP32); vec: levels per lane of the separate kernels (FP32
+        4 or 2, FP64 2)."""
         if fuse is None:
             fuse = 1 if precision == 1 else 0
+        if vec is None:
+            vec = 4 if precision == 1 else 2
         self._check(self.lib.dcm_set_launch_shape(self.h, int(precision), int(by), int(tasks),
-                                                  int(depth), int(fuse)))
+                                                  int(depth), int(fuse), int(vec)))
 
     def __del__(self):
         try:

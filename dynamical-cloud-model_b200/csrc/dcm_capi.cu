@@ -102,6 +102,7 @@ struct dcm_handle {
     // [1] the FP32 iterations of the mixed form): warps per sweep block, warp
     // tasks per warp of the reducing kernels (0 = fill the GPU), marching depth
     int tune_by[2] = {8, 8}, tune_tasks[2] = {0, 0}, tune_ni[2] = {4, 4}, tune_fuse[2] = {0, 1};
+    int tune_vec[2] = {2, 4};  // levels per lane (FP64 fixed at 2)
     // dcm_solver_limits: round budget of graph-driven solves (0: default) and
     // the FP64 breakdown threshold (< 0: the reference's tiny)
     int round_budget = 0;
@@ -1012,6 +1013,7 @@ SolverWork<float> solver_work_f(dcm_handle* h) {
     w.tasks = h->tune_tasks[1];
     w.ni = h->tune_ni[1];
     w.fuse = h->tune_fuse[1];
+    w.vw = h->tune_vec[1];
     w.max_blocks = (int)std::min<size_t>(h->npartials / 3, (size_t)1 << 30);
     w.cheb = h->cfg.precond == 1 ? 1 : 0;
     w.cheb_lo = h->cfg.precond_lo > 0.0 ? h->cfg.precond_lo : 0.05;
@@ -1518,33 +1520,40 @@ std::string tune_cache_path() {
     return std::string(home ? home : ".") + "/.cache/dcm_b200_solver_tune.txt";
 }
 
-// cache lines: "<sms> <ip> <jp> <kp> <precision> <by> <tasks> <depth> <fuse> <ms per iteration>"
-bool tune_lookup(int sms, const Dims& d, int prec, int* by, int* tasks, int* depth, int* fuse) {
+// cache lines: "<sms> <ip> <jp> <kp> <precision> <by> <tasks> <depth> <fuse> <vec>
+// <ms per iteration> v2" (lines without the v2 tag, from before the vector
+// width was tuned, are ignored)
+bool tune_lookup(int sms, const Dims& d, int prec, int* by, int* tasks, int* depth, int* fuse,
+                 int* vec) {
     std::ifstream f(tune_cache_path());
     std::string line;
     bool found = false;
     while (std::getline(f, line)) {
         std::istringstream is(line);
-        int a[9];
+        int a[10];
         double ms;
-        if (!(is >> a[0] >> a[1] >> a[2] >> a[3] >> a[4] >> a[5] >> a[6] >> a[7] >> a[8] >> ms))
+        std::string tag;
+        if (!(is >> a[0] >> a[1] >> a[2] >> a[3] >> a[4] >> a[5] >> a[6] >> a[7] >> a[8] >> a[9] >>
+              ms >> tag) ||
+            tag != "v2")
             continue;
         if (a[0] == sms && a[1] == d.ip && a[2] == d.jp && a[3] == d.kp && a[4] == prec) {
             *by = a[5];
             *tasks = a[6];
             *depth = a[7];
             *fuse = a[8];
+            *vec = a[9];
             found = true;  // the last entry wins
         }
     }
     return found;
 }
 
-void tune_store(int sms, const Dims& d, int prec, int by, int tasks, int depth, int fuse,
+void tune_store(int sms, const Dims& d, int prec, int by, int tasks, int depth, int fuse, int vec,
                 double ms) {
     std::ofstream f(tune_cache_path(), std::ios::app);
     if (f) f << sms << ' ' << d.ip << ' ' << d.jp << ' ' << d.kp << ' ' << prec << ' ' << by << ' '
-             << tasks << ' ' << depth << ' ' << fuse << ' ' << ms << '\n';
+             << tasks << ' ' << depth << ' ' << fuse << ' ' << vec << ' ' << ms << " v2\n";
 }
 
 template <typename T>
@@ -1567,7 +1576,7 @@ __global__ void k_tune_rhs(Dims d, T* b, T* x) {
 // device time of `iters` iterations of the solver in precision T with the
 // given launch shape (graph-driven, tolerance unreachable, itmax = iters)
 template <typename T>
-double tune_time(dcm_handle* h, int by, int tasks, int depth, int fuse, int iters) {
+double tune_time(dcm_handle* h, int by, int tasks, int depth, int fuse, int vec, int iters) {
     SolverWork<T> w;
     T *x, *b;
     if constexpr (std::is_same<T, double>::value) {
@@ -1586,6 +1595,7 @@ double tune_time(dcm_handle* h, int by, int tasks, int depth, int fuse, int iter
     w.tasks = tasks;
     w.ni = depth;
     w.fuse = fuse;
+    w.vw = std::is_same<T, float>::value ? vec : 0;
     const Metrics<T>& mt = metrics_of<T>(h);
     double best = 1e30;
     for (int rep = 0; rep < 3; rep++) {
@@ -1607,18 +1617,18 @@ double tune_time(dcm_handle* h, int by, int tasks, int depth, int fuse, int iter
 }  // namespace
 
 extern "C" int dcm_tune(dcm_handle* h, int precision, int use_cache, int* by, int* tasks,
-                        int* depth, int* fuse) {
+                        int* depth, int* fuse, int* vec) {
     CHECK_H();
     if (precision != 0 && precision != 1) return fail(h, DCM_E_ARG, "tune: precision");
     int sms = 0;
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
-    int b0 = 8, t0 = 0, n0 = 4, f0 = 0;
-    if (!(use_cache && tune_lookup(sms, h->d, precision, &b0, &t0, &n0, &f0))) {
+    int b0 = 8, t0 = 0, n0 = 4, f0 = 0, v0 = precision == 1 ? 4 : 2;
+    if (!(use_cache && tune_lookup(sms, h->d, precision, &b0, &t0, &n0, &f0, &v0))) {
         static const int BYS[3] = {2, 4, 8}, TASKS[3] = {0, 1, 2}, DEPTHS[4] = {1, 2, 4, 8};
         double best = 1e30;
-        auto consider = [&](int bv, int tv, int nv, int fv) -> bool {
-            const double ms = precision == 0 ? tune_time<double>(h, bv, tv, nv, 0, 12)
-                                             : tune_time<float>(h, bv, tv, nv, fv, 12);
+        auto consider = [&](int bv, int tv, int nv, int fv, int vv) -> bool {
+            const double ms = precision == 0 ? tune_time<double>(h, bv, tv, nv, 0, 0, 12)
+                                             : tune_time<float>(h, bv, tv, nv, fv, vv, 12);
             if (ms < 0) return false;
             if (ms < best) {
                 best = ms;
@@ -1626,45 +1636,57 @@ extern "C" int dcm_tune(dcm_handle* h, int precision, int use_cache, int* by, in
                 t0 = tv;
                 n0 = nv;
                 f0 = fv;
+                v0 = vv;
             }
             return true;
         };
-        for (int bi = 0; bi < 3; bi++)
-            for (int ti = 0; ti < 3; ti++)
-                for (int ni = 0; ni < 4; ni++)
-                    if (!consider(BYS[bi], TASKS[ti], DEPTHS[ni], 0))
-                        return fail(h, DCM_E_CUDA, "tune: a candidate launch shape failed");
-        // the fused preconditioner (FP32), without (1) and with (2) phase C's
-        // matvec as its fourth stage: the sweep shape does not apply
+        // FP32: 16-byte (4 levels per lane) and 8-byte (2 levels) vectors of
+        // the separate kernels; FP64 keeps 16-byte vectors (2 levels)
+        const int nvec = precision == 1 ? 2 : 1;
+        for (int vi = 0; vi < nvec; vi++) {
+            const int vv = precision == 1 ? (vi == 0 ? 4 : 2) : 2;
+            for (int bi = 0; bi < 3; bi++)
+                for (int ti = 0; ti < 3; ti++)
+                    for (int ni = 0; ni < 4; ni++)
+                        if (!consider(BYS[bi], TASKS[ti], DEPTHS[ni], 0, vv))
+                            return fail(h, DCM_E_CUDA, "tune: a candidate launch shape failed");
+        }
+        // the fused preconditioner (FP32, 16-byte vectors), without (1) and
+        // with (2) phase C's matvec as its fourth stage: the sweep shape does
+        // not apply
         if (precision == 1)
             for (int fv = 1; fv <= 2; fv++)
                 for (int ti = 0; ti < 3; ti++)
-                    if (!consider(8, TASKS[ti], 4, fv))
+                    if (!consider(8, TASKS[ti], 4, fv, 4))
                         return fail(h, DCM_E_CUDA, "tune: a candidate launch shape failed");
-        tune_store(sms, h->d, precision, b0, t0, n0, f0, best);
+        tune_store(sms, h->d, precision, b0, t0, n0, f0, v0, best);
     }
     h->tune_by[precision] = b0;
     h->tune_tasks[precision] = t0;
     h->tune_ni[precision] = n0;
     h->tune_fuse[precision] = precision == 1 ? f0 : 0;
+    h->tune_vec[precision] = precision == 1 ? v0 : 2;
     h->generation += 1;
     if (by) *by = b0;
     if (tasks) *tasks = t0;
     if (depth) *depth = n0;
     if (fuse) *fuse = h->tune_fuse[precision];
+    if (vec) *vec = h->tune_vec[precision];
     return DCM_OK;
 }
 
 extern "C" int dcm_set_launch_shape(dcm_handle* h, int precision, int by, int tasks, int depth,
-                                    int fuse) {
+                                    int fuse, int vec) {
     CHECK_H();
     if ((precision != 0 && precision != 1) || by < 1 || by > 8 || tasks < 0 || tasks > 15 ||
-        depth < 1 || depth > 63 || fuse < 0 || fuse > 2)
+        depth < 1 || depth > 63 || fuse < 0 || fuse > 2 ||
+        (precision == 1 ? (vec != 2 && vec != 4) : vec != 2) || (fuse && vec != 4))
         return fail(h, DCM_E_ARG, "set_launch_shape: bad argument");
     h->tune_by[precision] = by;
     h->tune_tasks[precision] = tasks;
     h->tune_ni[precision] = depth;
     h->tune_fuse[precision] = precision == 1 ? fuse : 0;
+    h->tune_vec[precision] = vec;
     h->generation += 1;
     return DCM_OK;
 }

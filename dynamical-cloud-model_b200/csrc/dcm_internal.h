@@ -90,6 +90,10 @@ struct SolverWork {
     int ni = 4;
     // FP32: fuse the three Jacobi sweeps of a phase (columns of <= 128 levels)
     int fuse = 1;
+    // FP32: levels per lane of the separate stencil and update kernels (4:
+    // 16-byte vectors; 2: 8-byte vectors, for short columns that would leave
+    // lanes of a 128-level warp task idle); 0 = 4
+    int vw = 0;
     // FP32 iterations of the mixed form: Chebyshev-weighted Jacobi sweeps on
     // the interval [cheb_lo, 2] of the spectrum of D^-1 A (0: the reference's
     // unweighted sweeps)

@@ -80,6 +80,7 @@ struct SolverArgs {
     int ni;           // i-planes a stencil warp task marches over
     int fuse;         // FP32: the three sweeps of a phase as one kernel (k_precond3)
     int fuse_mv = 0;  // with fuse: phase C's matvec as the fused kernel's fourth stage
+    int vw = 0;       // FP32 levels per lane of the separate kernels (2 or 4; 0 = 4)
     // Chebyshev-weighted sweeps (mixed form only): x1 = cw[0] s0, then
     // x_m+1 = x_m + cw[m] (s0 - (A x_m)/a_p), m = 1..3, in place of the
     // reference's x1 = s0, x_m+1 = x_m + s0 - (A x_m)/a_p
@@ -225,35 +226,49 @@ struct KVec<double> {
     using type = double2;
 };
 
-template <typename T>
-__device__ __forceinline__ void vld(const T* p, T (&v)[KVec<T>::V]) {
-    using VT = typename KVec<T>::type;
-    const VT a = __ldg(reinterpret_cast<const VT*>(p));
-    if constexpr (KVec<T>::V == 4) {
+// the vector type of N consecutive k-levels (16 or 8 bytes)
+template <typename T, int N>
+struct VecT;
+template <>
+struct VecT<float, 4> {
+    using type = float4;
+};
+template <>
+struct VecT<float, 2> {
+    using type = float2;
+};
+template <>
+struct VecT<double, 2> {
+    using type = double2;
+};
+
+template <typename VT, typename T, int N>
+__device__ __forceinline__ void vunpack(const VT& a, T (&v)[N]) {
+    if constexpr (N == 4) {
         v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
     } else {
         v[0] = a.x; v[1] = a.y;
     }
+}
+
+template <typename T, int N>
+__device__ __forceinline__ void vld(const T* p, T (&v)[N]) {
+    using VT = typename VecT<T, N>::type;
+    vunpack(__ldg(reinterpret_cast<const VT*>(p)), v);
 }
 // coherent load, for an array the kernel also writes
-template <typename T>
-__device__ __forceinline__ void vld_rw(const T* p, T (&v)[KVec<T>::V]) {
-    using VT = typename KVec<T>::type;
-    const VT a = *reinterpret_cast<const VT*>(p);
-    if constexpr (KVec<T>::V == 4) {
-        v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
-    } else {
-        v[0] = a.x; v[1] = a.y;
-    }
+template <typename T, int N>
+__device__ __forceinline__ void vld_rw(const T* p, T (&v)[N]) {
+    using VT = typename VecT<T, N>::type;
+    vunpack(*reinterpret_cast<const VT*>(p), v);
 }
 // store the levels k0 + c <= kp (a whole vector when all are)
-template <typename T>
-__device__ __forceinline__ void vst(T* p, const T (&v)[KVec<T>::V], int nvalid) {
-    using VT = typename KVec<T>::type;
-    constexpr int V = KVec<T>::V;
-    if (nvalid >= V) {
+template <typename T, int N>
+__device__ __forceinline__ void vst(T* p, const T (&v)[N], int nvalid) {
+    using VT = typename VecT<T, N>::type;
+    if (nvalid >= N) {
         VT a;
-        if constexpr (V == 4) {
+        if constexpr (N == 4) {
             a.x = v[0]; a.y = v[1]; a.z = v[2]; a.w = v[3];
         } else {
             a.x = v[0]; a.y = v[1];
@@ -261,17 +276,15 @@ __device__ __forceinline__ void vst(T* p, const T (&v)[KVec<T>::V], int nvalid) 
         *reinterpret_cast<VT*>(p) = a;
     } else {
 #pragma unroll
-        for (int c = 0; c < V; c++)
+        for (int c = 0; c < N; c++)
             if (c < nvalid) p[c] = v[c];
     }
 }
 
 // X values of a vector: the operand field, or for the first sweep s0 = q/a_p
 // formed from rh and vh
-template <typename T, int OP, int MODE>
-__device__ __forceinline__ void xload(const StenCtx<T, OP, MODE>& C, int o,
-                                      T (&x)[KVec<T>::V]) {
-    constexpr int V = KVec<T>::V;
+template <typename T, int OP, int MODE, int V>
+__device__ __forceinline__ void xload(const StenCtx<T, OP, MODE>& C, int o, T (&x)[V]) {
     if (OP == OP_SW1) {
         T a[V], b[V];
         vld(C.rh + o, a);
@@ -302,11 +315,11 @@ __device__ __forceinline__ T xload1(const StenCtx<T, OP, MODE>& C, int o) {
 // neighbours (periodic) are vector loads of the adjacent columns; the i
 // neighbours are the previous and the next plane of the march, kept in
 // registers, so each plane loads its i + 1 column and its two j neighbours.
-template <typename T, int OP, int MODE, int NV, bool MARCH>
+template <typename T, int OP, int MODE, int NV, bool MARCH, int V>
 __device__ __forceinline__ void sten_task(const StenCtx<T, OP, MODE>& C, int kc, int j, int i0,
                                           int ni, double (&acc)[NV]) {
     if (!MARCH) ni = 1;
-    constexpr int V = KVec<T>::V;
+    // V: levels per lane (16-byte vectors by default; 8-byte in FP32 for short columns)
     const Dims& d = C.d;
     const int lane = threadIdx.x & 31;
     const int ip = d.ip, jp = d.jp, kp = d.kp;
@@ -506,7 +519,7 @@ __device__ __forceinline__ void reduce_tail(const SolverArgs& a, double (&acc)[N
 // Sweeps (no reduction): one warp task per warp, grid (k-chunks, j/8, i).
 // Reducing kernels: persistent blocks, each warp strides over the warp tasks
 // and the block publishes one partial.
-template <typename T, int OP, int MODE>
+template <typename T, int OP, int MODE, int V = KVec<T>::V>
 __global__ void __launch_bounds__(256) k_sten(SolverArgs a, Coef<T> c, SolverBufs B, Red2 R,
                                               SolverScalars* S) {
     constexpr int NV = (OP == OP_SETUP || OP == OP_MATC) ? 2 : 1;
@@ -542,9 +555,8 @@ __global__ void __launch_bounds__(256) k_sten(SolverArgs a, Coef<T> c, SolverBuf
     if constexpr (!RED) {
         const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
         if (j <= d.jp)
-            sten_task<T, OP, MODE, NV, MARCH>(C, blockIdx.x, j, 1 + blockIdx.z * ni, ni, acc);
+            sten_task<T, OP, MODE, NV, MARCH, V>(C, blockIdx.x, j, 1 + blockIdx.z * ni, ni, acc);
     } else {
-        constexpr int V = KVec<T>::V;
         const int lane = threadIdx.x & 31;
         for (TaskIter t(blockIdx.x * blockDim.y + threadIdx.y, gridDim.x * blockDim.y, a.nkt,
                         d.jp);
@@ -564,7 +576,7 @@ __global__ void __launch_bounds__(256) k_sten(SolverArgs a, Coef<T> c, SolverBuf
                     prefetch_l2((const T*)B.v1 + o);
                 }
             }
-            sten_task<T, OP, MODE, NV, false>(C, t.kt, 1 + t.jr, t.i, 1, acc);
+            sten_task<T, OP, MODE, NV, false, V>(C, t.kt, 1 + t.jr, t.i, 1, acc);
         }
         reduce_tail<OP, NV>(a, acc, R, smem, S);
     }
@@ -818,6 +830,12 @@ __global__ void __launch_bounds__(precond3_warps<MODE, MV>() * 32, 1)
         }
         // stage 4 (MV): t = A cs at plane b-1 of the output rows, (t,t), (t,s)
         if (MV && outrow && b >= i0) {
+            // r and v1 of the next step's plane into L2 ahead of their use
+            if (live && b + 1 <= bend) {
+                const int on = col + KJ * wrapn(b, ip);
+                prefetch_l2(rr + on);
+                prefetch_l2(rv1 + on);
+            }
             const float4 c4 = slot(3, prv, w);  // own cs at plane b-1
             const float xc[4] = {c4.x, c4.y, c4.z, c4.w};
             if (b >= i0 + 1) {
@@ -901,7 +919,7 @@ __device__ __forceinline__ unsigned loop_cond(cudaGraphConditionalHandle h, Solv
 }
 
 // --- D: x, r updates, (r,r), (r,cr) -> err, next rho and bet -----------------
-template <typename T>
+template <typename T, int V = KVec<T>::V>
 __global__ void __launch_bounds__(256) k_bicg_update(SolverArgs a, Coef<T> c,
                                                      T* __restrict__ x,
                                                      const T* __restrict__ p,
@@ -924,7 +942,6 @@ __global__ void __launch_bounds__(256) k_bicg_update(SolverArgs a, Coef<T> c,
     const Dims& d = a.d;
     const T alf = (T)S->alf, omg = (T)S->omg;
     double acc[2] = {0.0, 0.0};
-    constexpr int V = KVec<T>::V;
     const int lane = threadIdx.x;
     for (TaskIter tk(blockIdx.x * blockDim.y + threadIdx.y, gridDim.x * blockDim.y, a.nkt, d.jp);
          tk.i <= d.ip; tk.next()) {
@@ -1076,9 +1093,13 @@ static int persistent_grid(K kernel) {
 
 // Warp tasks: (k-chunk of 32 V levels, j, i).
 template <typename T>
-static int kchunks(const Dims& d) {
-    return (d.kp + KVec<T>::V * BX - 1) / (KVec<T>::V * BX);
+static int kchunks(const Dims& d, int vw = 0) {
+    const int V = vw > 0 ? vw : KVec<T>::V;
+    return (d.kp + V * BX - 1) / (V * BX);
 }
+
+// levels per lane of the FP32 iteration kernels: a.vw (2 or 4), 4 by default
+static inline bool narrow(const SolverArgs& a) { return a.vw == 2; }
 
 // a kernel launch, with programmatic stream serialisation when `pdl`
 template <typename... P, typename... A>
@@ -1111,29 +1132,41 @@ static int red_grid(const SolverArgs& a, int full, int nkt, int ni = 1) {
     return (int)std::max(1LL, want);
 }
 
-template <typename T, int OP, int MODE>
-static void sten(const SolverArgs& a, const Coef<T>& c, const SolverBufs& B, SolverWork<T>& w,
-                 cudaStream_t st, int cat) {
-    ProfScope ps(cat, st);
+template <typename T, int OP, int MODE, int V>
+static void sten_v(const SolverArgs& a, const Coef<T>& c, const SolverBufs& B, SolverWork<T>& w,
+                   cudaStream_t st) {
     constexpr bool RED = OP == OP_SETUP || OP == OP_MATC || OP == OP_MATP;
     if (RED) {
-        static const int full = persistent_grid(k_sten<T, OP, MODE>);
-        launch(a.pdl, k_sten<T, OP, MODE>, dim3(red_grid(a, full, a.nkt, 1)), dim3(BX, BY), 0,
+        static const int full = persistent_grid(k_sten<T, OP, MODE, V>);
+        launch(a.pdl, k_sten<T, OP, MODE, V>, dim3(red_grid(a, full, a.nkt, 1)), dim3(BX, BY), 0,
                st, a, c, B, w.red, w.S);
     } else {
         // at most 256 threads: the kernels are compiled with __launch_bounds__(256)
         const int by = a.by >= 1 && a.by <= 256 / BX ? a.by : BY;
         const int ni = OP == OP_SW1 ? a.ni : 1;
         const dim3 grid(a.nkt, (a.d.jp + by - 1) / by, (a.d.ip + ni - 1) / ni);
-        launch(a.pdl, k_sten<T, OP, MODE>, grid, dim3(BX, by), 0, st, a, c, B, w.red, w.S);
+        launch(a.pdl, k_sten<T, OP, MODE, V>, grid, dim3(BX, by), 0, st, a, c, B, w.red, w.S);
     }
+}
+
+template <typename T, int OP, int MODE>
+static void sten(const SolverArgs& a, const Coef<T>& c, const SolverBufs& B, SolverWork<T>& w,
+                 cudaStream_t st, int cat) {
+    ProfScope ps(cat, st);
+    if constexpr (std::is_same<T, float>::value) {
+        if (narrow(a)) {
+            sten_v<T, OP, MODE, 2>(a, c, B, w, st);
+            return;
+        }
+    }
+    sten_v<T, OP, MODE, KVec<T>::V>(a, c, B, w, st);
 }
 
 
 // the fused preconditioner applies (FP32, one k-chunk per column)
 template <typename T>
 static bool fused_ok(const SolverArgs& a) {
-    return std::is_same<T, float>::value && a.fuse && a.nkt == 1;
+    return std::is_same<T, float>::value && a.fuse && !narrow(a) && a.nkt == 1;
 }
 
 // one fused preconditioner launch: PJ-row strips x i-chunks, at most one
@@ -1252,10 +1285,20 @@ static void launch_iteration(const SolverArgs& a, const Coef<T>& c, SolverWork<T
     // phase D
     {
         ProfScope ps(P_UPDATE, st);
-        static const int full = persistent_grid(k_bicg_update<T>);
-        launch(a.pdl, k_bicg_update<T>, dim3(red_grid(a, full, a.nkt)), dim3(BX, BY), 0, st, a,
-               c, x, (const T*)w.p, (const T*)w.sA, w.r, (const T*)w.v1, (const T*)w.t,
-               (const T*)w.cr, w.rh, w.red, w.S);
+        auto go = [&](auto kern) {
+            static const int full = persistent_grid(kern);
+            launch(a.pdl, kern, dim3(red_grid(a, full, a.nkt)), dim3(BX, BY), 0, st, a, c, x,
+                   (const T*)w.p, (const T*)w.sA, w.r, (const T*)w.v1, (const T*)w.t,
+                   (const T*)w.cr, w.rh, w.red, w.S);
+        };
+        if constexpr (std::is_same<T, float>::value) {
+            if (narrow(a))
+                go(k_bicg_update<T, 2>);
+            else
+                go(k_bicg_update<T>);
+        } else {
+            go(k_bicg_update<T>);
+        }
     }
 }
 
@@ -1416,7 +1459,8 @@ int solver_run(SolverWork<T>& w, const Dims& d, T* x, const T* b, const T* sw, c
     a.itmax = itmax;
     a.tol = tol;
     a.sc_floor = sc_floor;
-    a.nkt = kchunks<T>(d);
+    a.vw = std::is_same<T, float>::value ? w.vw : 0;
+    a.nkt = kchunks<T>(d, a.vw);
     a.max_updates = 0;
     a.max_cycle = 0;
     a.by = w.by;
@@ -1469,9 +1513,9 @@ int solver_run(SolverWork<T>& w, const Dims& d, T* x, const T* b, const T* sw, c
         SolveGraph& G = *w.graph;
         const void* kp[6] = {x, b, sw, dzn, w.r, w.S};
         const double kd[3] = {tol, sc_floor, a.tiny};
-        // launch shape: by < 16, tasks < 16, ni < 64, fuse < 4, pdl < 2
-        const int shape =
-            a.by + 16 * a.tasks + 256 * a.ni + 16384 * a.fuse + 65536 * (w.pdl ? 1 : 0);
+        // launch shape: by < 16, tasks < 16, ni < 64, fuse < 4, pdl < 2, vw < 8
+        const int shape = a.by + 16 * a.tasks + 256 * a.ni + 16384 * a.fuse +
+                          65536 * (w.pdl ? 1 : 0) + 131072 * a.vw;
         const int ki[6] = {itmax, wo, (post ? 1 : 0) + 2 * max_rounds, (int)sizeof(T) + 16 * shape,
                            d.ip * 4096 + d.jp, d.kp};
         if (!G.matches(kp, kd, ki)) {
@@ -1770,7 +1814,8 @@ int refine_run(SolverWork<float>& wf, SolverWork<double>& wd, const Dims& d, dou
     a.fuse = 0;
     no_cheb(a);
     SolverArgs af = a;             // vector warp tasks of the FP32 iterations
-    af.nkt = kchunks<float>(d);
+    af.vw = wf.vw;
+    af.nkt = kchunks<float>(d, af.vw);
     af.ni = wf.ni >= 1 ? wf.ni : 1;
     af.fuse = wf.fuse;
     af.fuse_mv = wf.fuse == 2 ? 1 : 0;
@@ -1857,7 +1902,7 @@ int refine_run(SolverWork<float>& wf, SolverWork<double>& wd, const Dims& d, dou
         const void* kp[6] = {x, b, sw, dzn, dx, wf.S};
         const double kd[3] = {tol, delta, af.cheb ? wf.cheb_lo : 0.0};
         const int shape = af.by + 16 * af.tasks + 256 * af.ni + 16384 * af.fuse +
-                          65536 * af.cheb + 131072 * (wf.pdl ? 1 : 0);
+                          65536 * af.cheb + 131072 * (wf.pdl ? 1 : 0) + 262144 * af.vw;
         const int ki[6] = {itmax, max_updates, 1 + 2 * max_rounds, 16 * shape,
                            d.ip * 4096 + d.jp, d.kp};
         if (!G.matches(kp, kd, ki)) {

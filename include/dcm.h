@@ -377,7 +377,11 @@ int dcm_solver_graph_info(dcm_handle *h, int *programmatic);
  * application run fused in one kernel (fuse 1: columns of at most 128
  * levels), and whether that kernel of phase C also forms t = A cs with its
  * dots (t,t), (t,s) as a fourth stage (fuse 2; otherwise the matvec is a
- * kernel of its own).
+ * kernel of its own), and in FP32 the vector width of the separate stencil
+ * and update kernels (vec: 4 levels per lane, 16-byte vectors, so that a
+ * warp task covers 128 levels; or 2 levels per lane, 8-byte vectors and 64
+ * levels per warp task, which keeps more lanes busy on short columns; the
+ * fused kernel always uses 4; FP64 uses 2, 16-byte vectors).
  * It times 12 BiCGSTAB iterations of each candidate on a synthetic
  * right-hand side and applies the fastest to the handle for that precision
  * (each precision keeps its own launch shape).  With use_cache the result is
@@ -387,12 +391,14 @@ int dcm_solver_graph_info(dcm_handle *h, int *programmatic);
  * it before dcm_state_upload or between steps, not concurrently with other
  * calls on the handle. */
 int dcm_tune(dcm_handle *h, int precision, int use_cache, int *by, int *tasks,
-             int *depth, int *fuse);
+             int *depth, int *fuse, int *vec);
 /* Sets the launch shape of one precision explicitly (same meaning and ranges
- * as dcm_tune's results; by <= 8, depth <= 63, fuse 0..2 only for
- * precision 1).  Default: by 8, tasks 0, depth 4, fuse 1 (FP32) / 0 (FP64). */
+ * as dcm_tune's results; by <= 8, depth <= 63, fuse 0..2 and vec 2 or 4 only
+ * for precision 1, a fused preconditioner only with vec 4; vec 2 for
+ * precision 0).  Default: by 8, tasks 0, depth 4, fuse 1, vec 4 (FP32) /
+ * fuse 0, vec 2 (FP64). */
 int dcm_set_launch_shape(dcm_handle *h, int precision, int by, int tasks,
-                         int depth, int fuse);
+                         int depth, int fuse, int vec);
 
 /* ---- batched ensemble (no counterpart in the reference) ------------------ */
 /* Independent domains of possibly different sizes on one device.  Each

@@ -82,11 +82,13 @@ def test_tune_and_cache(dcm, tmp_path, monkeypatch):
     monkeypatch.setenv("DCM_TUNE_CACHE", str(tmp_path / "tune.txt"))
     c = small_bubble()
     core = dcm.DynamicalCore(c.grid)
-    by, tasks, depth, fuse = core.tune(precision=1, use_cache=True)
-    assert by in (2, 4, 8) and tasks in (0, 1, 2) and depth in (1, 2, 4, 8) and fuse in (0, 1)
+    by, tasks, depth, fuse, vec = core.tune(precision=1, use_cache=True)
+    assert by in (2, 4, 8) and tasks in (0, 1, 2) and depth in (1, 2, 4, 8)
+    assert fuse in (0, 1, 2) and vec in (2, 4) and not (fuse and vec != 4)
     lines = (tmp_path / "tune.txt").read_text().splitlines()
     assert len(lines) == 1
-    assert core.tune(precision=1, use_cache=True) == (by, tasks, depth, fuse)  # from the cache
+    # from the cache
+    assert core.tune(precision=1, use_cache=True) == (by, tasks, depth, fuse, vec)
     assert len((tmp_path / "tune.txt").read_text().splitlines()) == 1
     # the tuned shape changes only the order of the dot-product sums
     _upload(core, c, 0)

@@ -171,3 +171,26 @@ def test_mixed_solve_timeout_status(dcm):
         assert st.err_last < c.ptol and st.iters_last > 5
     finally:
         core.close()
+
+
+@pytest.mark.parametrize("shape", [(24, 20, 16), (9, 30, 37), (40, 1, 12), (12, 10, 70)])
+def test_narrow_vectors_match_wide(dcm, shape):
+    """The FP32 iteration kernels with 2 levels per lane (8-byte vectors,
+    64-level warp tasks) against 4 levels per lane: the same operator, sweeps
+    and dots, only the dot products' partition differs, so iterations and
+    fields agree to FP32 round-off; columns of one, two and three warp tasks."""
+    ip, jp, kp = shape
+    c = cases.warm_bubble(ip=ip, jp=jp, kp=kp, dxyz=50.0, radius=200.0, zc=200.0, seed=44)
+    out = []
+    for vec in (2, 4):
+        core = dcm.DynamicalCore(c.grid)
+        core.set_launch_shape(1, fuse=0, vec=vec)
+        core.upload_state(c.state, c.dt, ptol=c.ptol, kord=c.kord, precision=1, precond=1)
+        core.driver_start()
+        its = [core.step(1).iters_last for _ in range(3)]
+        out.append((its, core.download_state()))
+        core.close()
+    (ia, fa), (ib, fb) = out
+    assert max(abs(a - b) for a, b in zip(ia, ib)) <= 4, (ia, ib)
+    for n in ("u", "v", "w", "th"):
+        assert relerr(fa[n], fb[n]) <= 1e-6, n
