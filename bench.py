@@ -142,6 +142,11 @@ STEP_PASSES = 60.0
 FUSED_JACOBI_PASSES = 3.5
 FUSED_REPLACED_PASSES = 11.5
 FUSED_ITER_PASSES = 25.0
+# With phase C's matvec as the fused kernel's fourth stage (launch shape
+# fuse = 2) phase C's launch also reads r, v1 and writes t (6 passes moved;
+# it replaces 11 + 4 = 15 algorithmic passes): per launch 5 moved and 13.5
+# replaced on average, 24 passes per iteration.
+FUSED_MV = {"jacobi": 5.0, "replaced": 13.5, "iter": 24.0}
 
 
 def make_case(pkg, name):
@@ -340,14 +345,18 @@ def run_b200(args, rank, world, local_rank, dist):
     classes = m32["classes"]
     dom = max(classes, key=lambda k: classes[k][0])
     dom_ms, dom_n = classes[dom]
-    fused = bool(m32["shape"]["fused_preconditioner"])
-    dom_passes = FUSED_JACOBI_PASSES if (fused and dom == "jacobi") else PASSES.get(dom, 0.0)
+    fuse_level = int(m32["shape"]["fused_preconditioner"])
+    fused = fuse_level > 0
+    f_jac, f_rep, f_iter = ((FUSED_MV["jacobi"], FUSED_MV["replaced"], FUSED_MV["iter"])
+                            if fuse_level == 2 else
+                            (FUSED_JACOBI_PASSES, FUSED_REPLACED_PASSES, FUSED_ITER_PASSES))
+    dom_passes = f_jac if (fused and dom == "jacobi") else PASSES.get(dom, 0.0)
     dom_bytes = dom_passes * N * w32
     dom_s = dom_ms / dom_n / 1e3 if dom_n else None
     # algorithmic bytes of one launch by the operator-fused model: a fused
     # preconditioner launch applies the three sweeps of a phase (11.5 passes
     # averaged over phases B and C)
-    dom_bytes_alg = (FUSED_REPLACED_PASSES * N * w32 if (fused and dom == "jacobi")
+    dom_bytes_alg = (f_rep * N * w32 if (fused and dom == "jacobi")
                      else dom_bytes)
     achieved_alg = dom_bytes_alg / dom_s / 1e9 if dom_n else None
     traffic = None
@@ -355,7 +364,8 @@ def run_b200(args, rank, world, local_rank, dist):
     if os.path.exists(tp):
         with open(tp) as f:
             tr = json.load(f).get(case.name, {}).get("fp32", {})
-        traffic = tr.get("jacobi_fused" if (fused and dom == "jacobi") else dom)
+        if not (dom == "jacobi" and fuse_level == 2):  # not captured for the fourth stage
+            traffic = tr.get("jacobi_fused" if (fused and dom == "jacobi") else dom)
 
     def step_model(m, w, iter_passes):
         it = m["iters"] / args.steps
@@ -422,7 +432,7 @@ def run_b200(args, rank, world, local_rank, dist):
     core.close()
     if rank != 0:
         return None
-    sm32 = step_model(m32, w32, FUSED_ITER_PASSES if fused else ITER_PASSES)
+    sm32 = step_model(m32, w32, f_iter if fused else ITER_PASSES)
     sm64 = step_model(m64, 8.0, ITER_PASSES)
     acc_last = acc.get(str(args.accuracy_steps), {})
     details = {
@@ -448,7 +458,7 @@ def run_b200(args, rank, world, local_rank, dist):
         "preconditioner": "FP32 iterations: Chebyshev-weighted Jacobi sweeps (3 sweeps, "
                           "interval [0.05, 2]); FP64: the reference's 3 Jacobi sweeps",
     }
-    min_bytes = FUSED_JACOBI_PASSES * N * w32 if (fused and dom == "jacobi") else dom_bytes
+    min_bytes = f_jac * N * w32 if (fused and dom == "jacobi") else dom_bytes
     return {
         "metric": metric_of(case), "value": m32["value"], "unit": "grid-pt-steps/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
