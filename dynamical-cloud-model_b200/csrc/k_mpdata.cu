@@ -484,25 +484,30 @@ __global__ void __launch_bounds__(256) k_limit(Dims d, Vel<T> Vt, const T* __res
 
 // ---- one antidiffusive iteration in one kernel --------------------------------
 // Antidiffusive velocities, the linked FCT limiter (beta, eq 18) and the
-// donor-cell pass of field 0 (:319-695), fused along i-planes.  A block owns
-// the output rows j0..j0+JT-1 of an i-chunk [i0, i1] and keeps R = JT + H + 1
-// warps, one per row j0-H .. j0+JT (H = 2 with the limiter, 1 without; halo
-// rows take the periodic image of their j).  A warp covers whole columns
-// (k = 1 + lane + 32c, c < NC), so every k neighbour is in the block and the
-// boundary planes k = 0, kp+1 hold the exchanges' value 0.  The stages march
-// over the planes skewed by one plane:
+// donor-cell pass of field 0 (:319-695), fused along i-planes over tiles of
+// rows and k-levels.  A block owns the output rows j0..j0+JT-1 of an i-chunk
+// [i0, i1] and of a k-tile of MPK_OUT levels kb..kb+MPK_OUT-1; it keeps
+// R = JT + H + 1 warps, one per row j0-H .. j0+JT (H = 2 with the limiter,
+// 1 without; halo rows take the periodic image of their j), and lane l of a
+// warp holds level kb - 2 + l, so a warp covers its tile with a halo of two
+// levels below and two above.  Levels outside 1..kp hold the exchanges'
+// boundary value 0 of every stage.  The stages march over the planes skewed
+// by one plane each:
 //   step f:  A (antidiffusive velocities) at plane f     (rows 0..R-1)
-//            beta at plane f                              (rows 1..R-1)
-//            L (limited velocities) at plane f-1          (rows 1..R-2)
-//            donor cell of field 0 at plane f-1           (owned rows)
-// with a barrier between stages.  j and k neighbours of a stage's inputs
-// come from shared planes (the v and w components of A, the two betas of
-// planes f-1 and f, the v and w components of L); i neighbours and a
-// point's own values stay in registers.  Only the limited velocities
-// (exchange_full images, the next iteration's input) and the new field 0
-// reach memory; A and beta never do.  Without the limiter the donor cell
-// runs on A at plane f and A is the output set.  Each quantity is the same
-// point function as the separate kernels evaluate.
+//            beta at plane f-1                            (rows 1..R-1)
+//            L (limited velocities) at plane f-2          (rows 1..R-2)
+//            donor cell of field 0 at plane f-3           (owned rows)
+// with one barrier per step: every value a stage takes from another warp
+// was written in the previous step, so the four stages of a step are
+// independent chains a warp can overlap.  k neighbours of a stage's inputs
+// are the neighbour lanes (shuffles), j neighbours the neighbour warps'
+// values in small shared planes (the v component of A, the betas, the v
+// component of L; two plane parities each), i neighbours and a point's own
+// values registers.
+// Only the limited velocities (exchange_full images, the next iteration's
+// input) and the new field 0 reach memory; A and beta never do.  Without the
+// limiter the donor cell runs on A at plane f and A is the output set.  Each
+// quantity is the same point function as the separate kernels evaluate.
 template <typename T>
 struct MpIterArgs {
     Dims d;
@@ -518,13 +523,16 @@ struct MpIterArgs {
     T dt_add;
     const MpScalars* M;     // field 0's shift and boundary values
     const MpScalars* gate;  // early return of the whole call
-    int JT, ni, P;          // owned rows, planes per chunk, k pitch of a shared plane
+    int JT, ni;             // owned rows, planes per chunk
 };
 
-// threads per block of the fused iteration: 24 warps (FP32, <= 85 registers)
-// or 12 (FP64, <= 170 registers)
+constexpr int MPK_OUT = 28;  // output levels of a k-tile (32 lanes, a halo of 2 each side)
+
+// rows (warps) per block of the fused iteration: 24 (FP32, <= 85 registers a
+// thread, the occupancy of the separate antidiffusive-velocity kernel) or 8
+// (FP64)
 template <typename T>
-constexpr int mp_iter_max_rows() { return sizeof(T) == 4 ? 24 : 12; }
+constexpr int mp_iter_max_rows() { return sizeof(T) == 4 ? 24 : 8; }
 
 template <typename T, bool MONO, bool LAST>
 __global__ void __launch_bounds__(32 * mp_iter_max_rows<T>()) k_mpdata_iter(MpIterArgs<T> a) {
@@ -533,117 +541,109 @@ __global__ void __launch_bounds__(32 * mp_iter_max_rows<T>()) k_mpdata_iter(MpIt
     if (a.gate->early) return;
     const Dims& d = a.d;
     const int lane = threadIdx.x & 31, r = threadIdx.x >> 5, R = blockDim.x >> 5;
-    const int P = a.P, PL = R * P, kp = d.kp;
+    const int kp = d.kp;
     constexpr int H = MONO ? 2 : 1;
     const int j0 = 1 + blockIdx.x * a.JT;
     const int jr = wrapj(j0 - H + r, d.jp);
     const int i0 = 1 + blockIdx.y * a.ni, i1 = min(i0 + a.ni - 1, d.ip);
-    const bool owned = r >= H && r <= R - 2 && j0 - H + r <= d.jp;
+    const int k = 1 + MPK_OUT * (int)blockIdx.z - 2 + lane;
+    const bool inK = k >= 1 && k <= kp;
+    const bool rowown = r >= H && r <= R - 2 && j0 - H + r <= d.jp;
+    const bool own = rowown && inK && lane >= 2 && lane < 2 + MPK_OUT;
     const T m = (T)a.M->m;
-    // shared planes [row][k], k = 0..kp+1, by plane parity f & 1:
-    //   A[2][u, v, w] (0..5); MONO also B[2][up, dn] (6..9), Lu[2] (10, 11),
-    //   Lv (12), Lw (13)
-    constexpr int NPL = MONO ? 14 : 6;
-    auto A_ = [&](int par, int comp) { return sm + (par * 3 + comp) * PL; };
-    auto B_ = [&](int par, int comp) { return sm + (6 + par * 2 + comp) * PL; };
-    auto Lu_ = [&](int par) { return sm + (10 + par) * PL; };
-    T* const sLv = sm + 12 * PL;
-    T* const sLw = sm + 13 * PL;
-    for (int q = threadIdx.x; q < NPL * R; q += blockDim.x) {
-        sm[q * P] = T(0);
-        sm[q * P + kp + 1] = T(0);
-    }
+    const T z = T(0);
+    constexpr unsigned FULL = 0xffffffffu;
+    // shared planes [parity][row][lane]: A_v (0, 1), beta_up (2, 3), beta_dn
+    // (4, 5), L_v (6, 7); a plane's values are read one step after they are
+    // written, so one barrier per step orders them
+    auto sp = [&](int plane, int par, int row) -> T& {
+        return sm[((plane * 2 + par) * R + row) * 32 + lane];
+    };
     auto Pf = [&](int kk, int jj, int ii) -> T { return a.pso[d.at(kk, jj, ii)]; };
-    const int fstart = i0 - (MONO ? 2 : 1), fend = MONO ? i1 + 1 : i1;
-    for (int f = fstart; f <= fend; f++) {
-        const int fi = wrapj(f, d.ip);
-        const int par = f & 1, pp = par ^ 1;
-        // ---- A at plane f (every row)
-        {
-            T* const Au = A_(par, 0);
-            T* const Av = A_(par, 1);
-            T* const Aw = A_(par, 2);
-            for (int k = 1 + lane; k <= kp; k += 32) {
-                T us, vs, ws;
-                antidiff_point(d, a.mt, a.dt, a.Vt, a.pso, k, jr, fi, us, vs, ws);
-                Au[r * P + k] = us;
-                Av[r * P + k] = vs;
-                Aw[r * P + k] = ws;
+    // own-point windows along i
+    T A1u = z, A1v = z, A1w = z;  // A at plane f-1
+    T A2u = z, A2v = z, A2w = z;  // A at plane f-2
+    T B2u = z, B2d = z;           // beta at plane f-2
+    T L3u = z, L3v = z, L3w = z;  // L at plane f-3
+    T L4u = z;                    // L_u at plane f-4
+    if (MONO) {
+        // step f: A at f, beta at f-1, L at f-2, donor cell at f-3
+        for (int f = i0 - 2; f <= i1 + 3; f++) {
+            const int p0 = f & 1, p1 = p0 ^ 1;  // parities of planes f (and f-2), f-1 (and f-3)
+            // ---- A at plane f (every row; lane 31 is never read)
+            T Au = z, Av = z, Aw = z;
+            if (f <= i1 + 1 && inK && lane < 31)
+                antidiff_point(d, a.mt, a.dt, a.Vt, a.pso, k, jr, wrapj(f, d.ip), Au, Av, Aw);
+            sp(0, p0, r) = Av;
+            // ---- beta at plane f-1 (lanes 1..30)
+            T Bu = z, Bd = z;
+            const T A1wm = __shfl_up_sync(FULL, A1w, 1);  // A_w at k-1, plane f-1
+            if (f >= i0 && f <= i1 + 2 && r >= 1 && inK && lane >= 1 && lane <= 30)
+                beta0_point(d, a.mt, a.dt, m, a.psi_in, a.pso, k, jr, wrapj(f - 1, d.ip), A2u,
+                            A1u, sp(0, p1, r - 1), A1v, A1wm, A1w, Bu, Bd);
+            sp(1, p1, r) = Bu;
+            sp(2, p1, r) = Bd;
+            // ---- L at plane f-2 (lanes 1..29)
+            const T b2un = __shfl_down_sync(FULL, B2u, 1), b2dn = __shfl_down_sync(FULL, B2d, 1);
+            T Lu = z, Lv = z, Lw = z;
+            if (f >= i0 + 1 && f <= i1 + 2 && r >= 1 && r <= R - 2 && inK && lane >= 1 &&
+                lane <= 29) {
+                Lu = limit_comp(A2u, B2u, B2d, Bu, Bd);
+                Lv = limit_comp(A2v, B2u, B2d, sp(1, p0, r + 1), sp(2, p0, r + 1));
+                Lw = limit_comp(A2w, B2u, B2d, b2un, b2dn);
+                if (own && f - 2 >= i0) {  // exchange_full(..., 0, 0), :669-674
+                    const int fm = wrapj(f - 2, d.ip);
+                    put_full(a.vout.u, d, k, jr, fm, Lu, z, z);
+                    put_full(a.vout.v, d, k, jr, fm, Lv, z, z);
+                    put_full(a.vout.w, d, k, jr, fm, Lw, z, z);
+                }
             }
+            sp(3, p0, r) = Lv;
+            // ---- donor cell of field 0 at plane f-3 (lanes 2..29, owned rows)
+            const T L3wm = __shfl_up_sync(FULL, L3w, 1);
+            if (f >= i0 + 3 && own) {
+                const int f3 = wrapj(f - 3, d.ip);
+                const T nv = donor_point(d, a.mt, a.dt, a.neumann, k, jr, f3, L3u, L4u, L3v,
+                                         sp(3, p1, r - 1), L3w, L3wm, Pf);
+                donor_store<T, LAST>(a.dst, d, k, jr, f3, nv, 1, a.sadd, a.dt_add, a.M, m);
+            }
+            __syncthreads();
+            A2u = A1u; A2v = A1v; A2w = A1w;
+            A1u = Au; A1v = Av; A1w = Aw;
+            B2u = Bu; B2d = Bd;
+            L4u = L3u;
+            L3u = Lu; L3v = Lv; L3w = Lw;
         }
-        __syncthreads();
-        if (MONO) {
-            // ---- beta at plane f
-            if (f >= i0 - 1 && r >= 1) {
-                const T *Au = A_(par, 0), *Av = A_(par, 1), *Aw = A_(par, 2), *Aup = A_(pp, 0);
-                T* const Bu = B_(par, 0);
-                T* const Bd = B_(par, 1);
-                for (int k = 1 + lane; k <= kp; k += 32) {
-                    const int o = r * P + k;
-                    T bu, bd;
-                    beta0_point(d, a.mt, a.dt, m, a.psi_in, a.pso, k, jr, fi, Aup[o], Au[o],
-                                Av[o - P], Av[o], Aw[o - 1], Aw[o], bu, bd);
-                    Bu[o] = bu;
-                    Bd[o] = bd;
-                }
+    } else {
+        // step f: A at f, donor cell on A at f-1
+        for (int f = i0 - 1; f <= i1 + 1; f++) {
+            const int p0 = f & 1, p1 = p0 ^ 1;
+            T Au = z, Av = z, Aw = z;
+            if (f <= i1 && inK && lane < 31)
+                antidiff_point(d, a.mt, a.dt, a.Vt, a.pso, k, jr, wrapj(f, d.ip), Au, Av, Aw);
+            sp(0, p0, r) = Av;
+            const T A1wm = __shfl_up_sync(FULL, A1w, 1);
+            if (f >= i0 + 1 && own) {
+                const int f1 = wrapj(f - 1, d.ip);
+                const T nv = donor_point(d, a.mt, a.dt, a.neumann, k, jr, f1, A1u, A2u, A1v,
+                                         sp(0, p1, r - 1), A1w, A1wm, Pf);
+                put_full(a.vout.u, d, k, jr, f1, A1u, z, z);  // :528-533
+                put_full(a.vout.v, d, k, jr, f1, A1v, z, z);
+                put_full(a.vout.w, d, k, jr, f1, A1w, z, z);
+                donor_store<T, LAST>(a.dst, d, k, jr, f1, nv, 1, a.sadd, a.dt_add, a.M, m);
             }
             __syncthreads();
-            // ---- L at plane f-1
-            const int fm = wrapj(f - 1, d.ip);
-            if (f >= i0 && r >= 1 && r <= R - 2) {
-                const T *Au = A_(pp, 0), *Av = A_(pp, 1), *Aw = A_(pp, 2);
-                const T *Bpu = B_(pp, 0), *Bpd = B_(pp, 1), *Bu = B_(par, 0), *Bd = B_(par, 1);
-                T* const Lu = Lu_(pp);
-                for (int k = 1 + lane; k <= kp; k += 32) {
-                    const int o = r * P + k;
-                    const T up = Bpu[o], dn = Bpd[o];
-                    const T lu = limit_comp(Au[o], up, dn, Bu[o], Bd[o]);
-                    const T lv = limit_comp(Av[o], up, dn, Bpu[o + P], Bpd[o + P]);
-                    const T lw = limit_comp(Aw[o], up, dn, Bpu[o + 1], Bpd[o + 1]);
-                    Lu[o] = lu;
-                    sLv[o] = lv;
-                    sLw[o] = lw;
-                    if (owned && f - 1 >= i0) {  // exchange_full(..., 0, 0), :669-674
-                        put_full(a.vout.u, d, k, jr, fm, lu, T(0), T(0));
-                        put_full(a.vout.v, d, k, jr, fm, lv, T(0), T(0));
-                        put_full(a.vout.w, d, k, jr, fm, lw, T(0), T(0));
-                    }
-                }
-            }
-            __syncthreads();
-            // ---- donor cell of field 0 at plane f-1
-            if (f >= i0 + 1 && owned) {
-                const T *Lu = Lu_(pp), *Lum = Lu_(par);  // L_u at planes f-1, f-2
-                for (int k = 1 + lane; k <= kp; k += 32) {
-                    const int o = r * P + k;
-                    const T nv = donor_point(d, a.mt, a.dt, a.neumann, k, jr, fm, Lu[o], Lum[o],
-                                             sLv[o], sLv[o - P], sLw[o], sLw[o - 1], Pf);
-                    donor_store<T, LAST>(a.dst, d, k, jr, fm, nv, 1, a.sadd, a.dt_add, a.M, m);
-                }
-            }
-        } else {
-            // ---- donor cell of field 0 at plane f on A
-            if (f >= i0 && owned) {
-                const T *Au = A_(par, 0), *Av = A_(par, 1), *Aw = A_(par, 2), *Aup = A_(pp, 0);
-                for (int k = 1 + lane; k <= kp; k += 32) {
-                    const int o = r * P + k;
-                    const T nv = donor_point(d, a.mt, a.dt, a.neumann, k, jr, fi, Au[o], Aup[o],
-                                             Av[o], Av[o - P], Aw[o], Aw[o - 1], Pf);
-                    put_full(a.vout.u, d, k, jr, fi, Au[o], T(0), T(0));  // :528-533
-                    put_full(a.vout.v, d, k, jr, fi, Av[o], T(0), T(0));
-                    put_full(a.vout.w, d, k, jr, fi, Aw[o], T(0), T(0));
-                    donor_store<T, LAST>(a.dst, d, k, jr, fi, nv, 1, a.sadd, a.dt_add, a.M, m);
-                }
-            }
+            A2u = A1u;
+            A1u = Au; A1v = Av; A1w = Aw;
         }
     }
 }
 
-// Launch shape of the fused iteration: rows per block from the shared-memory
-// budget and the row cap; i-chunks so that the grid fills every SM with as
+// Launch shape of the fused iteration: R rows per block (the row cap), k-tiles
+// of MPK_OUT levels, and i-chunks so that the grid fills every SM with as
 // many blocks as fit on it at once, with chunks of at least 4 planes.
 struct MpIterShape {
-    int R = 0, JT = 0, ni = 0, P = 0, nstrips = 0, nchunks = 0;
+    int R = 0, JT = 0, ni = 0, nstrips = 0, nchunks = 0, ntiles = 0;
     size_t smem = 0;
 };
 
@@ -653,18 +653,15 @@ __global__ void k_mpdata_iter(MpIterArgs<T> a);
 template <typename T>
 static MpIterShape mp_iter_shape(const Dims& d, bool mono, int max_rows) {
     MpIterShape s;
-    const int H = mono ? 2 : 1, npl = mono ? 14 : 6;
-    s.P = d.kp + 2;
-    const size_t row_bytes = (size_t)npl * s.P * sizeof(T);
-    const size_t budget = 200 * 1024;
-    int R = (int)std::min<size_t>(mp_iter_max_rows<T>(), budget / row_bytes);
-    R = std::min(R, max_rows);
+    const int H = mono ? 2 : 1;
+    int R = std::min(mp_iter_max_rows<T>(), max_rows);
     R = std::min(R, d.jp + H + 1);  // no more rows than the domain has
     if (R < H + 2) return s;        // not even one owned row
     s.R = R;
     s.JT = R - H - 1;
-    s.smem = row_bytes * R;
+    s.smem = (size_t)8 * R * 32 * sizeof(T);
     s.nstrips = (d.jp + s.JT - 1) / s.JT;
+    s.ntiles = (d.kp + MPK_OUT - 1) / MPK_OUT;
     int sms = 148;
     {
         int dev = 0;
@@ -679,8 +676,9 @@ static MpIterShape mp_iter_shape(const Dims& d, bool mono, int max_rows) {
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mpdata_iter<T, false, false>,
                                                       32 * R, s.smem);
     per_sm = std::max(per_sm, 1);
-    const int want = (sms * per_sm + s.nstrips - 1) / s.nstrips;
-    const int nch = std::max(1, std::min((d.ip + 3) / 4, want));
+    const long long plane_blocks = (long long)s.nstrips * s.ntiles;
+    const long long want = ((long long)sms * per_sm + plane_blocks - 1) / plane_blocks;
+    const int nch = (int)std::max(1LL, std::min((long long)(d.ip + 3) / 4, want));
     s.ni = (d.ip + nch - 1) / nch;
     s.nchunks = (d.ip + s.ni - 1) / s.ni;
     return s;
@@ -688,7 +686,7 @@ static MpIterShape mp_iter_shape(const Dims& d, bool mono, int max_rows) {
 
 template <typename T, bool MONO, bool LAST>
 static bool launch_mp_iter(const MpIterArgs<T>& args, const MpIterShape& s, cudaStream_t st) {
-    const dim3 grid(s.nstrips, s.nchunks), block(32 * s.R);
+    const dim3 grid(s.nstrips, s.nchunks, s.ntiles), block(32 * s.R);
     k_mpdata_iter<T, MONO, LAST><<<grid, block, s.smem, st>>>(args);
     return true;
 }
@@ -697,8 +695,10 @@ static bool launch_mp_iter(const MpIterArgs<T>& args, const MpIterShape& s, cuda
 // once at handle creation, outside any stream capture)
 template <typename T, bool MONO, bool LAST>
 static void mp_iter_attrs() {
-    cudaFuncSetAttribute(k_mpdata_iter<T, MONO, LAST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         210 * 1024);
+    // the shared planes are small (6 x rows x 32 values); prefer L1 for the
+    // stencil reads of the antidiffusive velocities
+    cudaFuncSetAttribute(k_mpdata_iter<T, MONO, LAST>,
+                         cudaFuncAttributePreferredSharedMemoryCarveout, 10);
 }
 
 void mpdata_init() {
@@ -806,7 +806,7 @@ int mpdata_run(MpdataWork<T>& w, const Dims& d, const Metrics<T>& mt, T dt,
             ia.pso = cur[0]; ia.vout = O; ia.dst = last ? psi_out[0] : nxt[0];
             ia.neumann = neumann; ia.sadd = (last && sadd) ? sadd[0] : nullptr;
             ia.dt_add = dt_add; ia.M = w.M; ia.gate = gate;
-            ia.JT = fs.JT; ia.ni = fs.ni; ia.P = fs.P;
+            ia.JT = fs.JT; ia.ni = fs.ni;
             bool okl;
             {
                 ProfScope ps_(P_ANTIDIFF, st);
