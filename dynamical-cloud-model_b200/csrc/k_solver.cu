@@ -600,7 +600,7 @@ __global__ void __launch_bounds__(256) k_sten(SolverArgs a, Coef<T> c, SolverBuf
 // arithmetic of the three unfused sweeps.
 constexpr int PJ = 16;        // output rows per block
 constexpr int PW = PJ + 6;    // warps per block
-constexpr int PD = 3;         // planes of r/a_p, v1/a_p (and old p) copied ahead
+constexpr int PD = 2;         // planes of r/a_p, v1/a_p (and old p) copied ahead
 constexpr int PR = 3;         // planes of 1/a_p kept (formed by stage 1, used by 2 and 3)
 
 // 16-byte asynchronous global -> shared copy (cp.async, L2 only) and its
