@@ -237,13 +237,15 @@ class DynamicalCore:
                                       C.byref(vec)))
         return by.value, tasks.value, depth.value, fuse.value, vec.value
 
-    def set_launch_shape(self, precision, by=8, tasks=0, depth=4, fuse=None, vec=None):
+    def set_launch_shape(self, precision, by=8, tasks=0, depth=None, fuse=None, vec=None):
         """Set the solver launch shape of one precision (dcm_set_launch_shape).
         fuse: 0 separate sweeps, 1 fused preconditioner, 2 fused with phase
         C's matvec (FP32); vec: levels per lane of the separate kernels (FP32
         4 or 2, FP64 2)."""
         if fuse is None:
             fuse = 1 if precision == 1 else 0
+        if depth is None:
+            depth = 1 if precision == 1 else 4
         if vec is None:
             vec = 4 if precision == 1 else 2
         self._check(self.lib.dcm_set_launch_shape(self.h, int(precision), int(by), int(tasks),

@@ -101,7 +101,7 @@ struct dcm_handle {
     // launch shape of the solver kernels per precision (dcm_tune; [0] FP64,
     // [1] the FP32 iterations of the mixed form): warps per sweep block, warp
     // tasks per warp of the reducing kernels (0 = fill the GPU), marching depth
-    int tune_by[2] = {8, 8}, tune_tasks[2] = {0, 0}, tune_ni[2] = {4, 4}, tune_fuse[2] = {0, 1};
+    int tune_by[2] = {8, 8}, tune_tasks[2] = {0, 0}, tune_ni[2] = {4, 1}, tune_fuse[2] = {0, 1};
     int tune_vec[2] = {2, 4};  // levels per lane (FP64 fixed at 2)
     // dcm_solver_limits: round budget of graph-driven solves (0: default) and
     // the FP64 breakdown threshold (< 0: the reference's tiny)
@@ -1653,12 +1653,13 @@ extern "C" int dcm_tune(dcm_handle* h, int precision, int use_cache, int* by, in
         }
         // the fused preconditioner (FP32, 16-byte vectors), without (1) and
         // with (2) phase C's matvec as its fourth stage: the sweep shape does
-        // not apply
+        // not apply; the depth is the march of the reducing kernels
         if (precision == 1)
             for (int fv = 1; fv <= 2; fv++)
                 for (int ti = 0; ti < 3; ti++)
-                    if (!consider(8, TASKS[ti], 4, fv, 4))
-                        return fail(h, DCM_E_CUDA, "tune: a candidate launch shape failed");
+                    for (int ni = 0; ni < 4; ni++)
+                        if (!consider(8, TASKS[ti], DEPTHS[ni], fv, 4))
+                            return fail(h, DCM_E_CUDA, "tune: a candidate launch shape failed");
         tune_store(sms, h->d, precision, b0, t0, n0, f0, v0, best);
     }
     h->tune_by[precision] = b0;

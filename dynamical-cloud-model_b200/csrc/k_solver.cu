@@ -519,7 +519,7 @@ __device__ __forceinline__ void reduce_tail(const SolverArgs& a, double (&acc)[N
 // Sweeps (no reduction): one warp task per warp, grid (k-chunks, j/8, i).
 // Reducing kernels: persistent blocks, each warp strides over the warp tasks
 // and the block publishes one partial.
-template <typename T, int OP, int MODE, int V = KVec<T>::V>
+template <typename T, int OP, int MODE, int V = KVec<T>::V, bool RM = false>
 __global__ void __launch_bounds__(256) k_sten(SolverArgs a, Coef<T> c, SolverBufs B, Red2 R,
                                               SolverScalars* S) {
     constexpr int NV = (OP == OP_SETUP || OP == OP_MATC) ? 2 : 1;
@@ -558,16 +558,23 @@ __global__ void __launch_bounds__(256) k_sten(SolverArgs a, Coef<T> c, SolverBuf
             sten_task<T, OP, MODE, NV, MARCH, V>(C, blockIdx.x, j, 1 + blockIdx.z * ni, ni, acc);
     } else {
         const int lane = threadIdx.x & 31;
+        // RM: a warp task is a column chunk over `rn` consecutive i-planes
+        // (the march depth of the launch shape): the march keeps the i-1 and
+        // i columns in registers, so each plane loads its i+1 column and its
+        // two j neighbours (a variant of its own: the march's registers would
+        // cost the unmarched kernel occupancy)
+        const int rn = RM && a.ni > 1 ? a.ni : 1;
+        const int nch = (d.ip + rn - 1) / rn;
         for (TaskIter t(blockIdx.x * blockDim.y + threadIdx.y, gridDim.x * blockDim.y, a.nkt,
                         d.jp);
-             t.i <= d.ip; t.next()) {
+             t.i <= nch; t.next()) {
             // the next task's streamed columns into L2 while this one runs:
             // a warp's tasks are otherwise serialised by their stores
             TaskIter u = t;
             u.next();
-            if (u.i <= d.ip) {
+            if (u.i <= nch) {
                 const int k0 = min(1 + V * (u.kt * BX + lane), d.kp);
-                const int o = d.at(k0, 1 + u.jr, u.i);
+                const int o = d.at(k0, 1 + u.jr, 1 + (u.i - 1) * rn);
                 prefetch_l2(C.gx + o);
                 if (OP == OP_SETUP) prefetch_l2((const T*)B.b + o);
                 if (OP == OP_MATP) prefetch_l2((const T*)B.cr + o);
@@ -576,7 +583,11 @@ __global__ void __launch_bounds__(256) k_sten(SolverArgs a, Coef<T> c, SolverBuf
                     prefetch_l2((const T*)B.v1 + o);
                 }
             }
-            sten_task<T, OP, MODE, NV, false, V>(C, t.kt, 1 + t.jr, t.i, 1, acc);
+            if constexpr (RM)
+                sten_task<T, OP, MODE, NV, true, V>(C, t.kt, 1 + t.jr, 1 + (t.i - 1) * rn, rn,
+                                                    acc);
+            else
+                sten_task<T, OP, MODE, NV, false, V>(C, t.kt, 1 + t.jr, t.i, 1, acc);
         }
         reduce_tail<OP, NV>(a, acc, R, smem, S);
     }
@@ -1137,9 +1148,15 @@ static void sten_v(const SolverArgs& a, const Coef<T>& c, const SolverBufs& B, S
                    cudaStream_t st) {
     constexpr bool RED = OP == OP_SETUP || OP == OP_MATC || OP == OP_MATP;
     if (RED) {
-        static const int full = persistent_grid(k_sten<T, OP, MODE, V>);
-        launch(a.pdl, k_sten<T, OP, MODE, V>, dim3(red_grid(a, full, a.nkt, 1)), dim3(BX, BY), 0,
-               st, a, c, B, w.red, w.S);
+        if (a.ni > 1) {
+            static const int full = persistent_grid(k_sten<T, OP, MODE, V, true>);
+            launch(a.pdl, k_sten<T, OP, MODE, V, true>, dim3(red_grid(a, full, a.nkt, a.ni)),
+                   dim3(BX, BY), 0, st, a, c, B, w.red, w.S);
+        } else {
+            static const int full = persistent_grid(k_sten<T, OP, MODE, V>);
+            launch(a.pdl, k_sten<T, OP, MODE, V>, dim3(red_grid(a, full, a.nkt, 1)),
+                   dim3(BX, BY), 0, st, a, c, B, w.red, w.S);
+        }
     } else {
         // at most 256 threads: the kernels are compiled with __launch_bounds__(256)
         const int by = a.by >= 1 && a.by <= 256 / BX ? a.by : BY;

@@ -372,8 +372,9 @@ int dcm_solver_graph_info(dcm_handle *h, int *programmatic);
  * kernels: warps per block of the Jacobi sweeps (by: 2, 4, 8), warp tasks per
  * warp of the reducing kernels (tasks: 0 = as many blocks as are resident,
  * each warp striding over many tasks; 1, 2 = that many tasks per warp), the
- * depth, the number of i-planes the first Jacobi sweep marches over (1, 2,
- * 4, 8), and in FP32 whether the three sweeps of each preconditioner
+ * depth, the number of i-planes the first Jacobi sweep and the reducing
+ * kernels (the solve's set-up and the two matvecs) march over (1, 2, 4, 8),
+ * and in FP32 whether the three sweeps of each preconditioner
  * application run fused in one kernel (fuse 1: columns of at most 128
  * levels), and whether that kernel of phase C also forms t = A cs with its
  * dots (t,t), (t,s) as a fourth stage (fuse 2; otherwise the matvec is a
@@ -395,8 +396,8 @@ int dcm_tune(dcm_handle *h, int precision, int use_cache, int *by, int *tasks,
 /* Sets the launch shape of one precision explicitly (same meaning and ranges
  * as dcm_tune's results; by <= 8, depth <= 63, fuse 0..2 and vec 2 or 4 only
  * for precision 1, a fused preconditioner only with vec 4; vec 2 for
- * precision 0).  Default: by 8, tasks 0, depth 4, fuse 1, vec 4 (FP32) /
- * fuse 0, vec 2 (FP64). */
+ * precision 0).  Default: by 8, tasks 0, depth 1, fuse 1, vec 4 (FP32) /
+ * depth 4, fuse 0, vec 2 (FP64). */
 int dcm_set_launch_shape(dcm_handle *h, int precision, int by, int tasks,
                          int depth, int fuse, int vec);
 
