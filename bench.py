@@ -266,6 +266,20 @@ def bench_config(case, args):
                    "L2" % mb)}
 
 
+def compact(obj, keep=("value", "ms_per_step")):
+    """Floats to 4 significant digits (except the top-level `keep` keys), so
+    that the JSON line stays short."""
+    def r(o, top=False):
+        if isinstance(o, dict):
+            return {k: (v if top and k in keep else r(v)) for k, v in o.items()}
+        if isinstance(o, list):
+            return [r(v) for v in o]
+        if isinstance(o, float):
+            return float("%.4g" % o)
+        return o
+    return r(obj, True)
+
+
 def write_details(d, name="bench_details.json"):
     """The long-form record (per-class kernel times, accuracy tables, step
     models, notes) beside the compact JSON line; returns its path."""
@@ -432,6 +446,7 @@ def run_b200(args, rank, world, local_rank, dist):
     core.close()
     if rank != 0:
         return None
+    extra = other_configs(args, local_rank) if (world == 1 and not args.no_extra) else None
     sm32 = step_model(m32, w32, f_iter if fused else ITER_PASSES)
     sm64 = step_model(m64, 8.0, ITER_PASSES)
     acc_last = acc.get(str(args.accuracy_steps), {})
@@ -482,8 +497,73 @@ def run_b200(args, rank, world, local_rank, dist):
                      "min_bytes_frac": (min_bytes / dom_s / 1e9 / peak) if dom_n else None},
         "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": m32["launches"],
         "clocks": {k: m32["clocks"].get(k) for k in ("sm_mhz", "sm_max_mhz", "reasons")},
+        "other_configs": extra,
         "details": write_details(details),
     }
+
+
+def other_configs(args, local_rank):
+    """The benchmark's other configurations, one GPU, compactly: the
+    128x1x64 shear layer (FP64, all 600 steps, beside the oracle on the host
+    cores), the 512x512x256 sheared convection with 8 tracers (mixed form,
+    steps 1..10), and the 64-member ensemble (steps 1..10, against the
+    sequential per-member loop)."""
+    pkg = load_pkg()
+    from dcm_b200 import cases
+    out = {}
+    # config 1
+    kh = cases.kelvin_helmholtz()
+    core = pkg.DynamicalCore(kh.grid, device=local_rank)
+    core.tune(precision=0, use_cache=True)
+    kw = dict(ptol=kh.ptol, kord=kh.kord, monotone=kh.monotone)
+    core.upload_state(kh.state, kh.dt, precision=0, **kw)
+    core.driver_start()
+    core.step(3)
+    core.upload_state(kh.state, kh.dt, precision=0, **kw)
+    core.driver_start()
+    st = core.step(kh.nsteps)
+    core.close()
+    n1 = kh.grid.npoints
+    c1 = {"workload": "%s FP64, steps 1..%d" % (kh.name, kh.nsteps),
+          "value": n1 * kh.nsteps / (st.ms_total / 1e3), "ms_per_step": st.ms_total / kh.nsteps,
+          "iters_per_step": st.iters_total / kh.nsteps}
+    if not args.no_cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        oracle.set_threads(os.cpu_count() or 1, True)
+        m = oracle.OracleModel(kh.grid, kh.state, kh.dt, **kw)
+        m.driver_start()
+        t0 = time.perf_counter()
+        m.step(kh.nsteps)
+        c1["oracle_value"] = n1 * kh.nsteps / (time.perf_counter() - t0)
+        c1["oracle_cores"] = os.cpu_count() or 1
+    out["1"] = c1
+    # config 4
+    sc = cases.sheared_convection()
+    core = pkg.DynamicalCore(sc.grid, device=local_rank)
+    core.tune(precision=1, use_cache=True)
+    kw = dict(ptol=sc.ptol, kord=sc.kord, monotone=sc.monotone, nq=sc.nq, c_s=sc.c_s,
+              c_e=sc.c_e, precision=1, precond=1, precond_lo=0.05)
+    core.upload_state(sc.state, sc.dt, **kw)
+    core.driver_start()
+    core.step(2)
+    core.upload_state(sc.state, sc.dt, **kw)
+    core.driver_start()
+    n4 = 10
+    st = core.step(n4)
+    core.close()
+    out["4"] = {"workload": "%s mixed, 8 tracers, steps 1..%d" % (sc.name, n4),
+                "value": sc.grid.npoints * n4 / (st.ms_total / 1e3),
+                "ms_per_step": st.ms_total / n4, "iters_per_step": st.iters_total / n4}
+    # config 5
+    ea = argparse.Namespace(**vars(args))
+    ea.steps, ea.warmup = 10, 3
+    e = run_ensemble(ea, 0, 1, local_rank, None)
+    out["5"] = {"workload": "%d-member ensemble mixed, steps 1..10" % args.members,
+                "value": e["value"], "ms_per_step": e["ms_per_step"],
+                "sequential_value": e["sequential"]["value"],
+                "speedup_vs_sequential": e["speedup_vs_sequential"]}
+    return out
 
 
 def run_ensemble(args, rank, world, local_rank, dist):
@@ -747,6 +827,9 @@ def main():
     ap.add_argument("--ref-budget", type=float, default=1800.0,
                     help="safety bound (s) of the reference arm, which times all K steps")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the other configurations (shear layer, sheared convection, "
+                         "ensemble)")
     ap.add_argument("--accuracy-steps", type=int, default=100)
     ap.add_argument("--members", type=int, default=64)
     ap.add_argument("--host-loop", action="store_true",
@@ -812,7 +895,7 @@ def main():
             dist.barrier()
             dist.destroy_process_group()
     if res is not None:
-        print(json.dumps(res), flush=True)
+        print(json.dumps(compact(res)), flush=True)
 
 
 if __name__ == "__main__":
