@@ -124,6 +124,7 @@ def library():
             "dcm_solver_graph_info": [P, C.POINTER(C.c_int)],
             "dcm_solver_limits": [P, C.c_int, C.c_double],
             "dcm_set_mpdata_shape": [P, C.c_int, C.c_int],
+            "dcm_set_small_solver": [P, C.c_int],
             "dcm_tune": [P, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
                          C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)],
             "dcm_set_launch_shape": [P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int],
@@ -157,7 +158,8 @@ EXPORTS = ("dcm_create", "dcm_destroy", "dcm_status_string", "dcm_last_error",
            "dcm_exchange_along_dim", "dcm_exchange_along_dim_wo", "dcm_state_upload",
            "dcm_driver_start", "dcm_step", "dcm_state_download", "dcm_profile_enable",
            "dcm_profile_read", "dcm_horizontal_means_noalloc", "dcm_solver_graphs",
-           "dcm_solver_graph_info", "dcm_solver_limits", "dcm_set_mpdata_shape", "dcm_tune",
+           "dcm_solver_graph_info", "dcm_solver_limits", "dcm_set_mpdata_shape",
+           "dcm_set_small_solver", "dcm_tune",
            "dcm_set_launch_shape", "dcm_ensemble_create", "dcm_ensemble_destroy", "dcm_ensemble_member",
            "dcm_ensemble_step", "dcm_ensemble_last_error", "dcm_exchange_full_wo",
            "dcm_calculate_subgrid_3d", "dcm_output_open", "dcm_output_write",
@@ -480,6 +482,11 @@ class DynamicalCore:
         (False or 0)."""
         mode = on if isinstance(on, int) and not isinstance(on, bool) else int(bool(on))
         self._check(self.lib.dcm_solver_graphs(self.h, mode))
+
+    def set_small_solver(self, max_points=16384):
+        """FP64 solves of domains with at most max_points interior points in one
+        block (0: never)."""
+        self._check(self.lib.dcm_set_small_solver(self.h, int(max_points)))
 
     def set_mpdata_shape(self, fuse=False, max_rows=32):
         """MPDATA iterations as one kernel per stage (default) or one fused

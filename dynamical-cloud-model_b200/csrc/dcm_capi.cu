@@ -107,6 +107,9 @@ struct dcm_handle {
     // the FP64 breakdown threshold (< 0: the reference's tiny)
     int round_budget = 0;
     double tiny = -1.0;
+    // dcm_set_small_solver: FP64 solves of at most this many interior points
+    // run as one block
+    long long small_max = 16384;
     // dcm_set_mpdata_shape: fused antidiffusive iterations (off by default:
     // slower on B200, see dcm.h), their row cap
     int mp_fuse = 0, mp_rows = 32;
@@ -255,6 +258,7 @@ SolverWork<double> solver_work(dcm_handle* h) {
     w.max_blocks = (int)std::min<size_t>(h->npartials / 3, (size_t)1 << 30);
     w.round_budget = h->round_budget;
     w.tiny = h->tiny;
+    w.small_max = h->small_max;
     return w;
 }
 
@@ -1463,6 +1467,14 @@ extern "C" int dcm_solver_graphs(dcm_handle* h, int on) {
     const int mode = on == 0 ? 0 : on == 2 ? 2 : 1;
     if (mode != h->graphs) h->generation += 1;  // an ensemble recaptures its steps
     h->graphs = mode;
+    return DCM_OK;
+}
+
+extern "C" int dcm_set_small_solver(dcm_handle* h, int max_points) {
+    CHECK_H();
+    if (max_points < 0) return fail(h, DCM_E_ARG, "set_small_solver: max_points");
+    if (max_points != h->small_max) h->generation += 1;
+    h->small_max = max_points;
     return DCM_OK;
 }
 

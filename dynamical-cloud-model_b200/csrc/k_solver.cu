@@ -1467,6 +1467,204 @@ static void no_cheb(SolverArgs& a) {
     for (double& x : a.cw) x = 1.0;
 }
 
+// --- small domains: the whole FP64 solve in one block ------------------------
+// A domain of a few thousand points (the 128 x 1 x 64 shear layer: 8,192)
+// leaves the multi-kernel iteration bound by launch latency: nine kernels of
+// a few microseconds each.  Here one block of SMALL_THREADS threads runs the
+// whole of bicgstab (dynamics.f90:367-435) in the reference's own algebra:
+// setup, and per iteration t = r - bet (omg v1), the three Jacobi sweeps of
+// precondition (:241-270; s = q/a_p, then s + (q - A s)/a_p), p = s + bet p,
+// v1 = A p, s = r - alf v1, cs = M s, t = A cs, the x and r updates, every
+// dot product a fixed-order block sum, every pass separated by a barrier.
+// Vectors stay in global memory (L1- and L2-resident at these sizes).  The
+// scalars and statuses are those of the multi-kernel path (breakdown,
+// non-finite, itmax, round budget), in the same SolverScalars.
+constexpr int SMALL_THREADS = 1024;
+
+// sum over the block, the same value in every thread (a fixed reduction tree)
+__device__ __forceinline__ double small_sum(double v, double* sh) {
+    constexpr unsigned FULL = 0xffffffffu;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    __syncthreads();  // the partials of the previous sum have been read
+    if (lane == 0) sh[w] = v;
+    __syncthreads();
+    double t = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(FULL, t, o);
+    return t;
+}
+
+struct SmallOp {
+    Dims d;
+    Coef<double> c;
+    // the interior point of flat index q (k fastest)
+    __device__ __forceinline__ void at(int q, int& k, int& j, int& i) const {
+        k = 1 + q % d.kp;
+        const int r = q / d.kp;
+        j = 1 + r % d.jp;
+        i = 1 + r / d.jp;
+    }
+    __device__ __forceinline__ double ap(int k, int j, int i) const {
+        return -ld(c.ae + i) - ld(c.aw + i) - ld(c.an + j) - ld(c.as + j) - ld(c.au + k) -
+               ld(c.ad + k);  // set_mat_a, dynamics.f90:93-95
+    }
+    // mat_ax (:219-222, a_c = 0) with the exchange's periodic x, y images and
+    // the Neumann rows x(0) = x(1), x(kp+1) = x(kp) (:206-211)
+    __device__ __forceinline__ double ax(const double* __restrict__ x, int k, int j, int i,
+                                         double ap_) const {
+        const int o = d.at(k, j, i);
+        const double xc = x[o];
+        const double xw = x[d.at(k, j, i == 1 ? d.ip : i - 1)];
+        const double xe = x[d.at(k, j, i == d.ip ? 1 : i + 1)];
+        const double xs = x[d.at(k, j == 1 ? d.jp : j - 1, i)];
+        const double xn = x[d.at(k, j == d.jp ? 1 : j + 1, i)];
+        const double xd = k == 1 ? xc : x[o - 1];
+        const double xu = k == d.kp ? xc : x[o + 1];
+        return ld(c.aw + i) * xw + ld(c.ae + i) * xe + ld(c.as + j) * xs + ld(c.an + j) * xn +
+               ld(c.ad + k) * xd + ld(c.au + k) * xu + ap_ * xc + 0.0;
+    }
+};
+
+__global__ void __launch_bounds__(SMALL_THREADS, 1)
+    k_bicgstab_small(SolverArgs a, SmallOp op, double* __restrict__ x,
+                     const double* __restrict__ b, double* __restrict__ r,
+                     double* __restrict__ cr, double* __restrict__ p, double* __restrict__ v1,
+                     double* __restrict__ tq, double* __restrict__ sa, double* __restrict__ sb,
+                     double* __restrict__ sv, SolverScalars* S, int max_rounds) {
+    __shared__ double sh[32];
+    const Dims& d = a.d;
+    const int n = d.ip * d.jp * d.kp;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    auto pass = [&](auto body) {
+        for (int q = tid; q < n; q += nt) {
+            int k, j, i;
+            op.at(q, k, j, i);
+            body(d.at(k, j, i), k, j, i);
+        }
+        __syncthreads();
+    };
+    // precondition: out = M q (three Jacobi sweeps, sa/sb ping-pong, the
+    // result in sb)
+    auto precondition = [&](const double* __restrict__ qv) {
+        pass([&](int o, int k, int j, int i) { sa[o] = qv[o] / op.ap(k, j, i); });
+        for (int sweep = 0; sweep < 3; sweep++) {
+            const double* __restrict__ src = sweep == 1 ? sb : sa;
+            double* __restrict__ dst = sweep == 1 ? sa : sb;
+            pass([&](int o, int k, int j, int i) {
+                const double apv = op.ap(k, j, i);
+                dst[o] = src[o] + (qv[o] - op.ax(src, k, j, i, apv)) / apv;
+            });
+        }
+    };
+    // ---- set-up (:367-383)
+    double bb = 0.0, rr = 0.0;
+    pass([&](int o, int k, int j, int i) {
+        const double rv = b[o] - op.ax(x, k, j, i, op.ap(k, j, i));
+        r[o] = rv;
+        cr[o] = rv;
+        p[o] = 0.0;
+        v1[o] = 0.0;
+        bb += b[o] * b[o];
+        rr += rv * rv;
+    });
+    bb = small_sum(bb, sh);
+    rr = small_sum(rr, sh);
+    double sc = sqrt(bb);
+    sc = sc > a.sc_floor ? sc : a.sc_floor;  // :370-371
+    double err = sc > 0.0 ? sqrt(rr) / sc : 0.0;
+    int status = 0, it = 0, early = 0;
+    double rho = 0.0, alf = 1.0, omg = 1.0, nrm = 1.0, bet = 0.0, tt = 0.0, ts = 0.0;
+    if (err < a.tol) {
+        early = 1;  // :382-383
+    } else if (!(err == err)) {
+        status = DCM_E_NONFINITE;
+    } else {
+        for (it = 1;; it++) {
+            if (it > max_rounds) {  // the round budget, as the graph-driven loop bounds it
+                status = DCM_E_TIMEOUT;
+                it = it - 1;
+                break;
+            }
+            double rc = 0.0;
+            pass([&](int o, int, int, int) { rc += r[o] * cr[o]; });
+            rho = small_sum(rc, sh);                 // :391
+            bet = (rho / nrm) * (alf / omg);         // :392
+            pass([&](int o, int, int, int) { tq[o] = r[o] - bet * (omg * v1[o]); });  // :393
+            precondition(tq);                        // s, :394-396
+            pass([&](int o, int, int, int) { p[o] = sb[o] + bet * p[o]; });           // :397
+            double cv = 0.0;
+            pass([&](int o, int k, int j, int i) {
+                const double v = op.ax(p, k, j, i, op.ap(k, j, i));  // :399-400
+                v1[o] = v;
+                cv += cr[o] * v;
+            });
+            nrm = small_sum(cv, sh);                 // :401
+            alf = rho / nrm;                         // :403
+            pass([&](int o, int, int, int) { sv[o] = r[o] - alf * v1[o]; });  // :404
+            precondition(sv);                        // cs in sb, :405-407
+            double t2 = 0.0, t3 = 0.0;
+            pass([&](int o, int k, int j, int i) {
+                const double tv = op.ax(sb, k, j, i, op.ap(k, j, i));  // :408-409
+                tq[o] = tv;
+                t2 += tv * tv;
+                t3 += tv * sv[o];
+            });
+            tt = small_sum(t2, sh);                  // :410
+            ts = small_sum(t3, sh);                  // :411
+            omg = ts / tt;                           // :412
+            if (fabs(omg) < a.tiny) {                // :414-417
+                status = DCM_E_BREAKDOWN;
+                break;
+            }
+            double r2 = 0.0;
+            pass([&](int o, int, int, int) {
+                x[o] = x[o] + alf * p[o] + omg * sb[o];  // :419
+                const double rv = sv[o] - omg * tq[o];   // :420
+                r[o] = rv;
+                r2 += rv * rv;
+            });
+            err = sqrt(small_sum(r2, sh)) / sc;      // :423
+            nrm = rho;                               // :425
+            if (err < a.tol) break;                  // :428
+            if (!(err == err)) {
+                status = DCM_E_NONFINITE;
+                break;
+            }
+            if (it >= a.itmax) {
+                status = DCM_E_NOCONV;               // :431-434
+                break;
+            }
+        }
+    }
+    if (tid == 0) {
+        S->sc_err = sc;
+        S->err = err;
+        S->rho = rho;
+        S->alf = alf;
+        S->omg = omg;
+        S->bet = bet;
+        S->nrm = nrm;
+        S->tt = tt;
+        S->ts = ts;
+        S->it = it;
+        S->rounds = it;
+        S->status = status;
+        S->early = early;
+        S->done = 1;
+        S->pause = 0;
+        S->ru = 0;
+    }
+}
+
+// the single-block solve applies (FP64, interior points <= w.small_max)
+template <typename T>
+static bool small_ok(const SolverWork<T>& w, const Dims& d) {
+    return std::is_same<T, double>::value && w.small_max > 0 &&
+           (long long)d.ip * d.jp * d.kp <= w.small_max;
+}
+
 template <typename T>
 int solver_run(SolverWork<T>& w, const Dims& d, T* x, const T* b, const T* sw, const T* dzn,
                double tol, int itmax, int wo, int chunk, cudaStream_t st, SolverScalars* host_S,
@@ -1503,6 +1701,25 @@ int solver_run(SolverWork<T>& w, const Dims& d, T* x, const T* b, const T* sw, c
                                                                               wo);
         }
     };
+    if constexpr (std::is_same<T, double>::value) {
+        if (small_ok(w, d)) {
+            // the whole solve as one block, then the halo fix-up: the same two
+            // launches whether captured into a graph or not
+            SmallOp op{d, c};
+            {
+                ProfScope ps(P_SETUP, st);
+                k_bicgstab_small<<<1, SMALL_THREADS, 0, st>>>(a, op, x, b, w.r, w.cr, w.p, w.v1,
+                                                              w.t, w.sA, w.sB, w.rh, w.S,
+                                                              max_rounds);
+            }
+            post_launch(st);
+            if (w.graph && w.emit) return cudaPeekAtLastError() == cudaSuccess ? DCM_OK : DCM_E_CUDA;
+            cudaMemcpyAsync(host_S, w.S, sizeof(SolverScalars), cudaMemcpyDeviceToHost, st);
+            if (cudaStreamSynchronize(st) != cudaSuccess) return DCM_E_CUDA;
+            if (launched_iters) *launched_iters = host_S->rounds;
+            return host_S->status;
+        }
+    }
     // the whole solve into the graph being captured on `s`: setup, the
     // WHILE loop of iterations, the halo fix-up
     auto emit = [&](cudaStream_t s, SolveGraph& G) {

@@ -333,6 +333,16 @@ int dcm_profile_read(dcm_handle *h, double *ms, long long *launches, int ncat);
  * results; while event timing is enabled the host-driven loop is used. */
 int dcm_solver_graphs(dcm_handle *h, int on);
 
+/* Small domains (no counterpart in the reference): FP64 pressure solves of
+ * domains with at most max_points interior points (default 16384; 0 = never)
+ * run as one kernel of one block, the whole of bicgstab (dynamics.f90:
+ * 367-435) in the reference's algebra with fixed-order block sums, instead of
+ * nine kernels per iteration: on a domain of a few thousand points the
+ * iteration is then bound by the block's passes, not by launch latency.  The
+ * statuses and the iteration counts reported are those of the multi-kernel
+ * solve. */
+int dcm_set_small_solver(dcm_handle *h, int max_points);
+
 /* MPDATA launch shape (no counterpart in the reference).  fuse = 0 (the
  * default): one kernel per stage of an antidiffusive iteration
  * (antidiffusive velocities, betas, limited velocities, donor cell).

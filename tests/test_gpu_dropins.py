@@ -322,3 +322,32 @@ def test_bicgstab_timeout_status(setup, dcm, graphs):
     assert it == 3
     it2, err2 = core.bicgstab(fz(g), b.copy(order="F"), fz(g), 1e-10)
     assert err2 < 1e-10 and it2 > 3
+
+
+def test_small_solver_matches_the_multi_kernel_solve(setup, dcm):
+    """The one-block FP64 solve of small domains against the nine-kernel
+    iteration on the same system: both stop at ||r|| < tol max(||b||, 0.01)
+    (dynamics.f90:370-428), so ||A (x1 - x2)|| <= 2 tol sc_err, and only the
+    dot products' summation order differs (iteration counts within one)."""
+    g, core, ocore = setup
+    rng = np.random.default_rng(31)
+    b = _poisson_rhs(g, rng)
+    x0 = rand_field(g, rng, -0.01, 0.01)
+    sw = rand_field(g, rng)
+    xs, xm = x0.copy(order="F"), x0.copy(order="F")
+    try:
+        core.set_small_solver(16384)
+        its, errs = core.bicgstab(xs, b.copy(order="F"), sw, 1e-10)
+        core.set_small_solver(0)
+        itm, errm = core.bicgstab(xm, b.copy(order="F"), sw, 1e-10)
+    finally:
+        core.set_small_solver()
+    assert errs < 1e-10 and errm < 1e-10
+    assert abs(its - itm) <= 1, (its, itm)
+    d = xs - xm
+    ad = fz(g)
+    ocore.mat_ax(np.asfortranarray(d), ad)
+    sc = max(np.sqrt(np.sum(b[1:-1, 1:-1, 1:-1] ** 2)), 0.01)
+    assert np.sqrt(np.sum(ad[1:-1, 1:-1, 1:-1] ** 2)) <= 2e-10 * sc
+    m = live_mask_p(g)
+    assert relerr(xs, xm, m) <= 1e-9

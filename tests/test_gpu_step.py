@@ -165,3 +165,23 @@ def test_reupload_with_the_same_layout(dcm, precision):
     core.driver_start()
     assert core.step(2).err_last < c2.ptol
     core.close()
+
+
+def test_small_solver_in_the_resident_step(dcm, orc):
+    """The 2-D shear layer's resident FP64 step with the one-block solve (the
+    default at this size) and with the multi-kernel solve: the same fields to
+    the solve's tolerance, iteration counts within one per step."""
+    c = cases.kelvin_helmholtz(ip=64, jp=1, kp=32)
+    out = []
+    for small in (16384, 0):
+        core = dcm.DynamicalCore(c.grid)
+        core.set_small_solver(small)
+        core.upload_state(c.state, c.dt, ptol=c.ptol, kord=c.kord, monotone=c.monotone)
+        core.driver_start()
+        its = [core.step(1).iters_last for _ in range(5)]
+        out.append((its, core.download_state()))
+        core.close()
+    (ia, fa), (ib, fb) = out
+    assert max(abs(x - y) for x, y in zip(ia, ib)) <= 1, (ia, ib)
+    for n in ("u", "w", "th"):
+        assert relerr(fa[n], fb[n]) <= 1e-8, n
