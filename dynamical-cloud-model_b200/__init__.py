@@ -483,9 +483,9 @@ class DynamicalCore:
         mode = on if isinstance(on, int) and not isinstance(on, bool) else int(bool(on))
         self._check(self.lib.dcm_solver_graphs(self.h, mode))
 
-    def set_small_solver(self, max_points=16384):
-        """FP64 solves of domains with at most max_points interior points in one
-        block (0: never)."""
+    def set_small_solver(self, max_points=8192):
+        """FP64 solves of domains with at most max_points interior points on
+        one thread-block cluster (0: never)."""
         self._check(self.lib.dcm_set_small_solver(self.h, int(max_points)))
 
     def set_mpdata_shape(self, fuse=False, max_rows=32):

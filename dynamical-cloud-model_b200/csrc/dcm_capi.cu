@@ -108,8 +108,8 @@ struct dcm_handle {
     int round_budget = 0;
     double tiny = -1.0;
     // dcm_set_small_solver: FP64 solves of at most this many interior points
-    // run as one block
-    long long small_max = 16384;
+    // run as one thread-block cluster
+    long long small_max = 8192;
     // dcm_set_mpdata_shape: fused antidiffusive iterations (off by default:
     // slower on B200, see dcm.h), their row cap
     int mp_fuse = 0, mp_rows = 32;

@@ -108,8 +108,8 @@ struct SolverWork {
     // (< 0: the reference's tiny)
     int round_budget = 0;
     double tiny = -1.0;
-    // FP64: domains of at most this many interior points solve in one block
-    // (k_bicgstab_small); 0 = never
+    // FP64: domains of at most this many interior points solve in one
+    // thread-block cluster (k_bicgstab_small); 0 = never
     long long small_max = 0;
 };
 

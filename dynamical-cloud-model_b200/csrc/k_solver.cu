@@ -42,6 +42,8 @@
 #include <mutex>
 #include <type_traits>
 
+#include <cooperative_groups.h>
+
 #include "dcm_internal.h"
 #include "dcm_prof.h"
 
@@ -1467,19 +1469,24 @@ static void no_cheb(SolverArgs& a) {
     for (double& x : a.cw) x = 1.0;
 }
 
-// --- small domains: the whole FP64 solve in one block ------------------------
+// --- small domains: the whole FP64 solve in one cluster ----------------------
 // A domain of a few thousand points (the 128 x 1 x 64 shear layer: 8,192)
 // leaves the multi-kernel iteration bound by launch latency: nine kernels of
-// a few microseconds each.  Here one block of SMALL_THREADS threads runs the
-// whole of bicgstab (dynamics.f90:367-435) in the reference's own algebra:
-// setup, and per iteration t = r - bet (omg v1), the three Jacobi sweeps of
-// precondition (:241-270; s = q/a_p, then s + (q - A s)/a_p), p = s + bet p,
-// v1 = A p, s = r - alf v1, cs = M s, t = A cs, the x and r updates, every
-// dot product a fixed-order block sum, every pass separated by a barrier.
-// Vectors stay in global memory (L1- and L2-resident at these sizes).  The
-// scalars and statuses are those of the multi-kernel path (breakdown,
-// non-finite, itmax, round budget), in the same SolverScalars.
+// a few microseconds each.  Here one thread-block cluster of SMALL_CL blocks
+// of SMALL_THREADS threads (one block per SM) runs the whole of bicgstab
+// (dynamics.f90:367-435) in the reference's own algebra: setup, and per
+// iteration t = r - bet (omg v1), the three Jacobi sweeps of precondition
+// (:241-270; s = q/a_p, then s + (q - A s)/a_p), p = s + bet p, v1 = A p,
+// s = r - alf v1, cs = M s, t = A cs, the x and r updates.  The points are
+// dealt to the cluster's threads in turn; every pass ends with a cluster
+// barrier (release / acquire at cluster scope, so the next pass reads the
+// neighbours other blocks wrote); every dot product is a fixed-order sum:
+// within a block by a shuffle tree, across the cluster by reading the blocks'
+// partials through distributed shared memory in rank order, so every thread
+// gets the same value.  Vectors stay in global memory (L2-resident at these
+// sizes).  The scalars and statuses are those of the multi-kernel path.
 constexpr int SMALL_THREADS = 1024;
+constexpr int SMALL_CL = 8;  // blocks of the cluster (the portable maximum)
 
 // sum over the block, the same value in every thread (a fixed reduction tree)
 __device__ __forceinline__ double small_sum(double v, double* sh) {
@@ -1534,16 +1541,33 @@ __global__ void __launch_bounds__(SMALL_THREADS, 1)
                      double* __restrict__ tq, double* __restrict__ sa, double* __restrict__ sb,
                      double* __restrict__ sv, SolverScalars* S, int max_rounds) {
     __shared__ double sh[32];
+    __shared__ double part[2];  // this block's partial of the current dot (two buffers)
+    namespace cg = cooperative_groups;
+    cg::cluster_group cl = cg::this_cluster();
     const Dims& d = a.d;
     const int n = d.ip * d.jp * d.kp;
+    const int rank = (int)cl.block_rank(), nb = (int)cl.num_blocks();
     const int tid = threadIdx.x, nt = blockDim.x;
+    const int first = rank * nt + tid, stride = nb * nt;
     auto pass = [&](auto body) {
-        for (int q = tid; q < n; q += nt) {
+        for (int q = first; q < n; q += stride) {
             int k, j, i;
             op.at(q, k, j, i);
             body(d.at(k, j, i), k, j, i);
         }
-        __syncthreads();
+        cl.sync();
+    };
+    int pb = 0;  // partial buffer of the next sum
+    // sum over the cluster, the same value in every thread: the block's
+    // shuffle-tree sum, then the blocks' partials in rank order
+    auto csum = [&](double v) {
+        const double bs = small_sum(v, sh);
+        if (tid == 0) part[pb] = bs;
+        cl.sync();
+        double t = 0.0;
+        for (int r2 = 0; r2 < nb; r2++) t += *cl.map_shared_rank(&part[pb], r2);
+        pb ^= 1;  // the next sum writes the other buffer while this one may still be read
+        return t;
     };
     // precondition: out = M q (three Jacobi sweeps, sa/sb ping-pong, the
     // result in sb)
@@ -1569,8 +1593,8 @@ __global__ void __launch_bounds__(SMALL_THREADS, 1)
         bb += b[o] * b[o];
         rr += rv * rv;
     });
-    bb = small_sum(bb, sh);
-    rr = small_sum(rr, sh);
+    bb = csum(bb);
+    rr = csum(rr);
     double sc = sqrt(bb);
     sc = sc > a.sc_floor ? sc : a.sc_floor;  // :370-371
     double err = sc > 0.0 ? sqrt(rr) / sc : 0.0;
@@ -1589,7 +1613,7 @@ __global__ void __launch_bounds__(SMALL_THREADS, 1)
             }
             double rc = 0.0;
             pass([&](int o, int, int, int) { rc += r[o] * cr[o]; });
-            rho = small_sum(rc, sh);                 // :391
+            rho = csum(rc);                 // :391
             bet = (rho / nrm) * (alf / omg);         // :392
             pass([&](int o, int, int, int) { tq[o] = r[o] - bet * (omg * v1[o]); });  // :393
             precondition(tq);                        // s, :394-396
@@ -1600,7 +1624,7 @@ __global__ void __launch_bounds__(SMALL_THREADS, 1)
                 v1[o] = v;
                 cv += cr[o] * v;
             });
-            nrm = small_sum(cv, sh);                 // :401
+            nrm = csum(cv);                 // :401
             alf = rho / nrm;                         // :403
             pass([&](int o, int, int, int) { sv[o] = r[o] - alf * v1[o]; });  // :404
             precondition(sv);                        // cs in sb, :405-407
@@ -1611,8 +1635,8 @@ __global__ void __launch_bounds__(SMALL_THREADS, 1)
                 t2 += tv * tv;
                 t3 += tv * sv[o];
             });
-            tt = small_sum(t2, sh);                  // :410
-            ts = small_sum(t3, sh);                  // :411
+            tt = csum(t2);                  // :410
+            ts = csum(t3);                  // :411
             omg = ts / tt;                           // :412
             if (fabs(omg) < a.tiny) {                // :414-417
                 status = DCM_E_BREAKDOWN;
@@ -1625,7 +1649,7 @@ __global__ void __launch_bounds__(SMALL_THREADS, 1)
                 r[o] = rv;
                 r2 += rv * rv;
             });
-            err = sqrt(small_sum(r2, sh)) / sc;      // :423
+            err = sqrt(csum(r2)) / sc;      // :423
             nrm = rho;                               // :425
             if (err < a.tol) break;                  // :428
             if (!(err == err)) {
@@ -1638,7 +1662,7 @@ __global__ void __launch_bounds__(SMALL_THREADS, 1)
             }
         }
     }
-    if (tid == 0) {
+    if (tid == 0 && rank == 0) {
         S->sc_err = sc;
         S->err = err;
         S->rho = rho;
@@ -1656,9 +1680,10 @@ __global__ void __launch_bounds__(SMALL_THREADS, 1)
         S->pause = 0;
         S->ru = 0;
     }
+    cl.sync();  // no block leaves while another may still read its partials
 }
 
-// the single-block solve applies (FP64, interior points <= w.small_max)
+// the one-cluster solve applies (FP64, interior points <= w.small_max)
 template <typename T>
 static bool small_ok(const SolverWork<T>& w, const Dims& d) {
     return std::is_same<T, double>::value && w.small_max > 0 &&
@@ -1708,9 +1733,19 @@ int solver_run(SolverWork<T>& w, const Dims& d, T* x, const T* b, const T* sw, c
             SmallOp op{d, c};
             {
                 ProfScope ps(P_SETUP, st);
-                k_bicgstab_small<<<1, SMALL_THREADS, 0, st>>>(a, op, x, b, w.r, w.cr, w.p, w.v1,
-                                                              w.t, w.sA, w.sB, w.rh, w.S,
-                                                              max_rounds);
+                cudaLaunchAttribute at[1];
+                at[0].id = cudaLaunchAttributeClusterDimension;
+                at[0].val.clusterDim.x = SMALL_CL;
+                at[0].val.clusterDim.y = 1;
+                at[0].val.clusterDim.z = 1;
+                cudaLaunchConfig_t cfg = {};
+                cfg.gridDim = dim3(SMALL_CL);
+                cfg.blockDim = dim3(SMALL_THREADS);
+                cfg.stream = st;
+                cfg.attrs = at;
+                cfg.numAttrs = 1;
+                cudaLaunchKernelEx(&cfg, k_bicgstab_small, a, op, x, b, w.r, w.cr, w.p, w.v1, w.t,
+                                   w.sA, w.sB, w.rh, w.S, max_rounds);
             }
             post_launch(st);
             if (w.graph && w.emit) return cudaPeekAtLastError() == cudaSuccess ? DCM_OK : DCM_E_CUDA;

@@ -334,11 +334,12 @@ int dcm_profile_read(dcm_handle *h, double *ms, long long *launches, int ncat);
 int dcm_solver_graphs(dcm_handle *h, int on);
 
 /* Small domains (no counterpart in the reference): FP64 pressure solves of
- * domains with at most max_points interior points (default 16384; 0 = never)
- * run as one kernel of one block, the whole of bicgstab (dynamics.f90:
- * 367-435) in the reference's algebra with fixed-order block sums, instead of
- * nine kernels per iteration: on a domain of a few thousand points the
- * iteration is then bound by the block's passes, not by launch latency.  The
+ * domains with at most max_points interior points (default 8192, the
+ * 128 x 1 x 64 shear layer; 0 = never) run as one kernel on one cluster of
+ * eight blocks (one per SM): the whole of bicgstab (dynamics.f90:367-435) in
+ * the reference's algebra, passes separated by cluster barriers, dot products
+ * summed in a fixed order through distributed shared memory, instead of nine
+ * kernels per iteration whose launch latency bounds such a domain.  The
  * statuses and the iteration counts reported are those of the multi-kernel
  * solve. */
 int dcm_set_small_solver(dcm_handle *h, int max_points);

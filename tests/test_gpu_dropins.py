@@ -325,10 +325,10 @@ def test_bicgstab_timeout_status(setup, dcm, graphs):
 
 
 def test_small_solver_matches_the_multi_kernel_solve(setup, dcm):
-    """The one-block FP64 solve of small domains against the nine-kernel
+    """The one-cluster FP64 solve of small domains against the nine-kernel
     iteration on the same system: both stop at ||r|| < tol max(||b||, 0.01)
     (dynamics.f90:370-428), so ||A (x1 - x2)|| <= 2 tol sc_err, and only the
-    dot products' summation order differs (iteration counts within one)."""
+    dot products' summation order differs (iteration counts within three)."""
     g, core, ocore = setup
     rng = np.random.default_rng(31)
     b = _poisson_rhs(g, rng)
@@ -336,14 +336,14 @@ def test_small_solver_matches_the_multi_kernel_solve(setup, dcm):
     sw = rand_field(g, rng)
     xs, xm = x0.copy(order="F"), x0.copy(order="F")
     try:
-        core.set_small_solver(16384)
+        core.set_small_solver(8192)
         its, errs = core.bicgstab(xs, b.copy(order="F"), sw, 1e-10)
         core.set_small_solver(0)
         itm, errm = core.bicgstab(xm, b.copy(order="F"), sw, 1e-10)
     finally:
         core.set_small_solver()
     assert errs < 1e-10 and errm < 1e-10
-    assert abs(its - itm) <= 1, (its, itm)
+    assert abs(its - itm) <= 3, (its, itm)
     d = xs - xm
     ad = fz(g)
     ocore.mat_ax(np.asfortranarray(d), ad)

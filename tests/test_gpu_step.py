@@ -168,12 +168,15 @@ def test_reupload_with_the_same_layout(dcm, precision):
 
 
 def test_small_solver_in_the_resident_step(dcm, orc):
-    """The 2-D shear layer's resident FP64 step with the one-block solve (the
-    default at this size) and with the multi-kernel solve: the same fields to
-    the solve's tolerance, iteration counts within one per step."""
+    """The 2-D shear layer's resident FP64 step with the one-cluster solve
+    (the default at this size) and with the multi-kernel solve: the same
+    fields to the solve's tolerance; the iteration counts part by summation-
+    order round-off (a few per step, as the reference's own counts do under a
+    change of decomposition), so they are held within 5 per step and 5 % in
+    total."""
     c = cases.kelvin_helmholtz(ip=64, jp=1, kp=32)
     out = []
-    for small in (16384, 0):
+    for small in (8192, 0):
         core = dcm.DynamicalCore(c.grid)
         core.set_small_solver(small)
         core.upload_state(c.state, c.dt, ptol=c.ptol, kord=c.kord, monotone=c.monotone)
@@ -182,6 +185,7 @@ def test_small_solver_in_the_resident_step(dcm, orc):
         out.append((its, core.download_state()))
         core.close()
     (ia, fa), (ib, fb) = out
-    assert max(abs(x - y) for x, y in zip(ia, ib)) <= 1, (ia, ib)
+    assert max(abs(x - y) for x, y in zip(ia, ib)) <= 5, (ia, ib)
+    assert abs(sum(ia) - sum(ib)) <= 0.05 * sum(ib), (ia, ib)
     for n in ("u", "w", "th"):
         assert relerr(fa[n], fb[n]) <= 1e-8, n
