@@ -618,14 +618,20 @@ constexpr int PR = 3;         // planes of 1/a_p kept (formed by stage 1, used b
 
 // 16-byte asynchronous global -> shared copy (cp.async, L2 only) and its
 // group bookkeeping: a lane reads back only the slots it filled itself, so
-// waiting on its own groups is enough (no barrier)
+// waiting on its own groups is enough (no barrier).  The memory clobbers keep
+// the compiler from moving a read of a ring slot below the copy that refills
+// it, or above the wait for the copy that fills it.
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
 }
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;"); }
+__device__ __forceinline__ void cp_async_commit() {
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
 template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N)); }
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
 
 __device__ __forceinline__ int wrapn(int q, int n) { return ((q - 1) % n + n) % n + 1; }
 
