@@ -1328,6 +1328,13 @@ static void launch_iteration(const SolverArgs& a, const Coef<T>& c, SolverWork<T
 }
 
 // ---- graph-driven loops ------------------------------------------------------
+// Iterations per body of a WHILE node.  Each iteration's update kernel
+// counts and tests the loop (loop_cond) and the last one's result decides
+// the next body; an iteration that follows the end of the solve (or a pause
+// for a reliable update) in the same body launches kernels that return at
+// once.  Two per body halve the per-body cost of the conditional node.
+constexpr int ITERS_PER_BODY = 2;
+
 // The first condition of an iteration loop, before its WHILE node; the update
 // kernel sets it after every iteration (loop_cond).
 __global__ void k_loop_cond(cudaGraphConditionalHandle h, SolverScalars* S, int max_rounds) {
@@ -1777,7 +1784,7 @@ int solver_run(SolverWork<T>& w, const Dims& d, T* x, const T* b, const T* sw, c
         ai.cond_max = max_rounds;
         ai.pdl = g_pdl_graphs && w.pdl;
         good = good && capture_into(G.side[0], body[0], [&](cudaStream_t s2) {
-                   launch_iteration<T>(ai, c, w, x, s2);
+                   for (int n = 0; n < ITERS_PER_BODY; n++) launch_iteration<T>(ai, c, w, x, s2);
                });
         post_launch(s);
         return good && cudaPeekAtLastError() == cudaSuccess;
@@ -2158,7 +2165,8 @@ int refine_run(SolverWork<float>& wf, SolverWork<double>& wd, const Dims& d, dou
                    ai.cond_max = max_rounds;
                    ai.pdl = g_pdl_graphs && wf.pdl;
                    g2 = g2 && capture_into(G.side[1], in[0], [&](cudaStream_t s2) {
-                            launch_iteration<float>(ai, cf, wf, dx, s2);
+                            for (int n = 0; n < ITERS_PER_BODY; n++)
+                                launch_iteration<float>(ai, cf, wf, dx, s2);
                         });
                    g2 = g2 && capture_cond_handle(s, &hb, 0);
                    if (g2) k_branch_pause<<<1, 1, 0, s>>>(hb, wf.S);
