@@ -21,7 +21,7 @@ go in `accuracy_vs_fp64`.
 The compact JSON line keeps the headline figures (mixed form, FP64 path,
 speed-up, accuracy after --accuracy-steps, roofline, CPU baseline,
 end-to-end); the long-form record (per-class kernel times, step models,
-accuracy tables) goes to gpurun_out/bench_details.json.
+accuracy tables) goes to the file --details names (bench_details.json).
 --run-case prints one line per step of a named case (profiling driver).
 
 N > 1 (torchrun, one process per GPU): the single domain does not shard
@@ -280,13 +280,13 @@ def compact(obj, keep=("value", "ms_per_step")):
     return r(obj, True)
 
 
-def write_details(d, name="bench_details.json"):
+def write_details(d, name):
     """The long-form record (per-class kernel times, accuracy tables, step
-    models, notes) beside the compact JSON line; returns its path."""
-    out = os.path.join(ROOT, "gpurun_out")
+    models, notes) beside the compact JSON line, at `name` (relative to the
+    repository root); returns its path."""
+    path = os.path.join(ROOT, name)
     try:
-        os.makedirs(out, exist_ok=True)
-        path = os.path.join(out, name)
+        os.makedirs(os.path.dirname(path), exist_ok=True)
         with open(path, "w") as f:
             json.dump(d, f, indent=1)
         return os.path.relpath(path, ROOT)
@@ -498,7 +498,7 @@ def run_b200(args, rank, world, local_rank, dist):
         "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": m32["launches"],
         "clocks": {k: m32["clocks"].get(k) for k in ("sm_mhz", "sm_max_mhz", "reasons")},
         "other_configs": extra,
-        "details": write_details(details),
+        "details": write_details(details, args.details),
     }
 
 
@@ -827,6 +827,8 @@ def main():
     ap.add_argument("--ref-budget", type=float, default=1800.0,
                     help="safety bound (s) of the reference arm, which times all K steps")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--details", default="bench_details.json",
+                    help="file (relative to the repository root) for the long-form record")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the other configurations (shear layer, sheared convection, "
                          "ensemble)")

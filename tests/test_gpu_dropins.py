@@ -3,8 +3,8 @@
 Same seeded inputs on both sides; every halo cell is random on input so the
 tests also pin which halo cells each routine reads and writes.  Copies and
 exchanges must be bit-exact; arithmetic routines must agree to 1e-12 relative
-max-norm per output field (the FP64 parity bar of the north star is 1e-10
-after one time step; single routines are held tighter).
+max-norm per output field (the FP64 parity bar is 1e-10 after one time
+step; single routines are held tighter).
 """
 import numpy as np
 import pytest
