@@ -2,8 +2,8 @@
  * dcm_oracle.c -- CPU restatement (FP64) of the reference dynamical-core
  * timestep of UoM-maul1609/dynamical-cloud-model.
  *
- * TEST INFRASTRUCTURE ONLY (the checker and the timed CPU baseline).  The
- * product never links it.  PARITY UNPINNED: the Fortran reference cannot be
+ * TEST INFRASTRUCTURE ONLY (the tests' parity reference and the timed CPU
+ * baseline).  The product never links it.  PARITY UNPINNED: the Fortran reference cannot be
  * compiled in this image and ships no golden vectors; see dcm_oracle.h.
  * Instead, independent numpy restatements of the same Fortran, array
  * statement by array statement (the tests/..._np.py files), agree with this file bit

@@ -4,7 +4,7 @@
  *
  * TEST INFRASTRUCTURE ONLY.  Nothing in the product links this library; only
  * tests/, __graft_entry__.smoke() and bench.py's CPU-baseline / reference arm
- * load it, as the checker or as the timed CPU baseline.
+ * load it, as the parity reference or as the timed CPU baseline.
  *
  * PARITY UNPINNED: the reference is Fortran 90 and no Fortran compiler exists
  * in this image, and the reference ships no tests, fixtures or golden vectors.

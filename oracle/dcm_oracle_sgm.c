@@ -3,7 +3,8 @@
  * model of UoM-maul1609/dynamical-cloud-model (sgm/subgrid_3d.f90:38-493):
  * calculate_subgrid_3d with its richardson and monin_obukhov helpers.
  *
- * TEST INFRASTRUCTURE ONLY (the checker).  The product never links it.
+ * TEST INFRASTRUCTURE ONLY (the tests' parity reference).  The product never
+ * links it.
  * PARITY UNPINNED: the Fortran reference cannot be compiled in this image and
  * ships no golden vectors; the restatement is cross-checked against an
  * independent numpy restatement in the tests instead.

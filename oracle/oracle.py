@@ -1,7 +1,7 @@
 """ctypes binding of the CPU restatement (dcm_oracle.c).
 
 TEST INFRASTRUCTURE ONLY: used by tests/, __graft_entry__.smoke() and the
-CPU-baseline / reference legs of bench.py, as the checker.  PARITY UNPINNED
+CPU-baseline / reference legs of bench.py, as the parity reference.  PARITY UNPINNED
 (no Fortran compiler in this image; the reference ships no golden vectors).
 
 The methods mirror the product binding (dynamical-cloud-model_b200) name for

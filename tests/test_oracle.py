@@ -1,4 +1,4 @@
-"""CPU tests of the oracle (the CPU restatement used as the checker).
+"""CPU tests of the oracle (the CPU restatement the GPU tests compare with).
 
 Parity with the Fortran reference is unpinned (no compiler for it here and no
 golden vectors in it); these tests pin the restatement to independent
