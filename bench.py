@@ -135,6 +135,10 @@ PASSES = {"jacobi": 23.0 / 6.0, "matvec": 4.0, "update": 10.0, "setup": 4.0,
 # field passes of one BiCGSTAB iteration and of the rest of a step
 ITER_PASSES = 41.0
 STEP_PASSES = 60.0
+# the reference's own algebra per iteration (dynamics.f90:391-423, every
+# field pass the statements make, no stored quotients): the algorithmic
+# model both forms' step_frac_algorithm count against
+REF_ITER_PASSES = 39.0
 # With the fused preconditioner (FP32) one "jacobi" launch applies all three
 # sweeps of a phase: it reads r/a_p, v1/a_p (and old p) and writes p or cs,
 # 4 passes in phase B and 3 in phase C; the iteration then moves 7 + 8 + 10 =
@@ -481,9 +485,11 @@ def run_b200(args, rank, world, local_rank, dist):
         "vs_baseline": None, "dtype": "f32+f64",
         "data": "synthetic (seeded %s, numpy PCG64 seed %d)" % (case.name, case.seed),
         "fp64": {"value": m64["value"], "ms_per_step": m64["ms"] / args.steps,
-                 "iters_per_step": m64["iters"] / args.steps, "step_frac": sm64["frac"]},
+                 "iters_per_step": m64["iters"] / args.steps, "step_frac": sm64["frac"],
+                 "step_frac_algorithm": step_model(m64, 8.0, REF_ITER_PASSES)["frac"]},
         "speedup_vs_fp64": m32["value"] / m64["value"],
         "iters_per_step": m32["iters"] / args.steps, "step_frac": sm32["frac"],
+        "step_frac_algorithm": step_model(m32, w32, REF_ITER_PASSES)["frac"],
         "accuracy_vs_fp64_steps": args.accuracy_steps,
         "accuracy_vs_fp64": {n: float("%.3g" % v["max"]) for n, v in acc_last.items()},
         "config": bench_config(case, args),
