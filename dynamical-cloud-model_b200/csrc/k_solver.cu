@@ -1493,7 +1493,12 @@ static void no_cheb(SolverArgs& a) {
 // s = r - alf v1, cs = M s, t = A cs, the x and r updates.  The points are
 // dealt to the cluster's threads in turn; every pass ends with a cluster
 // barrier (release / acquire at cluster scope, so the next pass reads the
-// neighbours other blocks wrote); every dot product is a fixed-order sum:
+// neighbours other blocks wrote).  Pointwise statements share a pass with
+// the statement before or after them (t and s with s/a_p, p with the last
+// sweep, (r,cr) with the r update), sums taken together share one barrier,
+// and a pass that a sum follows leaves its barrier to the sum's: 11 cluster
+// barriers per iteration, each value computed as the separate statements
+// compute it.  Every dot product is a fixed-order sum:
 // within a block by a shuffle tree, across the cluster by reading the blocks'
 // partials through distributed shared memory in rank order, so every thread
 // gets the same value.  Vectors stay in global memory (L2-resident at these
@@ -1514,6 +1519,31 @@ __device__ __forceinline__ double small_sum(double v, double* sh) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(FULL, t, o);
     return t;
+}
+
+// two sums over the block in one tree (each as small_sum forms it)
+__device__ __forceinline__ void small_sum2(double& a, double& b, double* sh) {
+    constexpr unsigned FULL = 0xffffffffu;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_xor_sync(FULL, a, o);
+        b += __shfl_xor_sync(FULL, b, o);
+    }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    __syncthreads();  // the partials of the previous sum have been read
+    if (lane == 0) {
+        sh[w] = a;
+        sh[32 + w] = b;
+    }
+    __syncthreads();
+    const bool in = lane < (int)(blockDim.x >> 5);
+    a = in ? sh[lane] : 0.0;
+    b = in ? sh[32 + lane] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_xor_sync(FULL, a, o);
+        b += __shfl_xor_sync(FULL, b, o);
+    }
 }
 
 struct SmallOp {
@@ -1553,8 +1583,8 @@ __global__ void __launch_bounds__(SMALL_THREADS, 1)
                      double* __restrict__ cr, double* __restrict__ p, double* __restrict__ v1,
                      double* __restrict__ tq, double* __restrict__ sa, double* __restrict__ sb,
                      double* __restrict__ sv, SolverScalars* S, int max_rounds) {
-    __shared__ double sh[32];
-    __shared__ double part[2];  // this block's partial of the current dot (two buffers)
+    __shared__ double sh[64];
+    __shared__ double part[2][2];  // this block's partials of the current sums (two buffers)
     namespace cg = cooperative_groups;
     cg::cluster_group cl = cg::this_cluster();
     const Dims& d = a.d;
@@ -1562,42 +1592,70 @@ __global__ void __launch_bounds__(SMALL_THREADS, 1)
     const int rank = (int)cl.block_rank(), nb = (int)cl.num_blocks();
     const int tid = threadIdx.x, nt = blockDim.x;
     const int first = rank * nt + tid, stride = nb * nt;
-    auto pass = [&](auto body) {
+    // a pass over this thread's points; `pass` ends with the cluster barrier,
+    // `each` leaves it to the cluster sum that follows (its barrier orders
+    // the pass's writes and reads before every later pass)
+    auto each = [&](auto body) {
         for (int q = first; q < n; q += stride) {
             int k, j, i;
             op.at(q, k, j, i);
             body(d.at(k, j, i), k, j, i);
         }
+    };
+    auto pass = [&](auto body) {
+        each(body);
         cl.sync();
     };
-    int pb = 0;  // partial buffer of the next sum
-    // sum over the cluster, the same value in every thread: the block's
-    // shuffle-tree sum, then the blocks' partials in rank order
-    auto csum = [&](double v) {
+    int pb = 0;  // partial buffer of the next sums
+    // two sums over the cluster, the same values in every thread: the
+    // block's shuffle-tree sums, then the blocks' partials in rank order
+    auto csum2 = [&](double& u, double& v) {
+        small_sum2(u, v, sh);
+        if (tid == 0) {
+            part[pb][0] = u;
+            part[pb][1] = v;
+        }
+        cl.sync();
+        double tu = 0.0, tv = 0.0;
+        for (int r2 = 0; r2 < nb; r2++) {
+            const double* pr = cl.map_shared_rank(&part[pb][0], r2);
+            tu += pr[0];
+            tv += pr[1];
+        }
+        pb ^= 1;  // the next sums write the other buffer while this one may still be read
+        u = tu;
+        v = tv;
+    };
+    auto csum1 = [&](double v) {
         const double bs = small_sum(v, sh);
-        if (tid == 0) part[pb] = bs;
+        if (tid == 0) part[pb][0] = bs;
         cl.sync();
         double t = 0.0;
-        for (int r2 = 0; r2 < nb; r2++) t += *cl.map_shared_rank(&part[pb], r2);
-        pb ^= 1;  // the next sum writes the other buffer while this one may still be read
+        for (int r2 = 0; r2 < nb; r2++) t += *cl.map_shared_rank(&part[pb][0], r2);
+        pb ^= 1;
         return t;
     };
-    // precondition: out = M q (three Jacobi sweeps, sa/sb ping-pong, the
-    // result in sb)
-    auto precondition = [&](const double* __restrict__ qv) {
-        pass([&](int o, int k, int j, int i) { sa[o] = qv[o] / op.ap(k, j, i); });
+    // precondition (:241-270) of the q that set_q forms and stores at a
+    // point: s = q/a_p in the same pass, then three Jacobi sweeps (sa/sb
+    // ping-pong, the result in sb); with bp the last sweep also forms
+    // p = s + bet p (:397) at its point
+    // (qv is not restrict-qualified: set_q writes the same array)
+    auto precondition = [&](const double* qv, auto set_q, bool bp, double bet) {
+        pass([&](int o, int k, int j, int i) { sa[o] = set_q(o) / op.ap(k, j, i); });
         for (int sweep = 0; sweep < 3; sweep++) {
             const double* __restrict__ src = sweep == 1 ? sb : sa;
             double* __restrict__ dst = sweep == 1 ? sa : sb;
             pass([&](int o, int k, int j, int i) {
                 const double apv = op.ap(k, j, i);
-                dst[o] = src[o] + (qv[o] - op.ax(src, k, j, i, apv)) / apv;
+                const double sn = src[o] + (qv[o] - op.ax(src, k, j, i, apv)) / apv;
+                dst[o] = sn;
+                if (bp && sweep == 2) p[o] = sn + bet * p[o];
             });
         }
     };
-    // ---- set-up (:367-383)
+    // ---- set-up (:367-383); cr = r, so (r,cr) of the first iteration is (r,r)
     double bb = 0.0, rr = 0.0;
-    pass([&](int o, int k, int j, int i) {
+    each([&](int o, int k, int j, int i) {
         const double rv = b[o] - op.ax(x, k, j, i, op.ap(k, j, i));
         r[o] = rv;
         cr[o] = rv;
@@ -1606,13 +1664,13 @@ __global__ void __launch_bounds__(SMALL_THREADS, 1)
         bb += b[o] * b[o];
         rr += rv * rv;
     });
-    bb = csum(bb);
-    rr = csum(rr);
+    csum2(bb, rr);
     double sc = sqrt(bb);
     sc = sc > a.sc_floor ? sc : a.sc_floor;  // :370-371
     double err = sc > 0.0 ? sqrt(rr) / sc : 0.0;
     int status = 0, it = 0, early = 0;
     double rho = 0.0, alf = 1.0, omg = 1.0, nrm = 1.0, bet = 0.0, tt = 0.0, ts = 0.0;
+    double rc = rr;  // (r,cr) for the next iteration
     if (err < a.tol) {
         early = 1;  // :382-383
     } else if (!(err == err)) {
@@ -1624,45 +1682,49 @@ __global__ void __launch_bounds__(SMALL_THREADS, 1)
                 it = it - 1;
                 break;
             }
-            double rc = 0.0;
-            pass([&](int o, int, int, int) { rc += r[o] * cr[o]; });
-            rho = csum(rc);                 // :391
+            rho = rc;                                // :391
             bet = (rho / nrm) * (alf / omg);         // :392
-            pass([&](int o, int, int, int) { tq[o] = r[o] - bet * (omg * v1[o]); });  // :393
-            precondition(tq);                        // s, :394-396
-            pass([&](int o, int, int, int) { p[o] = sb[o] + bet * p[o]; });           // :397
+            // t = r - bet (omg v1) (:393) and s = M t, p = s + bet p (:394-397)
+            precondition(tq, [&](int o) { return tq[o] = r[o] - bet * (omg * v1[o]); }, true,
+                         bet);
             double cv = 0.0;
-            pass([&](int o, int k, int j, int i) {
+            each([&](int o, int k, int j, int i) {
                 const double v = op.ax(p, k, j, i, op.ap(k, j, i));  // :399-400
                 v1[o] = v;
                 cv += cr[o] * v;
             });
-            nrm = csum(cv);                 // :401
+            nrm = csum1(cv);                         // :401
             alf = rho / nrm;                         // :403
-            pass([&](int o, int, int, int) { sv[o] = r[o] - alf * v1[o]; });  // :404
-            precondition(sv);                        // cs in sb, :405-407
+            // s = r - alf v1 (:404) and cs = M s (:405-407), cs in sb
+            precondition(sv, [&](int o) { return sv[o] = r[o] - alf * v1[o]; }, false, 0.0);
             double t2 = 0.0, t3 = 0.0;
-            pass([&](int o, int k, int j, int i) {
+            each([&](int o, int k, int j, int i) {
                 const double tv = op.ax(sb, k, j, i, op.ap(k, j, i));  // :408-409
                 tq[o] = tv;
                 t2 += tv * tv;
                 t3 += tv * sv[o];
             });
-            tt = csum(t2);                  // :410
-            ts = csum(t3);                  // :411
+            csum2(t2, t3);
+            tt = t2;                                 // :410
+            ts = t3;                                 // :411
             omg = ts / tt;                           // :412
             if (fabs(omg) < a.tiny) {                // :414-417
                 status = DCM_E_BREAKDOWN;
                 break;
             }
-            double r2 = 0.0;
-            pass([&](int o, int, int, int) {
+            // x and r (:419-420), with (r,r) for the test and (r,cr) for the
+            // next iteration's rho
+            double r2s = 0.0, rcs = 0.0;
+            each([&](int o, int, int, int) {
                 x[o] = x[o] + alf * p[o] + omg * sb[o];  // :419
                 const double rv = sv[o] - omg * tq[o];   // :420
                 r[o] = rv;
-                r2 += rv * rv;
+                r2s += rv * rv;
+                rcs += rv * cr[o];
             });
-            err = sqrt(csum(r2)) / sc;      // :423
+            csum2(r2s, rcs);
+            rc = rcs;
+            err = sqrt(r2s) / sc;                    // :423
             nrm = rho;                               // :425
             if (err < a.tol) break;                  // :428
             if (!(err == err)) {
