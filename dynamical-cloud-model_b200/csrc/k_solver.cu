@@ -1491,8 +1491,8 @@ static void no_cheb(SolverArgs& a) {
 // iteration t = r - bet (omg v1), the three Jacobi sweeps of precondition
 // (:241-270; s = q/a_p, then s + (q - A s)/a_p), p = s + bet p, v1 = A p,
 // s = r - alf v1, cs = M s, t = A cs, the x and r updates.  The points are
-// dealt to the cluster's threads in turn; every pass ends with a cluster
-// barrier (release / acquire at cluster scope, so the next pass reads the
+// dealt to the cluster's threads in turn; passes are separated by cluster
+// barriers (release / acquire at cluster scope, so the next pass reads the
 // neighbours other blocks wrote).  Pointwise statements share a pass with
 // the statement before or after them (t and s with s/a_p, p with the last
 // sweep, (r,cr) with the r update), sums taken together share one barrier,
