@@ -75,3 +75,37 @@ def test_binding_signatures_match_the_header():
     bad = {n: (len(getattr(lib, n).argtypes), k) for n, k in arity.items()
            if len(getattr(lib, n).argtypes or ()) != k}
     assert not bad, bad
+
+
+def test_header_compiles_as_c_and_links(tmp_path):
+    """A C99 translation unit includes include/dcm.h, takes the address of
+    every declared function and links against the library as a C host (the
+    layer under the Fortran ISO_C_BINDING interface) would; the program runs
+    without a GPU."""
+    import shutil
+    import subprocess
+
+    import pytest
+
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    dcm = load_dcm()
+    names = declared()
+    src = tmp_path / "abi.c"
+    src.write_text(
+        "#include <stdio.h>\n#include <string.h>\n#include \"dcm.h\"\n"
+        "int main(void) {\n"
+        "    void (*fns[])(void) = {\n" +
+        "".join("        (void (*)(void))%s,\n" % n for n in names) +
+        "    };\n"
+        "    if (strcmp(dcm_status_string(0), \"ok\") != 0) return 1;\n"
+        "    printf(\"%d\\n\", (int)(sizeof fns / sizeof fns[0]));\n"
+        "    return 0;\n}\n")
+    exe = tmp_path / "abi"
+    libdir = os.path.dirname(dcm.LIBPATH)
+    subprocess.run([cc, "-std=c99", "-Wall", "-Wextra", "-Werror", "-pedantic",
+                    "-I" + os.path.join(ROOT, "include"), str(src), dcm.LIBPATH,
+                    "-Wl,-rpath," + libdir, "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout
+    assert int(out) == len(names)
