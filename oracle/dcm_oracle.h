@@ -177,6 +177,20 @@ typedef struct {
     double *vism, *vist, *strain;         /* subgrid fields (viscous only) */
 } orc_state;
 
+/* ---- PAMM sedimentation transport (dcm_oracle_col.c): mpdata_vec_1d of
+ *      one column (pamm/sfvt/advection_1d.F90:463-778; w, dz, dzn, rhoa,
+ *      rhoan as w(-l_h+1:kp+r_h), psi_in(-r_h+1:kp+r_h, 1:nq)), and ncol
+ *      columns with the caller's nsub passes of dt/nsub each
+ *      (pamm/microphysics.f90:3139-3183).                                     */
+void orc_mpdata_vec_1d(double dt, const double *dz, const double *dzn, const double *rhoa,
+                       const double *rhoan, int kp, int nq, int l_h, int r_h, const double *w,
+                       double *psi_in, int kord, int monotone, int neumann);
+void orc_mpdata_vec_1d_columns(int ncol, int kp, int nq, int l_h, int r_h, const double *dt,
+                               const int *nsub, const double *dz, const double *dzn,
+                               const double *rhoa, const double *rhoan, int metric_stride,
+                               const double *w, double *psi, int kord, int monotone,
+                               int neumann);
+
 /* pre-loop velocity boundary fix-up (driver_code.f90:287-295) */
 void orc_driver_start(const orc_grid *g, orc_state *s);
 /* one pass of the time loop; returns ORC_* status of the pressure solve */

@@ -20,7 +20,8 @@ _dp = C.POINTER(C.c_double)
 
 def build(force=False):
     src = [os.path.join(HERE, f)
-           for f in ("dcm_oracle.c", "dcm_oracle_sgm.c", "dcm_oracle.h", "Makefile")]
+           for f in ("dcm_oracle.c", "dcm_oracle_sgm.c", "dcm_oracle_col.c", "dcm_oracle.h",
+                     "Makefile")]
     if force or not os.path.exists(LIBPATH) or \
             any(os.path.getmtime(s) > os.path.getmtime(LIBPATH) for s in src):
         subprocess.run(["make", "-s", "-C", HERE], check=True)
@@ -337,6 +338,36 @@ class OracleModel:
         if self.nq:
             out["q"] = self.q
         return out
+
+
+def mpdata_vec_1d_columns(dt, nsub, dz, dzn, rhoa, rhoan, w, psi, kord=1, monotone=False,
+                          neumann=0, l_h=1, r_h=1):
+    """The PAMM sedimentation transport of ncol columns, in place on psi
+    (dcm_oracle_col.c: mpdata_vec_1d, pamm/sfvt/advection_1d.F90:463-778,
+    nsub[c] passes of dt[c]/nsub[c]).  w: (ncol, kp+l_h+r_h), each row
+    w(-l_h+1:kp+r_h); psi: (ncol, nq, kp+2 r_h), each column's
+    psi_in(-r_h+1:kp+r_h, 1:nq); dz, dzn, rhoa, rhoan: (kp+l_h+r_h,) shared
+    or (ncol, kp+l_h+r_h) per column."""
+    L = library()
+    ncol, nq, npsi = psi.shape
+    kp = npsi - 2 * r_h
+    nw = kp + l_h + r_h
+    assert psi.dtype == np.float64 and psi.flags.c_contiguous
+    w = np.ascontiguousarray(w, dtype=np.float64)
+    assert w.shape == (ncol, nw)
+    met = [np.ascontiguousarray(a, dtype=np.float64) for a in (dz, dzn, rhoa, rhoan)]
+    stride = nw if met[0].ndim == 2 else 0
+    for a in met:
+        assert a.shape == ((ncol, nw) if stride else (nw,))
+    dt = np.ascontiguousarray(np.broadcast_to(np.asarray(dt, dtype=np.float64), (ncol,)))
+    ns = None if nsub is None else np.ascontiguousarray(
+        np.broadcast_to(np.asarray(nsub, dtype=np.int32), (ncol,)))
+    L.orc_mpdata_vec_1d_columns(
+        C.c_int(ncol), C.c_int(kp), C.c_int(nq), C.c_int(l_h), C.c_int(r_h), _p(dt),
+        None if ns is None else ns.ctypes.data_as(C.POINTER(C.c_int)), *[_p(a) for a in met],
+        C.c_int(stride), _p(w), _p(psi), C.c_int(kord), C.c_int(int(bool(monotone))),
+        C.c_int(neumann))
+    return psi
 
 
 def _fortran_stack(fields):
