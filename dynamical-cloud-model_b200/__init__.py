@@ -118,6 +118,8 @@ def library():
             "dcm_step": [P, C.c_int, C.POINTER(StepStats)],
             "dcm_state_download": [P, C.POINTER(_Fields)],
             "dcm_horizontal_means_noalloc": [C.c_int, C.c_int, C.c_int, P, P, P, P, P, P],
+            "dcm_mpdata_vec_1d": [C.c_int] * 5 + [_dp, C.POINTER(C.c_int)] + [_dp] * 4 +
+                                 [C.c_int, _dp, _dp, C.c_int, C.c_int, C.c_int],
             "dcm_profile_enable": [P, C.c_int],
             "dcm_profile_read": [P, _dp, C.POINTER(C.c_longlong), C.c_int],
             "dcm_solver_graphs": [P, C.c_int],
@@ -163,7 +165,8 @@ EXPORTS = ("dcm_create", "dcm_destroy", "dcm_status_string", "dcm_last_error",
            "dcm_set_launch_shape", "dcm_ensemble_create", "dcm_ensemble_destroy", "dcm_ensemble_member",
            "dcm_ensemble_step", "dcm_ensemble_last_error", "dcm_exchange_full_wo",
            "dcm_calculate_subgrid_3d", "dcm_output_open", "dcm_output_write",
-           "dcm_output_flush", "dcm_output_close", "dcm_output_last_error")
+           "dcm_output_flush", "dcm_output_close", "dcm_output_last_error",
+           "dcm_mpdata_vec_1d")
 
 PROF_CLASSES = ("setup", "jacobi", "matvec", "update", "post", "means", "sources", "rhs",
                 "adv_ref", "mp_shift", "upwind", "antidiff", "beta", "limit", "restore",
@@ -201,6 +204,41 @@ def check_decomposition(dims):
     st = library().dcm_check_decomposition(d)
     if st:
         raise DCMError(st, library().dcm_status_string(st).decode())
+
+
+def mpdata_vec_1d_columns(dt, nsub, dz, dzn, rhoa, rhoan, w, psi, kord=1, monotone=False,
+                          neumann=0, l_h=1, r_h=1):
+    """The PAMM sedimentation transport of ncol columns on the GPU, in place
+    on psi (dcm_mpdata_vec_1d: mpdata_vec_1d, pamm/sfvt/advection_1d.F90:463-778,
+    nsub[c] passes of dt[c]/nsub[c]).  w: (ncol, kp+l_h+r_h), each row
+    w(-l_h+1:kp+r_h); psi: (ncol, nq, kp+2 r_h) C-contiguous, each column's
+    psi_in(-r_h+1:kp+r_h, 1:nq); dz, dzn, rhoa, rhoan: (kp+l_h+r_h,) shared or
+    (ncol, kp+l_h+r_h) per column.  dt and nsub: scalars or one per column
+    (nsub None: one pass)."""
+    if not (isinstance(psi, np.ndarray) and psi.dtype == np.float64 and psi.ndim == 3 and
+            psi.flags.c_contiguous):
+        raise TypeError("psi: a C-contiguous float64 array (ncol, nq, kp+2 r_h)")
+    ncol, nq, npsi = psi.shape
+    kp = npsi - 2 * r_h
+    nw = kp + l_h + r_h
+    w = np.ascontiguousarray(w, dtype=np.float64)
+    if w.shape != (ncol, nw):
+        raise TypeError("w: shape (ncol, kp+l_h+r_h)")
+    met = [np.ascontiguousarray(a, dtype=np.float64) for a in (dz, dzn, rhoa, rhoan)]
+    stride = nw if met[0].ndim == 2 else 0
+    for a in met:
+        if a.shape != ((ncol, nw) if stride else (nw,)):
+            raise TypeError("dz, dzn, rhoa, rhoan: shape (kp+l_h+r_h,) or (ncol, kp+l_h+r_h)")
+    dt = np.ascontiguousarray(np.broadcast_to(np.asarray(dt, dtype=np.float64), (ncol,)))
+    ns = None if nsub is None else np.ascontiguousarray(
+        np.broadcast_to(np.asarray(nsub, dtype=np.int32), (ncol,)))
+    st = library().dcm_mpdata_vec_1d(
+        ncol, kp, nq, l_h, r_h, _ptr(dt),
+        None if ns is None else ns.ctypes.data_as(C.POINTER(C.c_int)), *[_ptr(a) for a in met],
+        stride, _ptr(w), _ptr(psi), int(kord), int(bool(monotone)), int(neumann))
+    if st:
+        raise DCMError(st, library().dcm_status_string(st).decode())
+    return psi
 
 
 class DynamicalCore:

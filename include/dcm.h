@@ -155,6 +155,25 @@ int dcm_advance_scalar_fields_3d(dcm_handle *h, double dt, double *q,
                                  const double *sq, double *th,
                                  const double *sth, int nq, int moisture);
 
+/* The PAMM microphysics' sedimentation transport, mpdata_vec_1d
+ * (pamm/sfvt/advection_1d.F90:463-778, with first_order_upstream_1d :35-74)
+ * for ncol independent columns at once, each with the caller's sub-stepping
+ * loop (pamm/microphysics.f90:3139-3145, 3158-3164, 3177-3183): column c takes
+ * nsub[c] passes of dt[c]/nsub[c] (nsub NULL: one pass).  Host arrays, column
+ * after column: w, ncol x (kp+l_h+r_h), each row w(-l_h+1:kp+r_h); psi, ncol x
+ * nq x (kp+2 r_h), each column psi_in(-r_h+1:kp+r_h, 1:nq) in Fortran order,
+ * advanced in place; dz, dzn, rhoa, rhoan shared by all columns
+ * (metric_stride 0, kp+l_h+r_h values each) or one row per column
+ * (metric_stride = kp+l_h+r_h).  kord, monotone, neumann as the reference's.
+ * Runs on the calling thread's current device and returns when psi is back
+ * on the host.  DCM_E_ARG for l_h or r_h < 1, nsub[c] < 1, or a column too
+ * tall for one warp's shared memory ((nq+4)(kp+2 r_h) + 3(kp+l_h+r_h) + nq
+ * doubles above 200 KiB). */
+int dcm_mpdata_vec_1d(int ncol, int kp, int nq, int l_h, int r_h, const double *dt,
+                      const int *nsub, const double *dz, const double *dzn,
+                      const double *rhoa, const double *rhoan, int metric_stride,
+                      const double *w, double *psi, int kord, int monotone, int neumann);
+
 /* Halo exchanges of mpi_module.f90 for one rank: exchange_full (:926-1271),
  * exchange_along_dim (:700-910), exchange_along_dim_wo (:1285-1494),
  * exchange_full_wo (:1511-1855). */

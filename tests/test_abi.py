@@ -109,3 +109,19 @@ def test_header_compiles_as_c_and_links(tmp_path):
                     "-Wl,-rpath," + libdir, "-o", str(exe)], check=True)
     out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout
     assert int(out) == len(names)
+
+
+def test_column_transport_checks_arguments_before_the_device():
+    """dcm_mpdata_vec_1d validates its arguments on the host: bad halo
+    widths or options return DCM_E_ARG and zero columns return DCM_OK,
+    without touching a device."""
+    dcm = load_dcm()
+    lib = dcm.library()
+    call = lambda *a: lib.dcm_mpdata_vec_1d(*a)  # noqa: E731
+    none = [None] * 4
+    assert call(3, 10, 1, 0, 1, None, None, *none, 0, None, None, 1, 0, 0) == dcm.DCM_E_ARG
+    assert call(3, 10, 1, 1, 0, None, None, *none, 0, None, None, 1, 0, 0) == dcm.DCM_E_ARG
+    assert call(3, 10, 1, 1, 1, None, None, *none, 0, None, None, 1, 0, 3) == dcm.DCM_E_ARG
+    assert call(3, 10, 1, 1, 1, None, None, *none, 7, None, None, 1, 0, 0) == dcm.DCM_E_ARG
+    assert call(3, 10, 1, 1, 1, None, None, *none, 0, None, None, 1, 0, 0) == dcm.DCM_E_ARG
+    assert call(0, 10, 1, 1, 1, None, None, *none, 0, None, None, 1, 0, 0) == dcm.DCM_OK
