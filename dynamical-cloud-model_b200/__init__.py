@@ -120,6 +120,8 @@ def library():
             "dcm_horizontal_means_noalloc": [C.c_int, C.c_int, C.c_int, P, P, P, P, P, P],
             "dcm_mpdata_vec_1d": [C.c_int] * 5 + [_dp, C.POINTER(C.c_int)] + [_dp] * 4 +
                                  [C.c_int, _dp, _dp, C.c_int, C.c_int, C.c_int],
+            "dcm_mpdata_vec_1d_device": [C.c_int] * 5 + [P, P] + [P] * 4 +
+                                        [C.c_int, P, P, C.c_int, C.c_int, C.c_int, P],
             "dcm_profile_enable": [P, C.c_int],
             "dcm_profile_read": [P, _dp, C.POINTER(C.c_longlong), C.c_int],
             "dcm_solver_graphs": [P, C.c_int],
@@ -166,7 +168,7 @@ EXPORTS = ("dcm_create", "dcm_destroy", "dcm_status_string", "dcm_last_error",
            "dcm_ensemble_step", "dcm_ensemble_last_error", "dcm_exchange_full_wo",
            "dcm_calculate_subgrid_3d", "dcm_output_open", "dcm_output_write",
            "dcm_output_flush", "dcm_output_close", "dcm_output_last_error",
-           "dcm_mpdata_vec_1d")
+           "dcm_mpdata_vec_1d", "dcm_mpdata_vec_1d_device")
 
 PROF_CLASSES = ("setup", "jacobi", "matvec", "update", "post", "means", "sources", "rhs",
                 "adv_ref", "mp_shift", "upwind", "antidiff", "beta", "limit", "restore",

@@ -207,7 +207,7 @@ __global__ void __launch_bounds__(32 * COL_WARPS) k_column_mpdata(ColArgs a) {
     __syncwarp();
     const size_t mo = (size_t)c * a.mstride + (a.l_h - 1);
     const double *dz = a.dz + mo, *dzn = a.dzn + mo, *rhoa = a.rhoa + mo, *rhoan = a.rhoan + mo;
-    const int ns = a.nsub ? a.nsub[c] : 1;
+    const int ns = a.nsub ? max(a.nsub[c], 1) : 1;
     const double dt = a.dt[c] / (double)ns;
     for (int s = 0; s < ns; s++)
         col_mpdata(a, dt, dz, dzn, rhoa, rhoan, win, psi, store, ws1, ws2, tmp, bup, bdn, ming,
@@ -217,43 +217,21 @@ __global__ void __launch_bounds__(32 * COL_WARPS) k_column_mpdata(ColArgs a) {
 
 }  // namespace
 
-extern "C" int dcm_mpdata_vec_1d(int ncol, int kp, int nq, int l_h, int r_h, const double* dt,
-                                 const int* nsub, const double* dz, const double* dzn,
-                                 const double* rhoa, const double* rhoan, int metric_stride,
-                                 const double* w, double* psi, int kord, int monotone,
-                                 int neumann) {
+// shape checks shared by both entry points; fills the launch shape
+static int column_shape(int ncol, int kp, int nq, int l_h, int r_h, int metric_stride,
+                        int kord, int neumann, ColArgs& a, int& warps, size_t& smem) {
     if (ncol < 0 || kp < 1 || nq < 1 || l_h < 1 || r_h < 1 || kord < 0 || neumann < 0 ||
         neumann > 2)
         return DCM_E_ARG;
     const int nw = kp + l_h + r_h, npsi = kp + 2 * r_h;
     if (metric_stride != 0 && metric_stride != nw) return DCM_E_ARG;
-    if (ncol == 0) return DCM_OK;
-    if (!dt || !dz || !dzn || !rhoa || !rhoan || !w || !psi) return DCM_E_ARG;
-    if (nsub)
-        for (int c = 0; c < ncol; c++)
-            if (nsub[c] < 1) return DCM_E_ARG;
     const int per_warp = (nq + 4) * npsi + 3 * nw + nq;
     const size_t warp_bytes = (size_t)per_warp * sizeof(double);
     constexpr size_t max_bytes = 200 * 1024;
     if (warp_bytes > max_bytes) return DCM_E_ARG;  // a column too tall for shared memory
-    const int warps = std::max(1, std::min<int>(COL_WARPS, (int)(max_bytes / warp_bytes)));
-    const size_t nmet = (size_t)(metric_stride ? ncol : 1) * nw;
-    const size_t bytes_dt = (size_t)ncol * sizeof(double), bytes_ns = (size_t)ncol * sizeof(int);
-    const size_t bytes_met = nmet * sizeof(double), bytes_w = (size_t)ncol * nw * sizeof(double);
-    const size_t bytes_psi = (size_t)ncol * nq * npsi * sizeof(double);
-    char* buf = nullptr;
-    const size_t al = 256;
-    auto up = [&](size_t b) { return (b + al - 1) / al * al; };
-    const size_t total = up(bytes_dt) + up(bytes_ns) + 4 * up(bytes_met) + up(bytes_w) +
-                         up(bytes_psi);
-    if (cudaMalloc(&buf, total) != cudaSuccess) return DCM_E_CUDA;
-    size_t off = 0;
-    auto take = [&](size_t b) {
-        char* p = buf + off;
-        off += up(b);
-        return p;
-    };
-    ColArgs a{};
+    warps = std::max(1, std::min<int>(COL_WARPS, (int)(max_bytes / warp_bytes)));
+    smem = (size_t)warps * warp_bytes;
+    a = ColArgs{};
     a.ncol = ncol;
     a.kp = kp;
     a.nq = nq;
@@ -264,8 +242,77 @@ extern "C" int dcm_mpdata_vec_1d(int ncol, int kp, int nq, int l_h, int r_h, con
     a.per_warp = per_warp;
     a.mstride = metric_stride;
     a.kord = kord;
-    a.monotone = monotone ? 1 : 0;
     a.neumann = neumann;
+    return DCM_OK;
+}
+
+static bool column_launch(const ColArgs& a, int warps, size_t smem, cudaStream_t st) {
+    if (smem > 48 * 1024 &&
+        cudaFuncSetAttribute(k_column_mpdata, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem) != cudaSuccess)
+        return false;
+    k_column_mpdata<<<(a.ncol + warps - 1) / warps, 32 * warps, smem, st>>>(a);
+    return cudaPeekAtLastError() == cudaSuccess;
+}
+
+extern "C" int dcm_mpdata_vec_1d_device(int ncol, int kp, int nq, int l_h, int r_h,
+                                        const double* dt, const int* nsub, const double* dz,
+                                        const double* dzn, const double* rhoa,
+                                        const double* rhoan, int metric_stride,
+                                        const double* w, double* psi, int kord, int monotone,
+                                        int neumann, void* stream) {
+    ColArgs a;
+    int warps = 1;
+    size_t smem = 0;
+    const int st = column_shape(ncol, kp, nq, l_h, r_h, metric_stride, kord, neumann, a,
+                                warps, smem);
+    if (st != DCM_OK || ncol == 0) return st;
+    if (!dt || !dz || !dzn || !rhoa || !rhoan || !w || !psi) return DCM_E_ARG;
+    if (cudaPeekAtLastError() != cudaSuccess) return DCM_E_CUDA;  // not ours to clear
+    a.monotone = monotone ? 1 : 0;
+    a.dt = dt;
+    a.nsub = nsub;
+    a.dz = dz;
+    a.dzn = dzn;
+    a.rhoa = rhoa;
+    a.rhoan = rhoan;
+    a.w = w;
+    a.psi = psi;
+    return column_launch(a, warps, smem, (cudaStream_t)stream) ? DCM_OK : DCM_E_CUDA;
+}
+
+extern "C" int dcm_mpdata_vec_1d(int ncol, int kp, int nq, int l_h, int r_h, const double* dt,
+                                 const int* nsub, const double* dz, const double* dzn,
+                                 const double* rhoa, const double* rhoan, int metric_stride,
+                                 const double* w, double* psi, int kord, int monotone,
+                                 int neumann) {
+    ColArgs a;
+    int warps = 1;
+    size_t smem = 0;
+    const int st = column_shape(ncol, kp, nq, l_h, r_h, metric_stride, kord, neumann, a,
+                                warps, smem);
+    if (st != DCM_OK || ncol == 0) return st;
+    if (!dt || !dz || !dzn || !rhoa || !rhoan || !w || !psi) return DCM_E_ARG;
+    if (nsub)
+        for (int c = 0; c < ncol; c++)
+            if (nsub[c] < 1) return DCM_E_ARG;
+    const int nw = a.nw, npsi = a.npsi;
+    const size_t nmet = (size_t)(metric_stride ? ncol : 1) * nw;
+    const size_t bytes_dt = (size_t)ncol * sizeof(double), bytes_ns = (size_t)ncol * sizeof(int);
+    const size_t bytes_met = nmet * sizeof(double), bytes_w = (size_t)ncol * nw * sizeof(double);
+    const size_t bytes_psi = (size_t)ncol * nq * npsi * sizeof(double);
+    const size_t al = 256;
+    auto up = [&](size_t b) { return (b + al - 1) / al * al; };
+    const size_t total = up(bytes_dt) + up(bytes_ns) + 4 * up(bytes_met) + up(bytes_w) +
+                         up(bytes_psi);
+    char* buf = nullptr;
+    if (cudaMalloc(&buf, total) != cudaSuccess) return DCM_E_CUDA;
+    size_t off = 0;
+    auto take = [&](size_t b) {
+        char* p = buf + off;
+        off += up(b);
+        return p;
+    };
     double* d_dt = (double*)take(bytes_dt);
     int* d_ns = (int*)take(bytes_ns);
     double* d_met[4];
@@ -279,6 +326,7 @@ extern "C" int dcm_mpdata_vec_1d(int ncol, int kp, int nq, int l_h, int r_h, con
         good = cudaMemcpy(d_met[q], h_met[q], bytes_met, cudaMemcpyHostToDevice) == cudaSuccess;
     if (good) good = cudaMemcpy(d_w, w, bytes_w, cudaMemcpyHostToDevice) == cudaSuccess;
     if (good) good = cudaMemcpy(d_psi, psi, bytes_psi, cudaMemcpyHostToDevice) == cudaSuccess;
+    a.monotone = monotone ? 1 : 0;
     a.dt = d_dt;
     a.nsub = nsub ? d_ns : nullptr;
     a.dz = d_met[0];
@@ -287,14 +335,7 @@ extern "C" int dcm_mpdata_vec_1d(int ncol, int kp, int nq, int l_h, int r_h, con
     a.rhoan = d_met[3];
     a.w = d_w;
     a.psi = d_psi;
-    const size_t smem = (size_t)warps * warp_bytes;
-    if (good && smem > 48 * 1024)
-        good = cudaFuncSetAttribute(k_column_mpdata, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)smem) == cudaSuccess;
-    if (good) {
-        k_column_mpdata<<<(ncol + warps - 1) / warps, 32 * warps, smem>>>(a);
-        good = cudaGetLastError() == cudaSuccess;
-    }
+    if (good) good = column_launch(a, warps, smem, 0);
     if (good) good = cudaMemcpy(psi, d_psi, bytes_psi, cudaMemcpyDeviceToHost) == cudaSuccess;
     const bool freed = cudaFree(buf) == cudaSuccess;
     return good && freed ? DCM_OK : DCM_E_CUDA;

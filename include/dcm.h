@@ -173,6 +173,16 @@ int dcm_mpdata_vec_1d(int ncol, int kp, int nq, int l_h, int r_h, const double *
                       const int *nsub, const double *dz, const double *dzn,
                       const double *rhoa, const double *rhoan, int metric_stride,
                       const double *w, double *psi, int kord, int monotone, int neumann);
+/* The same with every array in device memory, queued on `stream` (NULL: the
+ * default stream): for a host that keeps the columns on the GPU.  Allocates
+ * nothing, returns when the work is queued; nsub[c] < 1 counts as one pass.
+ * A CUDA error already pending on the calling thread returns DCM_E_CUDA at
+ * once, queueing nothing. */
+int dcm_mpdata_vec_1d_device(int ncol, int kp, int nq, int l_h, int r_h, const double *dt,
+                             const int *nsub, const double *dz, const double *dzn,
+                             const double *rhoa, const double *rhoan, int metric_stride,
+                             const double *w, double *psi, int kord, int monotone,
+                             int neumann, void *stream);
 
 /* Halo exchanges of mpi_module.f90 for one rank: exchange_full (:926-1271),
  * exchange_along_dim (:700-910), exchange_along_dim_wo (:1285-1494),

@@ -70,3 +70,30 @@ def test_column_transport_rejects_bad_arguments(dcm):
     lib = dcm.library()
     assert lib.dcm_mpdata_vec_1d(2, 10, 1, 0, 1, None, None, None, None, None, None, 0, None,
                                  None, 1, 0, 0) == dcm.DCM_E_ARG  # l_h < 1
+
+
+def test_device_entry_point_matches_the_host_one(dcm):
+    """dcm_mpdata_vec_1d_device on device arrays, queued on a stream, gives
+    the host entry point's result bit for bit (the same kernel)."""
+    import ctypes as C
+
+    import torch
+
+    ncol, nq, kp = 70, 3, 45
+    met, w, psi = _columns(400, ncol, nq, kp, 1, 1, True)
+    dt = np.linspace(0.5, 2.0, ncol)
+    nsub = (1 + np.arange(ncol) % 4).astype(np.int32)
+    ref = psi.copy()
+    dcm.mpdata_vec_1d_columns(dt, nsub, *met, w, ref, kord=3, monotone=True, neumann=1)
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to("cuda")  # noqa: E731
+    d_dt, d_ns, d_w, d_psi = dev(dt), dev(nsub), dev(w), dev(psi)
+    d_met = [dev(a) for a in met]
+    stream = torch.cuda.Stream()
+    torch.cuda.synchronize()  # the uploads (on torch's stream) have landed
+    p = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+    st = dcm.library().dcm_mpdata_vec_1d_device(
+        ncol, kp, nq, 1, 1, p(d_dt), p(d_ns), *[p(t) for t in d_met], kp + 2, p(d_w), p(d_psi),
+        3, 1, 1, C.c_void_p(stream.cuda_stream))
+    assert st == dcm.DCM_OK
+    stream.synchronize()
+    assert np.array_equal(d_psi.cpu().numpy(), ref)
