@@ -111,12 +111,14 @@ __device__ void col_mpdata(const ColArgs& a, double dt, const double* dz, const 
         return;
     }
     const int ow = a.l_h - 1;
-    double* w1 = ws1 + ow;  // level-0 views of the working velocities
-    double* w2 = ws2 + ow;
-    for (int i = lane; i < nw; i += 32) ws2[i] = 0.0;  // :530
+    const bool anti = a.kord > 1;
+    double* w1 = anti ? ws1 + ow : nullptr;  // level-0 views of the working velocities
+    double* w2 = anti ? ws2 + ow : nullptr;
+    if (anti)
+        for (int i = lane; i < nw; i += 32) ws2[i] = 0.0;  // :530 (read only when kord > 1)
     const double* wt = win + ow;                        // :534-535
     double* wt_sav = w1;
-    const double* ps = store + op;  // the limiter's psi (:542-545)
+    const double* ps = anti ? store + op : nullptr;  // the limiter's psi (:542-545)
     double* po = P(0);              // psi_old (:547)
     if (a.kord > 1)
         for (int i = lane; i < npsi; i += 32) store[i] = psi[i];
@@ -184,26 +186,44 @@ __device__ void col_mpdata(const ColArgs& a, double dt, const double* dz, const 
     __syncwarp();
 }
 
-__global__ void __launch_bounds__(32 * COL_WARPS) k_column_mpdata(ColArgs a) {
+// 8 blocks of 4 warps per SM (64 registers): the donor-cell form (the
+// sedimentation calls) took 0.237 ms for 65,536 columns of 128 levels and two
+// fields at this bound, 0.267 ms at 6 blocks and 0.361 ms unbounded (126
+// registers, 4 blocks)
+__global__ void __launch_bounds__(32 * COL_WARPS, 8) k_column_mpdata(ColArgs a) {
     extern __shared__ double col_sm[];
     const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int c = blockIdx.x * (blockDim.x >> 5) + wib;
     if (c >= a.ncol) return;  // the whole warp: no block-wide barrier follows
-    double* psi = col_sm + (size_t)wib * a.per_warp;  // [nq][npsi]
-    double* store = psi + (size_t)a.nq * a.npsi;      // [npsi]
-    double* win = store + a.npsi;                     // [nw]
-    double* ws1 = win + a.nw;
-    double* ws2 = ws1 + a.nw;
-    double* tmp = ws2 + a.nw;  // [npsi]
-    double* bup = tmp + a.npsi;
-    double* bdn = bup + a.npsi;
-    double* ming = bdn + a.npsi;  // [nq]
-    double* gpsi = a.psi + (size_t)c * a.nq * a.npsi;
-    for (int i = lane; i < a.nq * a.npsi; i += 32) psi[i] = gpsi[i];
-    for (int i = lane; i < a.nw; i += 32) {
-        win[i] = a.w[(size_t)c * a.nw + i];
-        ws1[i] = 0.0;
+    // [nq][npsi] fields, then with kord > 1 the limiter's psi, the input and
+    // the two working velocities, the flux buffer, beta_up, beta_down, the
+    // minima; with kord <= 1 (the donor cell alone) the flux buffer, the
+    // input velocity and the minima only, so that more columns fit an SM
+    double* psi = col_sm + (size_t)wib * a.per_warp;
+    double* rest = psi + (size_t)a.nq * a.npsi;
+    double *store = nullptr, *ws1 = nullptr, *ws2 = nullptr, *bup = nullptr, *bdn = nullptr;
+    double *tmp, *win, *ming;
+    if (a.kord > 1) {
+        store = rest;
+        win = store + a.npsi;
+        ws1 = win + a.nw;
+        ws2 = ws1 + a.nw;
+        tmp = ws2 + a.nw;
+        bup = tmp + a.npsi;
+        bdn = bup + a.npsi;
+        ming = bdn + a.npsi;
+    } else {
+        tmp = rest;
+        win = tmp + a.npsi;
+        ming = win + a.nw;
     }
+    double* gpsi = a.psi + (size_t)c * a.nq * a.npsi;
+#pragma unroll 4
+    for (int i = lane; i < a.nq * a.npsi; i += 32) psi[i] = gpsi[i];
+#pragma unroll 4
+    for (int i = lane; i < a.nw; i += 32) win[i] = a.w[(size_t)c * a.nw + i];
+    if (ws1)
+        for (int i = lane; i < a.nw; i += 32) ws1[i] = 0.0;
     __syncwarp();
     const size_t mo = (size_t)c * a.mstride + (a.l_h - 1);
     const double *dz = a.dz + mo, *dzn = a.dzn + mo, *rhoa = a.rhoa + mo, *rhoan = a.rhoan + mo;
@@ -212,6 +232,7 @@ __global__ void __launch_bounds__(32 * COL_WARPS) k_column_mpdata(ColArgs a) {
     for (int s = 0; s < ns; s++)
         col_mpdata(a, dt, dz, dzn, rhoa, rhoan, win, psi, store, ws1, ws2, tmp, bup, bdn, ming,
                    lane);
+#pragma unroll 4
     for (int i = lane; i < a.nq * a.npsi; i += 32) gpsi[i] = psi[i];
 }
 
@@ -225,7 +246,7 @@ static int column_shape(int ncol, int kp, int nq, int l_h, int r_h, int metric_s
         return DCM_E_ARG;
     const int nw = kp + l_h + r_h, npsi = kp + 2 * r_h;
     if (metric_stride != 0 && metric_stride != nw) return DCM_E_ARG;
-    const int per_warp = (nq + 4) * npsi + 3 * nw + nq;
+    const int per_warp = kord > 1 ? (nq + 4) * npsi + 3 * nw + nq : (nq + 1) * npsi + nw + nq;
     const size_t warp_bytes = (size_t)per_warp * sizeof(double);
     constexpr size_t max_bytes = 200 * 1024;
     if (warp_bytes > max_bytes) return DCM_E_ARG;  // a column too tall for shared memory

@@ -167,8 +167,9 @@ int dcm_advance_scalar_fields_3d(dcm_handle *h, double dt, double *q,
  * (metric_stride = kp+l_h+r_h).  kord, monotone, neumann as the reference's.
  * Runs on the calling thread's current device and returns when psi is back
  * on the host.  DCM_E_ARG for l_h or r_h < 1, nsub[c] < 1, or a column too
- * tall for one warp's shared memory ((nq+4)(kp+2 r_h) + 3(kp+l_h+r_h) + nq
- * doubles above 200 KiB). */
+ * tall for one warp's shared memory (above 200 KiB: (nq+4)(kp+2 r_h) +
+ * 3(kp+l_h+r_h) + nq doubles with kord > 1, (nq+1)(kp+2 r_h) + kp+l_h+r_h +
+ * nq with kord <= 1). */
 int dcm_mpdata_vec_1d(int ncol, int kp, int nq, int l_h, int r_h, const double *dt,
                       const int *nsub, const double *dz, const double *dzn,
                       const double *rhoa, const double *rhoan, int metric_stride,
