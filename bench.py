@@ -717,6 +717,77 @@ def run_reference(args, rank, world):
                     "d2h_bytes_per_step": 0}}
 
 
+def run_columns(args):
+    """--columns N: the PAMM sedimentation transport (dcm_mpdata_vec_1d_device)
+    on N seeded columns of 128 levels and two fields (fall speeds up to 8 m/s,
+    dt 2 s, the microphysics' n_step per column), device-resident, timed with
+    CUDA events over --steps calls after --warmup, L2 flushed before each;
+    beside it the oracle on all host cores over the same columns, once.  One
+    JSON line (kord 1, the sedimentation calls; kord 3 with the limiter)."""
+    import ctypes as C
+
+    import torch
+    pkg = load_pkg()
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    oracle.set_threads(os.cpu_count() or 1, False)
+    lib = pkg.library()
+    ncol, nq, kp = args.columns, 2, 128
+    nw = kp + 2
+    rng = np.random.default_rng(3)
+    z = np.linspace(0.0, 1.0, nw)
+    met = [np.ascontiguousarray(x) for x in (40.0 + 20.0 * z, 45.0 + 10.0 * z, 1.2 - 0.5 * z,
+                                             1.2 - 0.5 * z)]
+    w = -8.0 * rng.random((ncol, nw)) * rng.random((ncol, 1))
+    psi = 1e-3 * rng.random((ncol, nq, kp + 2)) * (rng.random((ncol, nq, kp + 2)) > 0.3)
+    dt = 2.0
+    nsub = np.maximum(np.ceil(np.max(np.abs(w), axis=1) * dt / met[0].min() * 2.0),
+                      1).astype(np.int32)
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to("cuda")  # noqa: E731
+    d_dt, d_ns, d_w, d_psi0 = dev(np.full(ncol, dt)), dev(nsub), dev(w), dev(psi)
+    d_met = [dev(a) for a in met]
+    d_psi = d_psi0.clone()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > L2
+    s = torch.cuda.current_stream()
+    p = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+    out = {"metric": "columns/s of the sedimentation transport (mpdata_vec_1d)",
+           "unit": "columns/s", "columns": ncol, "levels": kp, "fields": nq,
+           "mean_passes": float(nsub.mean()), "steps": args.steps, "warmup": args.warmup}
+    for kord, mono in ((1, 0), (3, 1)):
+        def call():
+            st = lib.dcm_mpdata_vec_1d_device(ncol, kp, nq, 1, 1, p(d_dt), p(d_ns),
+                                              *[p(t) for t in d_met], 0, p(d_w), p(d_psi),
+                                              kord, mono, 0, C.c_void_p(s.cuda_stream))
+            if st:
+                raise RuntimeError("dcm_mpdata_vec_1d_device: status %d" % st)
+        for _ in range(args.warmup):
+            d_psi.copy_(d_psi0)
+            call()
+        ms = []
+        for _ in range(args.steps):
+            d_psi.copy_(d_psi0)
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(s)
+            call()
+            e1.record(s)
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        got = d_psi.cpu().numpy()
+        ref = psi.copy()
+        t0 = time.perf_counter()
+        oracle.mpdata_vec_1d_columns(dt, nsub, *met, w, ref, kord=kord, monotone=mono)
+        t_orc = time.perf_counter() - t0
+        med = float(np.median(ms))
+        out["kord%d" % kord] = {
+            "monotone": bool(mono), "ms": med, "value": ncol / (med / 1e3),
+            "gbs": (2 * psi.nbytes + w.nbytes) / (med / 1e3) / 1e9,
+            "oracle_ms": t_orc * 1e3, "oracle_cores": os.cpu_count(),
+            "max_rel_err_vs_oracle": float(np.max(np.abs(got - ref)) / np.max(np.abs(ref)))}
+    print(json.dumps(compact(out)), flush=True)
+
+
 def accuracy_vs_oracle(args):
     """--accuracy-vs-oracle N: the mixed form (as the benchmark runs it) and
     the FP64 path on the GPU, and the oracle's FP64 restatement of the
@@ -873,12 +944,18 @@ def main():
     ap.add_argument("--output-every", type=int, default=1)
     ap.add_argument("--accuracy-vs-oracle", type=int, default=0,
                     help="N: errors of both forms against the oracle after 1, 10, N steps")
+    ap.add_argument("--columns", type=int, default=0,
+                    help="N: the PAMM sedimentation transport on N columns, timed, beside "
+                         "the oracle")
     args = ap.parse_args()
     if args.run_case:
         run_case(args)
         return
     if args.accuracy_vs_oracle:
         accuracy_vs_oracle(args)
+        return
+    if args.columns:
+        run_columns(args)
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
